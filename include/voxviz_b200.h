@@ -1,0 +1,350 @@
+/*
+ * voxviz_b200.h - C ABI of the B200-native GigaVoxels sparse-octree ray caster.
+ *
+ * Everything a caller binds is declared here: plain C types, raw pointers and
+ * sizes, int status codes, no exceptions and no torch types.  Every entry point
+ * names the reference interface it replaces (paths are relative to the
+ * apecoraro/VoxVizThesis project root).
+ *
+ * Conventions
+ *  - Volume space is the reference's normalized space [0,1]^3, Z up
+ *    (GigaVoxelsRenderer.cpp:1674-1690 maps the world box to it; the builders
+ *    here put the volume box at [0,1]^3 so world == normalized space).
+ *  - A node is two uint32 words, exactly GigaVoxelsOctTree::Node::GpuDataStruct
+ *    (GigaVoxelsOctTree.h:72-80, setters GigaVoxelsOctTree.cpp:1309-1383):
+ *      word0: bit31 brick resident, bit30 constant node,
+ *             bits 29..20 / 19..10 / 9..0 child-block base x / y / z in the
+ *             node-pool grid (0,0,0 = no children)
+ *      word1: constant node: RGBA8 r | g<<8 | b<<16 | a<<24
+ *             otherwise:     brick pointer x<<20 | y<<10 | z (texel coords in
+ *                            the brick-pool grid, already offset by the border)
+ *  - Node-pool words passed across this ABI are in the reference texture order
+ *    of OctTreeNodePool::create3DTexture (GigaVoxelsOctTree NodePool.cpp:90-223):
+ *    a dim_x * dim_y * dim_z grid, x fastest, 2 words per node.
+ *  - Bricks are 8^3 voxels stored with a 1-voxel border (10^3 texels), x
+ *    fastest.  A brick-pool slot s = (sz*slots_y + sy)*slots_x + sx holds the
+ *    texels of grid region [10*sx, 10*sx+10) x ... of the reference 3D texture
+ *    (GigaVoxelsBrickPool.cpp:75-101), stored contiguously (brick-linear).
+ *  - Functions that take a `vv_ctx` run on that context's CUDA device and
+ *    stream.  Calls on one context must be externally serialised.
+ */
+#ifndef VOXVIZ_B200_H
+#define VOXVIZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VV_ABI_VERSION 1
+
+/* Status codes (GigaVoxelsBrickPool.cpp:148-150 and GigaVoxelsReader.cpp:106-221
+ * report failure as bool + std::cerr; here every call returns one of these). */
+typedef enum vv_status {
+    VV_OK = 0,
+    VV_ERR_ARG = 1,      /* invalid argument or size                        */
+    VV_ERR_OOM = 2,      /* device or host allocation failed                */
+    VV_ERR_CUDA = 3,     /* CUDA runtime error                              */
+    VV_ERR_TIMEOUT = 4,  /* a bounded device wait or loop ran out           */
+    VV_ERR_BOUNDS = 5,   /* a device-side index check failed                */
+    VV_ERR_STATE = 6,    /* call out of order (e.g. render before upload)   */
+    VV_ERR_NODEV = 7     /* no CUDA device / extension not usable           */
+} vv_status;
+
+/* Brick-pool texel formats. RGBA8 is GL_RGBA8 (GigaVoxelsBrickPool.cpp:45);
+ * the float formats hold the same normalized [0,1] values. */
+typedef enum vv_fmt {
+    VV_FMT_RGBA8 = 0,   /* 4 x uint8, unorm                              */
+    VV_FMT_FP16 = 1,    /* 4 x IEEE binary16                             */
+    VV_FMT_BF16 = 2,    /* 4 x bfloat16                                  */
+    VV_FMT_FP32 = 3     /* 4 x float                                     */
+} vv_fmt;
+
+#define VV_BRICK_DIM 8          /* interior voxels per axis               */
+#define VV_BRICK_STORED 10      /* stored texels per axis (1-voxel border) */
+#define VV_BRICK_TEXELS 1000    /* texels per stored brick                */
+#define VV_USAGE_SLOTS 12       /* node-usage entries per pixel (3 x RGBA32UI) */
+
+/* Per-draw uniforms.  The first block is exactly the set of uniforms read by
+ * VoxViz/Shaders/GigaVoxelsNoLighting.frag:3-26, derived on the host as
+ * GigaVoxelsRenderer::drawVolume does (GigaVoxelsRenderer.cpp:1630-1816).
+ * The second block replaces rasterisation of the volume box
+ * (GigaVoxels.vert:11-19) and of the near-plane quad (NearPlaneQuad.vert:11-20):
+ * pixel (px,py) (origin bottom-left, as gl_FragCoord) looks through the
+ * near-plane point near_origin + (px+0.5)*near_dx + (py+0.5)*near_dy. */
+typedef struct vv_uniforms {
+    float ray_step_size;           /* RayStepSize                          */
+    float brick_step_vector[3];    /* BrickStepVector                      */
+    float camera_position[3];      /* CameraPosition (normalized space)    */
+    float camera_up[3];            /* CameraUp (unit, world)               */
+    float camera_left[3];          /* CameraLeft (unit, world)             */
+    float vol_extent_min[3];       /* VolExtentMin                         */
+    float vol_extent_max[3];       /* VolExtentMax                         */
+    float brick_dimension[3];      /* BrickDimension                       */
+    float root_voxel_half_size;    /* RootVoxelHalfSize                    */
+    float brick_pool_dimension[3]; /* BrickPoolDimension (texels)          */
+    float pixel_size;              /* PixelSize                            */
+    float lod_scalar;              /* LodScalar                            */
+    float alpha_stop;              /* early-termination alpha (the shader's
+                                      literal 0.995f; a parameter here)    */
+    int32_t oct_tree_depth_minus_one; /* OctTreeDepthMinusOne             */
+    int32_t max_nodes_to_push;     /* MaxNodesToPushThisFrame              */
+    int32_t root_node_is_constant; /* RootNodeIsConstant                   */
+    int32_t jitter_tex_size;       /* JitterTexSize                        */
+    /* ray generation */
+    int32_t width;
+    int32_t height;
+    int32_t camera_inside;         /* 1: rays start on the near plane      */
+    int32_t max_segments;          /* loop bound per ray (0 = derived)     */
+    float near_origin[3];
+    float near_dx[3];
+    float near_dy[3];
+} vv_uniforms;
+
+/* One node-word update (OctTreeNodePool::update3DTexture,
+ * GigaVoxelsOctTreeNodePool.cpp:256-288). */
+typedef struct vv_node_patch {
+    uint32_t x, y, z;      /* node-pool grid position */
+    uint32_t word0, word1;
+} vv_node_patch;
+
+/* Outputs of one draw.  Pointers are DEVICE pointers on the context's device
+ * (NULL = not wanted; the context then uses internal scratch where a later
+ * pass needs the data). */
+typedef struct vv_frame_out {
+    float* color;             /* [H][W][4] FragColor (before blending)        */
+    uint32_t* usage;          /* [H][W][12] NodeUsageList[3] (GigaVoxels*.frag) */
+    uint32_t* mask;           /* [H][W] selection mask (GenerateSelectionMask.frag) */
+    uint32_t* requests;       /* [request_cap][4] CompressNodeUsageList output */
+    uint32_t* request_count;  /* [1] active-pixel count (histopyramid top), uncapped */
+    int32_t request_cap;      /* max compacted entries written (reference: 32768) */
+    int32_t compress_max_push;/* CompressNodeUsageList MaxNodesToPushThisFrame  */
+    int32_t passes;           /* VV_PASS_* bit set: which passes to run        */
+} vv_frame_out;
+
+#define VV_PASS_RAYCAST 1
+#define VV_PASS_SELECT 2
+#define VV_PASS_COMPACT 4
+#define VV_PASS_ALL 7
+
+typedef struct vv_ctx vv_ctx;
+
+typedef struct vv_params {
+    int32_t device;       /* CUDA device ordinal */
+    int32_t flags;        /* reserved, 0 */
+    int64_t reserved[4];
+} vv_params;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Replaces the GL context + BrickPool singleton set-up of
+ * GigaVoxelsRenderer::init (GigaVoxelsRenderer.cpp:341-607). */
+int vv_ctx_create(const vv_params* params, vv_ctx** out);
+int vv_ctx_destroy(vv_ctx* ctx);
+/* Last error message of this context ("" if none); valid until the next call. */
+const char* vv_last_error(const vv_ctx* ctx);
+const char* vv_status_string(int status);
+/* Use this CUDA stream (cudaStream_t) for every later call; NULL = default. */
+int vv_ctx_set_stream(vv_ctx* ctx, void* cuda_stream);
+int vv_ctx_synchronize(vv_ctx* ctx);
+/* Sticky device status word (VV_OK or the first device-side error code). */
+int vv_ctx_device_status(vv_ctx* ctx, int32_t* status, int32_t clear);
+int vv_abi_version(void);
+
+/* ---- node pool ---------------------------------------------------------- */
+
+/* Upload a whole node pool for octree slot `tree` (0..VV_MAX_TREES-1) from host
+ * words in reference texture order.  Replaces OctTreeNodePool::create3DTexture
+ * (GigaVoxelsOctTreeNodePool.cpp:90-223). dim_x/dim_y/dim_z must be even. */
+#define VV_MAX_TREES 8
+int vv_nodepool_upload(vv_ctx* ctx, int32_t tree, const uint32_t* words,
+                       int32_t dim_x, int32_t dim_y, int32_t dim_z);
+/* Apply n host-side patches.  Replaces OctTreeNodePool::update
+ * (GigaVoxelsOctTreeNodePool.cpp:230-288). */
+int vv_nodepool_patch(vv_ctx* ctx, int32_t tree, const vv_node_patch* patches,
+                      int32_t n);
+/* Read the node pool back in reference texture order (for checking). */
+int vv_nodepool_download(vv_ctx* ctx, int32_t tree, uint32_t* words);
+
+/* ---- brick pool ----------------------------------------------------------- */
+
+/* Create the brick pool: slots_x*slots_y*slots_z slots of 10^3 texels in
+ * `fmt`.  Replaces BrickPool::init / initSpecial (GigaVoxelsBrickPool.cpp:55-251).
+ * slots_* * 10 must be <= 1023 (10-bit brick pointers). */
+int vv_brickpool_create(vv_ctx* ctx, int32_t slots_x, int32_t slots_y,
+                        int32_t slots_z, int32_t fmt);
+/* Copy n bricks from host memory into the given slots.  `texels` holds n
+ * consecutive bricks of 1000 texels in the pool's format.  Replaces the PBO
+ * staging + glTexSubImage3D of BrickPool::uploadBrick / uploadPBOToTextures
+ * (GigaVoxelsBrickPool.cpp:451-559,729-813). */
+int vv_upload_bricks(vv_ctx* ctx, const uint32_t* slots, int32_t n,
+                     const void* texels);
+/* Same with device-resident brick data (`texels_dev`, `slots_dev` device ptrs). */
+int vv_upload_bricks_device(vv_ctx* ctx, const uint32_t* slots_dev, int32_t n,
+                            const void* texels_dev);
+/* Read the whole pool back (slot-major, brick-linear) into host memory. */
+int vv_brickpool_download(vv_ctx* ctx, void* texels);
+/* Device address of the pool texels (for callers that manage data on device). */
+int vv_brickpool_device_ptr(vv_ctx* ctx, void** ptr, size_t* bytes);
+
+/* The 2D jitter texture (GLUtils::Create2DJitterTexture, GLUtils.cpp:455-497):
+ * size*size uint8 values in [1,255], row-major. */
+int vv_set_jitter(vv_ctx* ctx, const uint8_t* table, int32_t size);
+
+/* ---- the hot path --------------------------------------------------------- */
+
+/* One draw of octree `tree`: the ray cast of GigaVoxelsNoLighting.frag
+ * (main :490-751), then GenerateSelectionMask.frag, ComputeActiveTexels.frag
+ * + GenerateHistoPyramid.frag and CompressNodeUsageList.frag, as run by
+ * GigaVoxelsRenderer::drawVolume / generateNodeUsageSelectionMask /
+ * generateSelectionMaskHistoPyramid / compressNodeUsageList
+ * (GigaVoxelsRenderer.cpp:1584-2135).  Asynchronous on the context stream. */
+int vv_render(vv_ctx* ctx, int32_t tree, const vv_uniforms* u,
+              const vv_frame_out* out);
+
+/* ---- host data model: terrain octree (GigaVoxelsOctTree) ----------------- */
+
+typedef struct vv_octree vv_octree;
+
+/* Synthetic terrain: seeded 2D fBm value-noise heightfield voxelised into a
+ * (8 << depth)^3 volume; colour by 8 equal height bands. */
+typedef struct vv_terrain_desc {
+    uint32_t seed;
+    int32_t depth;             /* leaf level L (OctTreeDepthMinusOne) */
+    int32_t octaves;           /* 4 */
+    float lacunarity;          /* 2.0 */
+    float gain;                /* 0.5 */
+    int32_t base_cells;        /* lattice cells across the volume at octave 0 */
+    int32_t collapse_constant; /* 1: constant nodes are leaves (.gvx trees);
+                                  0: full tree as GigaVoxelsOctTree::build */
+    int32_t threads;           /* host threads for the build (0 = all) */
+} vv_terrain_desc;
+
+typedef struct vv_octree_info {
+    int32_t depth;             /* L */
+    int32_t volume_dim;        /* 8 << L */
+    int64_t node_count;        /* allocated nodes (8 per block) */
+    int32_t pool_dim[3];       /* node-pool grid */
+    int64_t nonconst_count;    /* non-constant nodes (bricks that exist) */
+    int32_t root_is_constant;
+    uint32_t root_word0, root_word1;
+} vv_octree_info;
+
+/* GigaVoxelsOctTree::build (GigaVoxelsOctTree.cpp:1656-1701) for the terrain. */
+int vv_octree_build_terrain(const vv_terrain_desc* desc, vv_octree** out);
+void vv_octree_destroy(vv_octree* tree);
+int vv_octree_get_info(const vv_octree* tree, vv_octree_info* info);
+/* Host mirror of the node pool in reference texture order, no brick resident
+ * (2 * pool_dim product words). */
+int vv_octree_node_words(const vv_octree* tree, uint32_t* words);
+/* Node record for grid position (x,y,z): level (0 = root), mip-level voxel
+ * origin of its brick region, constant flag, parent grid position. */
+typedef struct vv_node_info {
+    int32_t valid;
+    int32_t level;
+    int32_t origin[3];         /* brick origin in mip-level voxels (8*i)   */
+    int32_t is_constant;
+    int32_t has_children;
+    int32_t parent[3];         /* -1 for the root */
+} vv_node_info;
+int vv_octree_node_info(const vv_octree* tree, uint32_t x, uint32_t y,
+                        uint32_t z, vv_node_info* info);
+/* Produce the stored 10^3 bricks of n nodes (given by grid position, 3
+ * uint32 each) in `fmt` into `out` (n * 1000 texels).  This is
+ * Node::copyMipMapToBrick (GigaVoxelsOctTree.cpp:1428-1488) over the mip
+ * pyramid of GenerateMipMaps (:1030-1194). */
+int vv_octree_produce_bricks(const vv_octree* tree, const uint32_t* xyz,
+                             int32_t n, int32_t fmt, void* out);
+/* Dense mip level (RGBA8, x fastest) for checking on small volumes. */
+int vv_octree_mip_level(const vv_octree* tree, int32_t level, uint32_t* out,
+                        size_t out_words);
+/* Column heights of the leaf level (dim*dim int32, x fastest). */
+int vv_octree_heights(const vv_octree* tree, int32_t* out);
+
+/* ---- camera + uniform derivation ---------------------------------------- */
+
+/* vox::Camera essentials (VoxVizCore/Camera.h). */
+typedef struct vv_camera {
+    float position[3];     /* normalized volume space */
+    float look[3];         /* unit */
+    float up[3];           /* unit, orthogonal to look */
+    float fov_y_deg;       /* Camera default 45 (Camera.cpp:36) */
+    float near_dist;
+    int32_t width, height;
+    int32_t frame;         /* Camera::getFrameCount */
+} vv_camera;
+
+/* Derive the draw uniforms exactly as GigaVoxelsRenderer::drawVolume
+ * (GigaVoxelsRenderer.cpp:1630-1816) with the octree and the camera. */
+int vv_compute_uniforms(const vv_octree_info* tree, const vv_camera* cam,
+                        int32_t pool_slots_x, int32_t pool_slots_y,
+                        int32_t pool_slots_z, float lod_scalar,
+                        float alpha_stop, vv_uniforms* out);
+/* Camera::getPixelSize (Camera.cpp:128-196). */
+float vv_camera_pixel_size(const vv_camera* cam);
+/* Seeded jitter texture values in [1,255] (size*size bytes). */
+int vv_make_jitter(uint32_t seed, int32_t size, uint8_t* out);
+
+/* ---- renderer: the plugin frame protocol -------------------------------- */
+
+typedef struct vv_renderer vv_renderer;
+
+typedef struct vv_renderer_desc {
+    int32_t fmt;               /* brick pool format                        */
+    int64_t pool_bytes;        /* brick pool budget (0 = all bricks fit)    */
+    int32_t preload_all;       /* 1: make every brick resident at init      */
+    int32_t request_cap;       /* compacted-list cap (0 = no cap)           */
+    float lod_scalar;          /* 1.0 = one voxel per pixel                 */
+    float alpha_stop;          /* 0.99 in the benchmark configs             */
+    uint32_t jitter_seed;
+    int32_t max_width, max_height;
+    int32_t producer_threads;  /* host brick producers (0 = all cores)      */
+} vv_renderer_desc;
+
+typedef struct vv_renderer_stats {
+    int64_t frame;
+    int64_t requests;          /* compacted entries this frame              */
+    int64_t active_pixels;
+    int64_t bricks_uploaded;   /* this frame                                */
+    int64_t bricks_uploaded_total;
+    int64_t resident_bricks;
+    int64_t evictions_total;
+    int32_t pool_slots;
+} vv_renderer_stats;
+
+/* vox::Renderer lifecycle of the "gv" renderer (VoxVizCore/Renderer.h:20-110,
+ * GigaVoxelsRenderer.cpp).  init: pools + initial bricks. */
+int vv_renderer_create(vv_ctx* ctx, vv_octree* tree, const vv_renderer_desc* d,
+                       vv_renderer** out);
+void vv_renderer_destroy(vv_renderer* r);
+/* draw(): ray cast + selection mask + histopyramid + compaction on device. */
+int vv_renderer_draw(vv_renderer* r, const vv_camera* cam);
+/* postDraw() + update(): read back the compacted page requests, run the
+ * NodeUsageListProcessor / BrickPool::update policy (deterministic LRU),
+ * produce and upload bricks and patch node words. */
+int vv_renderer_update(vv_renderer* r);
+int vv_renderer_get_stats(const vv_renderer* r, vv_renderer_stats* out);
+/* Device pointers of the last frame's buffers (valid until next draw). */
+int vv_renderer_frame_buffers(vv_renderer* r, float** color, uint32_t** usage,
+                              uint32_t** mask, uint32_t** requests,
+                              uint32_t** request_count);
+/* Copy the last frame's colour (H*W*4 floats) to host memory. */
+int vv_renderer_read_color(vv_renderer* r, float* host_rgba);
+/* Host copy of the compacted request list of the last update (n x 4 words). */
+int vv_renderer_last_requests(const vv_renderer* r, uint32_t* out, int32_t cap,
+                              int32_t* n);
+/* Slot of every resident brick: out_xyz[i*3..] node grid position,
+ * out_slot[i]; returns the count in *n. */
+int vv_renderer_residency(const vv_renderer* r, uint32_t* out_xyz,
+                          uint32_t* out_slot, int64_t cap, int64_t* n);
+/* Uniforms of the last draw. */
+int vv_renderer_last_uniforms(const vv_renderer* r, vv_uniforms* out);
+vv_ctx* vv_renderer_ctx(vv_renderer* r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VOXVIZ_B200_H */

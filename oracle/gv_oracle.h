@@ -1,0 +1,32 @@
+/* gv_oracle.h - C interface of the CPU oracle (test infrastructure only).
+ * Loaded by tests/, the smoke check and the cpu_baseline leg of bench.py. */
+#ifndef GV_ORACLE_H
+#define GV_ORACLE_H
+#include <stdint.h>
+#include "../include/voxviz_b200.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_scene {
+    const uint32_t* nodes;  /* node pool, reference texture order, 2 words/texel */
+    int32_t node_dim[3];
+    const void* bricks;     /* brick pool, slot-major brick-linear texels */
+    int32_t fmt;            /* vv_fmt */
+    int32_t slots[3];
+    const uint8_t* jitter;  /* jitter_tex_size^2 values */
+} oracle_scene;
+
+/* Rows [row0,row1) of the ray cast.  precision 32: float colour (4 floats per
+ * pixel), 64: double colour.  usage: 12 words per pixel (may be NULL). */
+int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
+                   void* color, uint32_t* usage, int threads, int32_t* status);
+int oracle_max_iterations(const vv_uniforms* u);
+int oracle_select(const uint32_t* usage, int w, int h, uint32_t* mask);
+int oracle_compress(const uint32_t* usage, const uint32_t* mask, int w, int h, int max_push, int cap,
+                    uint32_t* out, uint32_t* total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,127 @@
+"""ctypes binding of the CPU oracle (liboracle_gv.so).  TEST INFRASTRUCTURE.
+
+Only tests/, the smoke check and the cpu_baseline leg of bench.py use this
+module; the product never loads it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "build" / "liboracle_gv.so"
+
+
+class OracleScene(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_void_p),
+        ("node_dim", C.c_int32 * 3),
+        ("bricks", C.c_void_p),
+        ("fmt", C.c_int32),
+        ("slots", C.c_int32 * 3),
+        ("jitter", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (no-op when up to date)."""
+    r = subprocess.run(["make", "-s", "-C", str(HERE)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB.exists():
+        build()
+    lib = C.CDLL(str(LIB))
+    from voxviz_b200._native import Uniforms
+    lib.oracle_raycast.restype = C.c_int
+    lib.oracle_raycast.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_int, C.c_int, C.c_int,
+                                   C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]
+    lib.oracle_max_iterations.restype = C.c_int
+    lib.oracle_max_iterations.argtypes = [C.POINTER(Uniforms)]
+    lib.oracle_select.restype = C.c_int
+    lib.oracle_select.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    lib.oracle_compress.restype = C.c_int
+    lib.oracle_compress.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                    C.POINTER(C.c_uint32)]
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+class Scene:
+    """Node words (dz,dy,dx,2), brick pool (slots, bytes), format and jitter."""
+
+    def __init__(self, words: np.ndarray, pool: np.ndarray, slots, fmt: int, jitter: np.ndarray):
+        self.words = np.ascontiguousarray(words, dtype=np.uint32)
+        self.pool = np.ascontiguousarray(pool)
+        self.jitter = np.ascontiguousarray(jitter, dtype=np.uint8)
+        self.s = OracleScene()
+        self.s.nodes = _p(self.words)
+        dz, dy, dx = self.words.shape[:3]
+        self.s.node_dim[:] = [dx, dy, dz]
+        self.s.bricks = _p(self.pool)
+        self.s.fmt = int(fmt)
+        self.s.slots[:] = [int(v) for v in slots]
+        self.s.jitter = _p(self.jitter)
+
+
+def raycast(u, scene: Scene, precision: int = 32, rows=None, threads: int = 0, want_usage: bool = True):
+    """Returns (color (H,W,4) float32/float64, usage (H,W,12) uint32, status)."""
+    lib = load()
+    W, H = u.width, u.height
+    r0, r1 = (0, H) if rows is None else rows
+    color = np.zeros((H, W, 4), dtype=np.float64 if precision == 64 else np.float32)
+    usage = np.zeros((H, W, 12), dtype=np.uint32) if want_usage else None
+    st = C.c_int32(0)
+    rc = lib.oracle_raycast(C.byref(u), C.byref(scene.s), precision, r0, r1, _p(color),
+                            _p(usage) if usage is not None else None, threads, C.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"oracle_raycast failed: {rc}")
+    return color, usage, st.value
+
+
+def select(usage: np.ndarray) -> np.ndarray:
+    lib = load()
+    H, W = usage.shape[:2]
+    u = np.ascontiguousarray(usage, dtype=np.uint32)
+    mask = np.zeros((H, W), dtype=np.uint32)
+    lib.oracle_select(_p(u), W, H, _p(mask))
+    return mask
+
+
+def compress(usage: np.ndarray, mask: np.ndarray, max_push: int, cap: int):
+    """Returns (list (n,4) uint32 in key order, total active pixels)."""
+    lib = load()
+    H, W = usage.shape[:2]
+    u = np.ascontiguousarray(usage, dtype=np.uint32)
+    m = np.ascontiguousarray(mask, dtype=np.uint32)
+    out = np.zeros((max(cap, 1), 4), dtype=np.uint32)
+    tot = C.c_uint32(0)
+    lib.oracle_compress(_p(u), _p(m), W, H, max_push, cap, _p(out), C.byref(tot))
+    n = min(tot.value, cap)
+    return out[:n].copy(), tot.value
+
+
+def max_iterations(u) -> int:
+    return load().oracle_max_iterations(C.byref(u))
+
+
+def cpu_count() -> int:
+    return len(os.sched_getaffinity(0))

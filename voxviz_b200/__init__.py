@@ -1,0 +1,339 @@
+"""voxviz_b200 - B200-native GigaVoxels sparse-octree ray caster.
+
+Python binding over the C ABI of ``include/voxviz_b200.h``.  Every call goes
+through ``libvoxviz_b200.so``; there is no Python or CPU fallback for the hot
+path (a missing library raises).
+
+The objects mirror the reference's host API:
+
+* :class:`Octree` - ``gv::GigaVoxelsOctTree`` built from a synthetic terrain
+  (VoxViz/GigaVoxels/GigaVoxelsOctTree.h:34-516)
+* :class:`Context` - device pools and the draw entry point
+  (node pool: GigaVoxelsOctTreeNodePool.h, brick pool: GigaVoxelsBrickPool.h)
+* :class:`Renderer` - the ``"gv"`` ``vox::Renderer`` frame protocol
+  (VoxViz/VoxVizCore/Renderer.h:20-110, GigaVoxelsRenderer.cpp)
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _native as N
+from ._native import (FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_FP16, VV_FMT_FP32, VV_FMT_RGBA8,  # noqa: F401
+                      VV_PASS_ALL, VV_PASS_COMPACT, VV_PASS_RAYCAST, VV_PASS_SELECT, Camera, FrameOut,
+                      NodePatch, OctreeInfo, Uniforms, VVError)
+
+__all__ = ["Octree", "Context", "Renderer", "make_camera", "look_at", "compute_uniforms", "make_jitter",
+           "pixel_size", "lib", "VVError", "Uniforms", "Camera", "FMT_NAMES", "TEXEL_BYTES"]
+
+
+def lib() -> C.CDLL:
+    return N.load()
+
+
+def _check(rc: int, ctx=None, what: str = "") -> None:
+    if rc != N.VV_OK:
+        L = lib()
+        msg = L.vv_last_error(ctx).decode() if ctx is not None else L.vv_last_error(None).decode()
+        base = L.vv_status_string(rc).decode()
+        raise VVError(rc, f"{what}: {base}" + (f" ({msg})" if msg else ""))
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def fmt_code(fmt) -> int:
+    return FMT_NAMES[fmt] if isinstance(fmt, str) else int(fmt)
+
+
+# ---------------------------------------------------------------- camera ---
+
+def look_at(eye: Sequence[float], target: Sequence[float], world_up=(0.0, 0.0, 1.0)):
+    """Unit look and up vectors for a camera at eye looking at target (Z up,
+    as vox::Camera's m_worldUp, Camera.cpp:22)."""
+    e = np.asarray(eye, dtype=np.float64)
+    look = np.asarray(target, dtype=np.float64) - e
+    look /= np.linalg.norm(look)
+    wu = np.asarray(world_up, dtype=np.float64)
+    left = np.cross(wu, look)
+    if np.linalg.norm(left) < 1e-9:
+        left = np.cross(np.array([0.0, 1.0, 0.0]), look)
+    left /= np.linalg.norm(left)
+    up = np.cross(look, left)
+    up /= np.linalg.norm(up)
+    return look, up
+
+
+def make_camera(position, look, up, width: int, height: int, frame: int = 0, fov_y_deg: float = 45.0,
+                near: float = 1e-3) -> Camera:
+    c = Camera()
+    c.position[:] = [float(v) for v in position]
+    c.look[:] = [float(v) for v in look]
+    c.up[:] = [float(v) for v in up]
+    c.fov_y_deg = fov_y_deg
+    c.near_dist = near
+    c.width = width
+    c.height = height
+    c.frame = frame
+    return c
+
+
+def pixel_size(cam: Camera) -> float:
+    return float(lib().vv_camera_pixel_size(C.byref(cam)))
+
+
+def make_jitter(seed: int, size: int = 32) -> np.ndarray:
+    out = np.empty(size * size, dtype=np.uint8)
+    _check(lib().vv_make_jitter(seed, size, _ptr(out)), what="make_jitter")
+    return out
+
+
+def compute_uniforms(info: OctreeInfo, cam: Camera, slots: Sequence[int], lod_scalar: float = 1.0,
+                     alpha_stop: float = 0.99) -> Uniforms:
+    u = Uniforms()
+    _check(lib().vv_compute_uniforms(C.byref(info), C.byref(cam), int(slots[0]), int(slots[1]), int(slots[2]),
+                                     lod_scalar, alpha_stop, C.byref(u)), what="compute_uniforms")
+    return u
+
+
+# ---------------------------------------------------------------- octree ---
+
+class Octree:
+    """A terrain octree (host data model, ``gv::GigaVoxelsOctTree``)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def terrain(cls, seed: int = 1, depth: int = 5, collapse: bool = True, octaves: int = 4,
+                lacunarity: float = 2.0, gain: float = 0.5, base_cells: int = 4, threads: int = 0) -> "Octree":
+        d = N.TerrainDesc(seed=seed, depth=depth, octaves=octaves, lacunarity=lacunarity, gain=gain,
+                          base_cells=base_cells, collapse_constant=1 if collapse else 0, threads=threads)
+        h = C.c_void_p()
+        _check(lib().vv_octree_build_terrain(C.byref(d), C.byref(h)), what="octree build")
+        return cls(h.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vv_octree_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def info(self) -> OctreeInfo:
+        i = OctreeInfo()
+        _check(lib().vv_octree_get_info(self._h, C.byref(i)), what="octree info")
+        return i
+
+    def node_words(self) -> np.ndarray:
+        """Node pool in reference texture order: shape (dz, dy, dx, 2) uint32."""
+        i = self.info
+        dx, dy, dz = i.pool_dim
+        out = np.zeros((dz, dy, dx, 2), dtype=np.uint32)
+        _check(lib().vv_octree_node_words(self._h, _ptr(out)), what="node words")
+        return out
+
+    def node_info(self, x: int, y: int, z: int) -> N.NodeInfo:
+        ni = N.NodeInfo()
+        _check(lib().vv_octree_node_info(self._h, x, y, z, C.byref(ni)), what="node info")
+        return ni
+
+    def produce_bricks(self, xyz: np.ndarray, fmt="rgba8") -> np.ndarray:
+        f = fmt_code(fmt)
+        xyz = np.ascontiguousarray(xyz, dtype=np.uint32).reshape(-1, 3)
+        n = xyz.shape[0]
+        out = np.zeros((n, 1000 * TEXEL_BYTES[f]), dtype=np.uint8)
+        _check(lib().vv_octree_produce_bricks(self._h, _ptr(xyz), n, f, _ptr(out)), what="produce bricks")
+        return out
+
+    def mip_level(self, level: int) -> np.ndarray:
+        d = (8 << self.info.depth) >> level
+        out = np.zeros((d, d, d), dtype=np.uint32)
+        _check(lib().vv_octree_mip_level(self._h, level, _ptr(out), out.size), what="mip level")
+        return out
+
+    def heights(self) -> np.ndarray:
+        d = 8 << self.info.depth
+        out = np.zeros((d, d), dtype=np.int32)
+        _check(lib().vv_octree_heights(self._h, _ptr(out)), what="heights")
+        return out
+
+
+# --------------------------------------------------------------- context ---
+
+class Context:
+    """A device context (``vv_ctx``): node pools, the brick pool, the draw."""
+
+    def __init__(self, device: int = 0):
+        p = N.Params(device=device, flags=0)
+        h = C.c_void_p()
+        _check(lib().vv_ctx_create(C.byref(p), C.byref(h)), what="ctx create")
+        self._h = h
+        self.fmt = VV_FMT_RGBA8
+        self.slots = (0, 0, 0)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vv_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _ck(self, rc: int, what: str) -> None:
+        _check(rc, self._h, what)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._ck(lib().vv_ctx_set_stream(self._h, C.c_void_p(stream_ptr)), "set stream")
+
+    def synchronize(self) -> None:
+        self._ck(lib().vv_ctx_synchronize(self._h), "synchronize")
+
+    def device_status(self, clear: bool = True) -> int:
+        s = C.c_int32()
+        self._ck(lib().vv_ctx_device_status(self._h, C.byref(s), 1 if clear else 0), "device status")
+        return s.value
+
+    def upload_nodes(self, words: np.ndarray, tree: int = 0) -> None:
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        dz, dy, dx = w.shape[:3]
+        self._ck(lib().vv_nodepool_upload(self._h, tree, _ptr(w), dx, dy, dz), "node upload")
+        self._node_dims = (dx, dy, dz)
+
+    def download_nodes(self, tree: int = 0) -> np.ndarray:
+        dx, dy, dz = self._node_dims
+        out = np.zeros((dz, dy, dx, 2), dtype=np.uint32)
+        self._ck(lib().vv_nodepool_download(self._h, tree, _ptr(out)), "node download")
+        return out
+
+    def patch_nodes(self, patches: np.ndarray, tree: int = 0) -> None:
+        """patches: (n, 5) uint32 rows x, y, z, word0, word1."""
+        p = np.ascontiguousarray(patches, dtype=np.uint32).reshape(-1, 5)
+        self._ck(lib().vv_nodepool_patch(self._h, tree, _ptr(p), p.shape[0]), "node patch")
+
+    def create_brickpool(self, slots: Sequence[int], fmt="rgba8") -> None:
+        f = fmt_code(fmt)
+        self._ck(lib().vv_brickpool_create(self._h, int(slots[0]), int(slots[1]), int(slots[2]), f), "brick pool")
+        self.fmt = f
+        self.slots = tuple(int(s) for s in slots)
+
+    def upload_bricks(self, slot_ids: np.ndarray, texels: np.ndarray) -> None:
+        s = np.ascontiguousarray(slot_ids, dtype=np.uint32)
+        t = np.ascontiguousarray(texels)
+        assert t.nbytes == s.size * 1000 * TEXEL_BYTES[self.fmt]
+        self._ck(lib().vv_upload_bricks(self._h, _ptr(s), s.size, _ptr(t)), "brick upload")
+
+    def download_bricks(self) -> np.ndarray:
+        n = self.slots[0] * self.slots[1] * self.slots[2]
+        out = np.zeros((n, 1000 * TEXEL_BYTES[self.fmt]), dtype=np.uint8)
+        self._ck(lib().vv_brickpool_download(self._h, _ptr(out)), "brick download")
+        return out
+
+    def set_jitter(self, table: np.ndarray) -> None:
+        t = np.ascontiguousarray(table, dtype=np.uint8)
+        size = int(round(np.sqrt(t.size)))
+        self._ck(lib().vv_set_jitter(self._h, _ptr(t), size), "jitter")
+
+    def render(self, u: Uniforms, color=0, usage=0, mask=0, requests=0, request_count=0, request_cap=0,
+               compress_max_push=4, passes=VV_PASS_ALL, tree: int = 0) -> None:
+        """One draw; every buffer argument is a device pointer (int) or 0."""
+        o = FrameOut(color=color or None, usage=usage or None, mask=mask or None, requests=requests or None,
+                     request_count=request_count or None, request_cap=request_cap,
+                     compress_max_push=compress_max_push, passes=passes)
+        self._ck(lib().vv_render(self._h, tree, C.byref(u), C.byref(o)), "render")
+
+
+# -------------------------------------------------------------- renderer ---
+
+class Renderer:
+    """The ``"gv"`` renderer plugin: init, draw, update (postDraw + update)."""
+
+    def __init__(self, ctx: Context, octree: Octree, fmt="rgba8", pool_bytes: int = 0, preload_all: bool = True,
+                 request_cap: int = 0, lod_scalar: float = 1.0, alpha_stop: float = 0.99, jitter_seed: int = 7,
+                 producer_threads: int = 0):
+        d = N.RendererDesc(fmt=fmt_code(fmt), pool_bytes=pool_bytes, preload_all=1 if preload_all else 0,
+                           request_cap=request_cap, lod_scalar=lod_scalar, alpha_stop=alpha_stop,
+                           jitter_seed=jitter_seed, max_width=0, max_height=0, producer_threads=producer_threads)
+        h = C.c_void_p()
+        _check(lib().vv_renderer_create(ctx.handle, octree.handle, C.byref(d), C.byref(h)), ctx.handle,
+               "renderer create")
+        self._h = h
+        self.ctx = ctx
+        self.octree = octree
+        self.fmt = fmt_code(fmt)
+
+    def close(self) -> None:
+        if self._h:
+            lib().vv_renderer_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc: int, what: str) -> None:
+        _check(rc, self.ctx.handle, what)
+
+    def draw(self, cam: Camera) -> None:
+        self._ck(lib().vv_renderer_draw(self._h, C.byref(cam)), "draw")
+
+    def update(self) -> None:
+        self._ck(lib().vv_renderer_update(self._h), "update")
+
+    def stats(self) -> dict:
+        s = N.RendererStats()
+        self._ck(lib().vv_renderer_get_stats(self._h, C.byref(s)), "stats")
+        return {k: getattr(s, k) for k, _ in N.RendererStats._fields_}
+
+    def frame_buffers(self) -> dict:
+        ptrs = [C.c_void_p() for _ in range(5)]
+        self._ck(lib().vv_renderer_frame_buffers(self._h, *[C.byref(p) for p in ptrs]), "frame buffers")
+        return dict(zip(["color", "usage", "mask", "requests", "request_count"], [p.value for p in ptrs]))
+
+    def read_color(self) -> np.ndarray:
+        u = self.last_uniforms()
+        out = np.zeros((u.height, u.width, 4), dtype=np.float32)
+        self._ck(lib().vv_renderer_read_color(self._h, _ptr(out)), "read color")
+        return out
+
+    def last_requests(self) -> np.ndarray:
+        n = C.c_int32()
+        self._ck(lib().vv_renderer_last_requests(self._h, None, 0, C.byref(n)), "requests")
+        out = np.zeros((n.value, 4), dtype=np.uint32)
+        self._ck(lib().vv_renderer_last_requests(self._h, _ptr(out), n.value, C.byref(n)), "requests")
+        return out
+
+    def residency(self):
+        n = C.c_int64()
+        self._ck(lib().vv_renderer_residency(self._h, None, None, 0, C.byref(n)), "residency")
+        xyz = np.zeros((n.value, 3), dtype=np.uint32)
+        slot = np.zeros(n.value, dtype=np.uint32)
+        self._ck(lib().vv_renderer_residency(self._h, _ptr(xyz), _ptr(slot), n.value, C.byref(n)), "residency")
+        return xyz, slot
+
+    def last_uniforms(self) -> Uniforms:
+        u = Uniforms()
+        self._ck(lib().vv_renderer_last_uniforms(self._h, C.byref(u)), "uniforms")
+        return u

@@ -1,0 +1,234 @@
+// capi.cpp - C ABI of the host data model (octree, camera, renderer).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "ctx.h"
+#include "octree.h"
+#include "renderer.h"
+
+struct vv_octree {
+    std::shared_ptr<const vv::TerrainVolume> volume;
+    std::unique_ptr<vv::GigaVoxelsOctTree> tree;
+};
+
+struct vv_renderer {
+    std::unique_ptr<vv::GigaVoxelsRenderer> impl;
+    vv_ctx* ctx = nullptr;
+};
+
+extern "C" {
+
+int vv_octree_build_terrain(const vv_terrain_desc* d, vv_octree** out) {
+    if (!d || !out) return VV_ERR_ARG;
+    *out = nullptr;
+    if (d->depth < 0 || d->depth > 10 || d->octaves < 1 || d->base_cells < 1) return VV_ERR_ARG;
+    try {
+        vv::TerrainParams p;
+        p.seed = d->seed;
+        p.depth = d->depth;
+        p.octaves = d->octaves;
+        p.lacunarity = d->lacunarity;
+        p.gain = d->gain;
+        p.base_cells = d->base_cells;
+        p.threads = d->threads;
+        auto o = std::make_unique<vv_octree>();
+        o->volume = std::make_shared<vv::TerrainVolume>(p);
+        o->tree = vv::GigaVoxelsOctTree::build(o->volume, d->collapse_constant != 0);
+        *out = o.release();
+        return VV_OK;
+    } catch (const std::bad_alloc&) {
+        return VV_ERR_OOM;
+    } catch (const std::exception&) {
+        return VV_ERR_ARG;
+    }
+}
+
+void vv_octree_destroy(vv_octree* t) { delete t; }
+
+int vv_octree_get_info(const vv_octree* t, vv_octree_info* info) {
+    if (!t || !info) return VV_ERR_ARG;
+    std::memset(info, 0, sizeof(*info));
+    info->depth = t->tree->depth();
+    info->volume_dim = 8 << t->tree->depth();
+    info->node_count = (int64_t)t->tree->node_count();
+    for (int a = 0; a < 3; ++a) info->pool_dim[a] = t->tree->pool_dim()[a];
+    info->nonconst_count = (int64_t)t->tree->nonconst_count();
+    info->root_is_constant = t->tree->is_constant(0) ? 1 : 0;
+    info->root_word0 = t->tree->word0(0);
+    info->root_word1 = t->tree->word1(0);
+    return VV_OK;
+}
+
+int vv_octree_node_words(const vv_octree* t, uint32_t* words) {
+    if (!t || !words) return VV_ERR_ARG;
+    t->tree->words_grid(words);
+    return VV_OK;
+}
+
+int vv_octree_node_info(const vv_octree* t, uint32_t x, uint32_t y, uint32_t z, vv_node_info* info) {
+    if (!t || !info) return VV_ERR_ARG;
+    std::memset(info, 0, sizeof(*info));
+    const uint32_t n = t->tree->index_of(x, y, z);
+    if (n == vv::kNoParent || t->tree->level(n) < 0) return VV_OK;
+    info->valid = 1;
+    info->level = t->tree->level(n);
+    int i, j, k;
+    t->tree->origin(n, i, j, k);
+    info->origin[0] = 8 * i;
+    info->origin[1] = 8 * j;
+    info->origin[2] = 8 * k;
+    info->is_constant = t->tree->is_constant(n) ? 1 : 0;
+    info->has_children = t->tree->has_children(n) ? 1 : 0;
+    const uint32_t p = t->tree->parent(n);
+    if (p == vv::kNoParent) {
+        info->parent[0] = info->parent[1] = info->parent[2] = -1;
+    } else {
+        uint32_t px, py, pz;
+        t->tree->grid_of(p, px, py, pz);
+        info->parent[0] = (int32_t)px;
+        info->parent[1] = (int32_t)py;
+        info->parent[2] = (int32_t)pz;
+    }
+    return VV_OK;
+}
+
+int vv_octree_produce_bricks(const vv_octree* t, const uint32_t* xyz, int32_t n, int32_t fmt, void* out) {
+    if (!t || n < 0 || (n > 0 && (!xyz || !out))) return VV_ERR_ARG;
+    const size_t tb = vv::texel_bytes(fmt);
+    if (!tb) return VV_ERR_ARG;
+    for (int32_t i = 0; i < n; ++i) {
+        const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        if (idx == vv::kNoParent || t->tree->level(idx) < 0) return VV_ERR_ARG;
+    }
+    unsigned char* o = (unsigned char*)out;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int32_t i = 0; i < n; ++i) {
+        const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        t->tree->produce_brick(idx, fmt, o + (size_t)i * VV_BRICK_TEXELS * tb);
+    }
+    return VV_OK;
+}
+
+int vv_octree_mip_level(const vv_octree* t, int32_t level, uint32_t* out, size_t out_words) {
+    if (!t || !out || level < 0 || level > t->tree->depth()) return VV_ERR_ARG;
+    const vv::TerrainVolume& v = t->tree->volume();
+    const int d = v.mip(level).dim;
+    if (out_words < (size_t)d * d * d) return VV_ERR_ARG;
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < d; ++z)
+        for (int y = 0; y < d; ++y)
+            for (int x = 0; x < d; ++x) out[((size_t)z * d + y) * d + x] = v.voxel(level, x, y, z);
+    return VV_OK;
+}
+
+int vv_octree_heights(const vv_octree* t, int32_t* out) {
+    if (!t || !out) return VV_ERR_ARG;
+    const auto& h = t->tree->volume().heights();
+    std::memcpy(out, h.data(), h.size() * sizeof(int32_t));
+    return VV_OK;
+}
+
+int vv_compute_uniforms(const vv_octree_info* tree, const vv_camera* cam, int32_t sx, int32_t sy, int32_t sz,
+                        float lod_scalar, float alpha_stop, vv_uniforms* out) {
+    if (!tree || !cam || !out || cam->width <= 0 || cam->height <= 0) return VV_ERR_ARG;
+    const int slots[3] = {sx, sy, sz};
+    vv::compute_uniforms(tree->depth, tree->root_is_constant != 0, *cam, slots, lod_scalar, alpha_stop, *out);
+    return VV_OK;
+}
+
+float vv_camera_pixel_size(const vv_camera* cam) { return cam ? vv::camera_pixel_size(*cam) : 0.0f; }
+
+int vv_make_jitter(uint32_t seed, int32_t size, uint8_t* out) {
+    if (!out || size <= 0 || size > 256) return VV_ERR_ARG;
+    vv::make_jitter(seed, size, out);
+    return VV_OK;
+}
+
+int vv_renderer_create(vv_ctx* ctx, vv_octree* tree, const vv_renderer_desc* d, vv_renderer** out) {
+    if (!ctx || !tree || !d || !out) return VV_ERR_ARG;
+    *out = nullptr;
+    try {
+        auto r = std::make_unique<vv_renderer>();
+        r->ctx = ctx;
+        r->impl = std::make_unique<vv::GigaVoxelsRenderer>(ctx, tree, tree->tree.get(), *d);
+        int rc = r->impl->init();
+        if (rc) return rc;
+        *out = r.release();
+        return VV_OK;
+    } catch (const std::bad_alloc&) {
+        return VV_ERR_OOM;
+    }
+}
+
+void vv_renderer_destroy(vv_renderer* r) { delete r; }
+
+int vv_renderer_draw(vv_renderer* r, const vv_camera* cam) {
+    if (!r || !cam) return VV_ERR_ARG;
+    return r->impl->draw(*cam);
+}
+
+int vv_renderer_update(vv_renderer* r) {
+    if (!r) return VV_ERR_ARG;
+    return r->impl->update();
+}
+
+int vv_renderer_get_stats(const vv_renderer* r, vv_renderer_stats* out) {
+    if (!r || !out) return VV_ERR_ARG;
+    r->impl->stats(*out);
+    return VV_OK;
+}
+
+int vv_renderer_frame_buffers(vv_renderer* r, float** color, uint32_t** usage, uint32_t** mask, uint32_t** requests,
+                              uint32_t** request_count) {
+    if (!r) return VV_ERR_ARG;
+    if (color) *color = r->impl->d_color;
+    if (usage) *usage = r->impl->d_usage;
+    if (mask) *mask = r->impl->d_mask;
+    if (requests) *requests = r->impl->d_requests;
+    if (request_count) *request_count = r->impl->d_count;
+    return VV_OK;
+}
+
+int vv_renderer_read_color(vv_renderer* r, float* host_rgba) {
+    if (!r || !host_rgba || !r->impl->d_color) return VV_ERR_ARG;
+    const size_t bytes = (size_t)r->impl->width * r->impl->height * 16;
+    if (cudaMemcpyAsync(host_rgba, r->impl->d_color, bytes, cudaMemcpyDeviceToHost, r->ctx->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(r->ctx->stream) != cudaSuccess) return VV_ERR_CUDA;
+    return VV_OK;
+}
+
+int vv_renderer_last_requests(const vv_renderer* r, uint32_t* out, int32_t cap, int32_t* n) {
+    if (!r || !n) return VV_ERR_ARG;
+    const auto& q = r->impl->last_requests();
+    const int32_t cnt = (int32_t)(q.size() / 4);
+    *n = cnt;
+    if (out) std::memcpy(out, q.data(), (size_t)std::min(cnt, cap) * 16);
+    return VV_OK;
+}
+
+int vv_renderer_residency(const vv_renderer* r, uint32_t* out_xyz, uint32_t* out_slot, int64_t cap, int64_t* n) {
+    if (!r || !n) return VV_ERR_ARG;
+    std::vector<uint32_t> xyz, slot;
+    r->impl->residency(xyz, slot);
+    *n = (int64_t)slot.size();
+    const size_t m = (size_t)std::min<int64_t>(cap, (int64_t)slot.size());
+    if (out_xyz) std::memcpy(out_xyz, xyz.data(), m * 3 * 4);
+    if (out_slot) std::memcpy(out_slot, slot.data(), m * 4);
+    return VV_OK;
+}
+
+int vv_renderer_last_uniforms(const vv_renderer* r, vv_uniforms* out) {
+    if (!r || !out) return VV_ERR_ARG;
+    *out = r->impl->last_uniforms();
+    return VV_OK;
+}
+
+vv_ctx* vv_renderer_ctx(vv_renderer* r) { return r ? r->ctx : nullptr; }
+
+}  // extern "C"

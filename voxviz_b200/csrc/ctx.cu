@@ -1,0 +1,419 @@
+// ctx.cu - device context, pools and the render entry point of the C ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ctx.h"
+#include "kernels.cuh"
+
+using namespace vv;
+
+namespace {
+
+thread_local std::string g_global_error;
+
+int fail(vv_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_global_error = msg;
+    return code;
+}
+
+int cuda_fail(vv_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, VV_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define VV_CUDA(c, expr)                                  \
+    do {                                                  \
+        cudaError_t e_ = (expr);                          \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #expr); \
+    } while (0)
+
+size_t fmt_texel_bytes(int fmt) {
+    switch (fmt) {
+        case VV_FMT_RGBA8: return 4;
+        case VV_FMT_FP16: return 8;
+        case VV_FMT_BF16: return 8;
+        case VV_FMT_FP32: return 16;
+        default: return 0;
+    }
+}
+
+// Grow a device buffer to at least `bytes`.
+int ensure(vv_ctx* c, void** ptr, size_t* cap, size_t bytes, const char* what) {
+    if (*cap >= bytes && *ptr) return VV_OK;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    size_t want = std::max(bytes, (size_t)256);
+    cudaError_t e = cudaMalloc(ptr, want);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return fail(c, VV_ERR_OOM, std::string("cudaMalloc ") + what + ": " + cudaGetErrorString(e));
+    }
+    *cap = want;
+    return VV_OK;
+}
+
+int ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes) {
+    if (*cap >= bytes && *ptr) return VV_OK;
+    if (*ptr) cudaFreeHost(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    size_t want = std::max(bytes, (size_t)4096);
+    cudaError_t e = cudaMallocHost(ptr, want);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return fail(c, VV_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+    }
+    *cap = want;
+    return VV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vv_abi_version(void) { return VV_ABI_VERSION; }
+
+const char* vv_status_string(int s) {
+    switch (s) {
+        case VV_OK: return "ok";
+        case VV_ERR_ARG: return "invalid argument";
+        case VV_ERR_OOM: return "out of memory";
+        case VV_ERR_CUDA: return "CUDA error";
+        case VV_ERR_TIMEOUT: return "device loop bound reached";
+        case VV_ERR_BOUNDS: return "device index out of bounds";
+        case VV_ERR_STATE: return "call out of order";
+        case VV_ERR_NODEV: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int vv_ctx_create(const vv_params* params, vv_ctx** out) {
+    if (!out) return fail(nullptr, VV_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return fail(nullptr, VV_ERR_NODEV, "no CUDA device available");
+    int dev = params ? params->device : 0;
+    if (dev < 0 || dev >= n) return fail(nullptr, VV_ERR_ARG, "device ordinal out of range");
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return fail(nullptr, VV_ERR_CUDA, cudaGetErrorString(e));
+    vv_ctx* c = new vv_ctx();
+    c->device = dev;
+    e = cudaMalloc(&c->d_status, sizeof(int));
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(nullptr, VV_ERR_OOM, "cudaMalloc status word");
+    }
+    cudaMemset(c->d_status, 0, sizeof(int));
+    // default jitter: constant 128 (1/2 step) until the caller sets a table
+    std::vector<uint8_t> jit(32 * 32, 128);
+    if (cudaMalloc(&c->d_jitter, jit.size()) != cudaSuccess) {
+        cudaFree(c->d_status);
+        delete c;
+        return fail(nullptr, VV_ERR_OOM, "cudaMalloc jitter");
+    }
+    cudaMemcpy(c->d_jitter, jit.data(), jit.size(), cudaMemcpyHostToDevice);
+    c->jitter_size = 32;
+    *out = c;
+    return VV_OK;
+}
+
+int vv_ctx_destroy(vv_ctx* c) {
+    if (!c) return VV_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto& t : c->trees)
+        if (t.nodes) cudaFree(t.nodes);
+    if (c->bricks) cudaFree(c->bricks);
+    void* bufs[] = {c->d_status, c->d_jitter, c->d_usage, c->d_mask, c->d_counts, c->d_offsets,
+                    c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    delete c;
+    return VV_OK;
+}
+
+const char* vv_last_error(const vv_ctx* c) { return c ? c->err.c_str() : g_global_error.c_str(); }
+
+int vv_ctx_set_stream(vv_ctx* c, void* s) {
+    if (!c) return VV_ERR_ARG;
+    c->stream = (cudaStream_t)s;
+    return VV_OK;
+}
+
+int vv_ctx_synchronize(vv_ctx* c) {
+    if (!c) return VV_ERR_ARG;
+    cudaSetDevice(c->device);
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_ctx_device_status(vv_ctx* c, int32_t* status, int32_t clear) {
+    if (!c || !status) return VV_ERR_ARG;
+    cudaSetDevice(c->device);
+    int v = 0;
+    VV_CUDA(c, cudaMemcpyAsync(&v, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    *status = v;
+    if (clear) VV_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    return VV_OK;
+}
+
+int vv_nodepool_upload(vv_ctx* c, int32_t tree, const uint32_t* words, int32_t dx, int32_t dy, int32_t dz) {
+    if (!c || !words || tree < 0 || tree >= VV_MAX_TREES) return fail(c, VV_ERR_ARG, "bad node pool arguments");
+    if (dx <= 0 || dy <= 0 || dz <= 0 || (dx & 1) || (dy & 1) || (dz & 1) || dx > 1024 || dy > 1024 || dz > 1024)
+        return fail(c, VV_ERR_ARG, "node pool dims must be even and <= 1024");
+    cudaSetDevice(c->device);
+    DeviceTree& t = c->trees[tree];
+    const size_t cells = (size_t)dx * dy * dz;
+    if (t.nodes && t.cells != cells) {
+        cudaFree(t.nodes);
+        t.nodes = nullptr;
+    }
+    if (!t.nodes) {
+        cudaError_t e = cudaMalloc(&t.nodes, cells * sizeof(uint2));
+        if (e != cudaSuccess) {
+            t.nodes = nullptr;
+            return fail(c, VV_ERR_OOM, "cudaMalloc node pool");
+        }
+    }
+    t.cells = cells;
+    t.dim[0] = dx;
+    t.dim[1] = dy;
+    t.dim[2] = dz;
+    int rc = ensure(c, (void**)&c->d_grid_words, &c->grid_words_cap, cells * sizeof(uint2), "node staging");
+    if (rc) return rc;
+    VV_CUDA(c, cudaMemcpyAsync(c->d_grid_words, words, cells * sizeof(uint2), cudaMemcpyHostToDevice, c->stream));
+    VV_CUDA(c, launch_node_upload(c->d_grid_words, t.nodes, t.dim, c->stream));
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_nodepool_patch(vv_ctx* c, int32_t tree, const vv_node_patch* patches, int32_t n) {
+    if (!c || tree < 0 || tree >= VV_MAX_TREES || n < 0 || (n > 0 && !patches))
+        return fail(c, VV_ERR_ARG, "bad patch arguments");
+    DeviceTree& t = c->trees[tree];
+    if (!t.nodes) return fail(c, VV_ERR_STATE, "node pool not uploaded");
+    if (n == 0) return VV_OK;
+    cudaSetDevice(c->device);
+    const size_t bytes = (size_t)n * sizeof(vv_node_patch);
+    int rc = ensure(c, (void**)&c->d_patches, &c->patches_cap, bytes, "patch staging");
+    if (rc) return rc;
+    rc = ensure_host(c, &c->h_stage, &c->h_stage_cap, bytes);
+    if (rc) return rc;
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));  // staging buffer reuse
+    std::memcpy(c->h_stage, patches, bytes);
+    VV_CUDA(c, cudaMemcpyAsync(c->d_patches, c->h_stage, bytes, cudaMemcpyHostToDevice, c->stream));
+    VV_CUDA(c, launch_node_patch(c->d_patches, n, t.nodes, t.dim, c->d_status, c->stream));
+    return VV_OK;
+}
+
+int vv_nodepool_download(vv_ctx* c, int32_t tree, uint32_t* words) {
+    if (!c || !words || tree < 0 || tree >= VV_MAX_TREES) return fail(c, VV_ERR_ARG, "bad arguments");
+    DeviceTree& t = c->trees[tree];
+    if (!t.nodes) return fail(c, VV_ERR_STATE, "node pool not uploaded");
+    cudaSetDevice(c->device);
+    int rc = ensure(c, (void**)&c->d_grid_words, &c->grid_words_cap, t.cells * sizeof(uint2), "node staging");
+    if (rc) return rc;
+    VV_CUDA(c, launch_node_download(t.nodes, c->d_grid_words, t.dim, c->stream));
+    VV_CUDA(c, cudaMemcpyAsync(words, c->d_grid_words, t.cells * sizeof(uint2), cudaMemcpyDeviceToHost, c->stream));
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_brickpool_create(vv_ctx* c, int32_t sx, int32_t sy, int32_t sz, int32_t fmt) {
+    if (!c) return VV_ERR_ARG;
+    if (sx <= 0 || sy <= 0 || sz <= 0 || sx * 10 > 1023 || sy * 10 > 1023 || sz * 10 > 1023)
+        return fail(c, VV_ERR_ARG, "brick pool slots per axis must be in [1,102]");
+    const size_t tb = fmt_texel_bytes(fmt);
+    if (!tb) return fail(c, VV_ERR_ARG, "unknown brick format");
+    cudaSetDevice(c->device);
+    if (c->bricks) {
+        VV_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->bricks);
+        c->bricks = nullptr;
+    }
+    const long long total = (long long)sx * sy * sz;
+    const size_t bytes = (size_t)total * VV_BRICK_TEXELS * tb;
+    cudaError_t e = cudaMalloc(&c->bricks, bytes);
+    if (e != cudaSuccess) {
+        c->bricks = nullptr;
+        return fail(c, VV_ERR_OOM, "cudaMalloc brick pool");
+    }
+    VV_CUDA(c, cudaMemsetAsync(c->bricks, 0, bytes, c->stream));
+    c->slots[0] = sx;
+    c->slots[1] = sy;
+    c->slots[2] = sz;
+    c->total_slots = total;
+    c->fmt = fmt;
+    c->brick_bytes = VV_BRICK_TEXELS * tb;
+    c->pool_bytes = bytes;
+    return VV_OK;
+}
+
+int vv_upload_bricks_device(vv_ctx* c, const uint32_t* slots_dev, int32_t n, const void* texels_dev) {
+    if (!c || n < 0 || (n > 0 && (!slots_dev || !texels_dev))) return fail(c, VV_ERR_ARG, "bad upload arguments");
+    if (!c->bricks) return fail(c, VV_ERR_STATE, "brick pool not created");
+    cudaSetDevice(c->device);
+    VV_CUDA(c, launch_brick_scatter(slots_dev, n, texels_dev, c->bricks, c->brick_bytes, c->total_slots,
+                                    c->d_status, c->stream));
+    return VV_OK;
+}
+
+int vv_upload_bricks(vv_ctx* c, const uint32_t* slots, int32_t n, const void* texels) {
+    if (!c || n < 0 || (n > 0 && (!slots || !texels))) return fail(c, VV_ERR_ARG, "bad upload arguments");
+    if (!c->bricks) return fail(c, VV_ERR_STATE, "brick pool not created");
+    if (n == 0) return VV_OK;
+    cudaSetDevice(c->device);
+    const size_t bb = (size_t)n * c->brick_bytes, sb = (size_t)n * sizeof(uint32_t);
+    int rc = ensure(c, &c->d_up_bricks, &c->up_bricks_cap, bb, "brick staging");
+    if (rc) return rc;
+    rc = ensure(c, (void**)&c->d_up_slots, &c->up_slots_cap, sb, "slot staging");
+    if (rc) return rc;
+    VV_CUDA(c, cudaMemcpyAsync(c->d_up_bricks, texels, bb, cudaMemcpyHostToDevice, c->stream));
+    VV_CUDA(c, cudaMemcpyAsync(c->d_up_slots, slots, sb, cudaMemcpyHostToDevice, c->stream));
+    VV_CUDA(c, launch_brick_scatter(c->d_up_slots, n, c->d_up_bricks, c->bricks, c->brick_bytes, c->total_slots,
+                                    c->d_status, c->stream));
+    // The caller's host buffers may be pageable and reused right after return.
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_brickpool_download(vv_ctx* c, void* texels) {
+    if (!c || !texels) return VV_ERR_ARG;
+    if (!c->bricks) return fail(c, VV_ERR_STATE, "brick pool not created");
+    cudaSetDevice(c->device);
+    VV_CUDA(c, cudaMemcpyAsync(texels, c->bricks, c->pool_bytes, cudaMemcpyDeviceToHost, c->stream));
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_brickpool_device_ptr(vv_ctx* c, void** ptr, size_t* bytes) {
+    if (!c || !ptr) return VV_ERR_ARG;
+    *ptr = c->bricks;
+    if (bytes) *bytes = c->pool_bytes;
+    return VV_OK;
+}
+
+int vv_set_jitter(vv_ctx* c, const uint8_t* table, int32_t size) {
+    if (!c || !table || size <= 0 || size > 256) return fail(c, VV_ERR_ARG, "bad jitter table");
+    cudaSetDevice(c->device);
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->d_jitter) cudaFree(c->d_jitter);
+    c->d_jitter = nullptr;
+    VV_CUDA(c, cudaMalloc(&c->d_jitter, (size_t)size * size));
+    VV_CUDA(c, cudaMemcpy(c->d_jitter, table, (size_t)size * size, cudaMemcpyHostToDevice));
+    c->jitter_size = size;
+    return VV_OK;
+}
+
+int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out* out) {
+    if (!c || !u || !out || tree < 0 || tree >= VV_MAX_TREES) return fail(c, VV_ERR_ARG, "bad render arguments");
+    const DeviceTree& t = c->trees[tree];
+    if (!t.nodes) return fail(c, VV_ERR_STATE, "node pool not uploaded");
+    if (!c->bricks) return fail(c, VV_ERR_STATE, "brick pool not created");
+    const int W = u->width, H = u->height;
+    if (W <= 0 || H <= 0 || W > 16384 || H > 16384) return fail(c, VV_ERR_ARG, "bad viewport");
+    if (u->jitter_tex_size != c->jitter_size) return fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
+    if (!(u->ray_step_size > 0.0f)) return fail(c, VV_ERR_ARG, "ray_step_size must be > 0");
+    for (int a = 0; a < 3; ++a)
+        if (u->brick_pool_dimension[a] != (float)(c->slots[a] * 10))
+            return fail(c, VV_ERR_ARG, "brick_pool_dimension does not match the brick pool");
+    cudaSetDevice(c->device);
+    const size_t npix = (size_t)W * H;
+    const int passes = out->passes ? out->passes : VV_PASS_ALL;
+
+    uint4* usage = (uint4*)out->usage;
+    if (!usage && (passes & (VV_PASS_SELECT | VV_PASS_COMPACT))) {
+        int rc = ensure(c, (void**)&c->d_usage, &c->usage_cap, npix * 48, "usage scratch");
+        if (rc) return rc;
+        usage = (uint4*)c->d_usage;
+    }
+    if (passes & VV_PASS_RAYCAST) {
+        RaycastParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.u = *u;
+        p.nodes = t.nodes;
+        p.node_dim[0] = t.dim[0];
+        p.node_dim[1] = t.dim[1];
+        p.node_dim[2] = t.dim[2];
+        p.bricks = c->bricks;
+        p.slots[0] = c->slots[0];
+        p.slots[1] = c->slots[1];
+        p.slots[2] = c->slots[2];
+        p.jitter = c->d_jitter;
+        p.color = (float4*)out->color;
+        p.usage = usage;
+        p.status = c->d_status;
+        p.max_iter = vv_max_iterations(u);
+        VV_CUDA(c, launch_raycast(c->fmt, p, c->stream));
+    }
+    if (!(passes & (VV_PASS_SELECT | VV_PASS_COMPACT))) return VV_OK;
+
+    // level dims of the histopyramid (GigaVoxelsRenderer.cpp:1967-2046)
+    CompactParams cp;
+    std::memset(&cp, 0, sizeof(cp));
+    cp.width = W;
+    cp.height = H;
+    {
+        int w = W, h = H, l = 0;
+        long long off = 0;
+        while (true) {
+            if (l >= 24) return fail(c, VV_ERR_ARG, "viewport too large for the pyramid");
+            cp.level_w[l] = w;
+            cp.level_h[l] = h;
+            cp.level_off[l] = off;
+            off += (long long)w * h;
+            ++l;
+            if (w == 1 && h == 1) break;
+            if (w != 1) w >>= 1;
+            if (h != 1) h >>= 1;
+        }
+        cp.levels = l;
+        int rc = ensure(c, (void**)&c->d_counts, &c->counts_cap, (size_t)off * 4, "pyramid counts");
+        if (rc) return rc;
+        rc = ensure(c, (void**)&c->d_offsets, &c->offsets_cap, (size_t)off * 4, "pyramid offsets");
+        if (rc) return rc;
+    }
+    uint32_t* mask = out->mask;
+    if (!mask) {
+        int rc = ensure(c, (void**)&c->d_mask, &c->mask_cap, npix * 4, "mask scratch");
+        if (rc) return rc;
+        mask = c->d_mask;
+    }
+    VV_CUDA(c, launch_select(usage, mask, c->d_counts, W, H, c->stream));
+    if (!(passes & VV_PASS_COMPACT)) return VV_OK;
+    cp.counts = c->d_counts;
+    cp.offsets = c->d_offsets;
+    cp.usage = usage;
+    cp.mask = mask;
+    cp.requests = out->requests;
+    cp.request_count = out->request_count;
+    cp.cap = out->requests ? out->request_cap : 0;
+    cp.max_push = out->compress_max_push > 0 ? out->compress_max_push : 4;
+    VV_CUDA(c, launch_compact(cp, c->stream));
+    return VV_OK;
+}
+
+}  // extern "C"
+
+namespace vv {
+
+int vv_max_iterations(const vv_uniforms* u) {
+    // Every leaf segment advances the ray by at least one half-voxel step of
+    // the leaf level and a descent has at most depth+1 fetches, so a ray
+    // entering anywhere needs fewer than (sqrt(3) / step + 2) * (depth + 2)
+    // iterations.  The bound has a factor 2 of margin.
+    double segs = 1.7320508 / (double)u->ray_step_size + 2.0;
+    double it = 2.0 * segs * (double)(u->oct_tree_depth_minus_one + 2) + 64.0;
+    if (u->max_segments > 0) it = (double)u->max_segments;
+    if (it > 2.0e9) it = 2.0e9;
+    return (int)it;
+}
+
+}  // namespace vv

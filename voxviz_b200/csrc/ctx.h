@@ -1,0 +1,58 @@
+// ctx.h - the device context behind the vv_ctx handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/voxviz_b200.h"
+
+namespace vv {
+
+struct DeviceTree {
+    uint2* nodes = nullptr;  // block-linear node pool
+    int dim[3] = {0, 0, 0};
+    size_t cells = 0;
+};
+
+int vv_max_iterations(const vv_uniforms* u);
+
+}  // namespace vv
+
+struct vv_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int* d_status = nullptr;
+    vv::DeviceTree trees[VV_MAX_TREES];
+    // brick pool
+    void* bricks = nullptr;
+    int slots[3] = {0, 0, 0};
+    long long total_slots = 0;
+    int fmt = VV_FMT_RGBA8;
+    size_t brick_bytes = 0;
+    size_t pool_bytes = 0;
+    // jitter
+    uint8_t* d_jitter = nullptr;
+    int jitter_size = 0;
+    // scratch
+    uint32_t* d_usage = nullptr;
+    size_t usage_cap = 0;
+    uint32_t* d_mask = nullptr;
+    size_t mask_cap = 0;
+    uint32_t* d_counts = nullptr;
+    size_t counts_cap = 0;
+    uint32_t* d_offsets = nullptr;
+    size_t offsets_cap = 0;
+    uint32_t* d_up_slots = nullptr;
+    size_t up_slots_cap = 0;
+    void* d_up_bricks = nullptr;
+    size_t up_bricks_cap = 0;
+    vv_node_patch* d_patches = nullptr;
+    size_t patches_cap = 0;
+    uint32_t* d_grid_words = nullptr;
+    size_t grid_words_cap = 0;
+    void* h_stage = nullptr;
+    size_t h_stage_cap = 0;
+};

@@ -1,0 +1,55 @@
+// kernels.cuh - device-side launch interfaces of the GigaVoxels hot path.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/voxviz_b200.h"
+
+namespace vv {
+
+// Everything one ray-cast launch reads (kernel parameter, __grid_constant__).
+struct RaycastParams {
+    vv_uniforms u;
+    const uint2* nodes;      // node pool, block-linear: 8 nodes of a 2x2x2 cell contiguous
+    int node_dim[3];         // node-pool grid dims (even)
+    const void* bricks;      // brick pool, slot-major brick-linear texels
+    int slots[3];            // slots per axis
+    const uint8_t* jitter;   // jitter_tex_size^2 bytes
+    float4* color;           // [H*W] or nullptr
+    uint4* usage;            // [H*W*3] (12 uint32 per pixel)
+    int* status;             // sticky device status word
+    int max_iter;            // bound on outer-loop iterations per ray
+};
+
+// Pyramid/compaction launch state.
+struct CompactParams {
+    int width, height;
+    int levels;                       // pyramid levels (level 0 = full res)
+    int level_w[24], level_h[24];
+    long long level_off[24];          // element offset of each level in counts/offsets
+    uint32_t* counts;                 // pyramid counts (all levels)
+    uint32_t* offsets;                // exclusive offsets (all levels)
+    const uint4* usage;
+    const uint32_t* mask;
+    uint32_t* requests;               // [cap][4]
+    uint32_t* request_count;
+    int cap;
+    int max_push;
+};
+
+cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s);
+cudaError_t launch_select(const uint4* usage, uint32_t* mask, uint32_t* level0, int w, int h,
+                          cudaStream_t s);
+cudaError_t launch_compact(const CompactParams& p, cudaStream_t s);
+cudaError_t launch_node_upload(const uint32_t* grid_words, uint2* nodes, const int dim[3],
+                               cudaStream_t s);
+cudaError_t launch_node_download(const uint2* nodes, uint32_t* grid_words, const int dim[3],
+                                 cudaStream_t s);
+cudaError_t launch_node_patch(const vv_node_patch* patches, int n, uint2* nodes, const int dim[3],
+                              int* status, cudaStream_t s);
+cudaError_t launch_brick_scatter(const uint32_t* slots, int n, const void* src, void* pool,
+                                 size_t brick_bytes, long long total_slots, int* status,
+                                 cudaStream_t s);
+
+}  // namespace vv

@@ -1,0 +1,321 @@
+// octree.cpp - terrain octree builder, node-pool layout and brick production.
+#include "octree.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "../../include/voxviz_b200.h"
+
+namespace vv {
+
+// Node::computeNodeType (GigaVoxelsOctTree.cpp:1490-1609).  The region is the
+// node's 8^3 mip voxels plus a 1-voxel border on every side that is inside
+// the level; a region that reaches the volume edge is compared against
+// transparent black (:1556-1568).  Transparent voxels match any transparent
+// value (:1577-1580).
+bool classify_node(const TerrainVolume& vol, int d, int i, int j, int k, uint32_t& const_value) {
+    const int L = vol.depth();
+    const int m = L - d;
+    const MipLevel& M = vol.mip(m);
+    const int dim = M.dim;
+    const int idx[3] = {i, j, k};
+    int a0[3], a1[3];
+    bool edge = false;
+    for (int ax = 0; ax < 3; ++ax) {
+        a0[ax] = 8 * idx[ax];
+        a1[ax] = a0[ax] + 8;
+        if (a0[ax] != 0) a0[ax] -= 1;
+        if (a1[ax] <= dim - 1) a1[ax] += 1;
+        if (a1[ax] > dim) a1[ax] = dim;
+        if (a0[ax] == 0 || a1[ax] == dim) edge = true;
+    }
+    const uint32_t cv = edge ? 0u : vol.voxel(m, a0[0], a0[1], a0[2]);
+    int minS = INT_MAX, maxE = 0;
+    for (int y = a0[1]; y < a1[1]; ++y)
+        for (int x = a0[0]; x < a1[0]; ++x) {
+            size_t c = (size_t)y * dim + x;
+            int s = M.s[c];
+            minS = std::min(minS, s);
+            maxE = std::max(maxE, s + (int)M.r[c]);
+        }
+    if (a0[2] >= maxE) {  // every voxel transparent black
+        const_value = cv;
+        return true;
+    }
+    if (a1[2] <= minS) {  // every voxel pure solid, colour by band
+        if (edge) return false;
+        if (vol.band(m, a0[2]) != vol.band(m, a1[2] - 1)) return false;
+        const_value = cv;
+        return true;
+    }
+    const bool cv_clear = (cv >> 24) == 0u;
+    for (int z = a0[2]; z < a1[2]; ++z)
+        for (int y = a0[1]; y < a1[1]; ++y)
+            for (int x = a0[0]; x < a1[0]; ++x) {
+                uint32_t v = vol.voxel(m, x, y, z);
+                if ((v >> 24) == 0u && cv_clear) continue;
+                if (v != cv) return false;
+            }
+    const_value = cv;
+    return true;
+}
+
+namespace {
+struct LevelNodes {
+    std::vector<uint16_t> i, j, k;
+    std::vector<uint32_t> parent;       // local index in the previous level
+    std::vector<uint32_t> first_child;  // local index in the next level or UINT32_MAX
+    std::vector<uint32_t> cval;
+    std::vector<uint8_t> isc;
+    std::vector<uint32_t> nidx;         // global node index
+    size_t size() const { return i.size(); }
+    void push(int a, int b, int c, uint32_t p) {
+        i.push_back((uint16_t)a);
+        j.push_back((uint16_t)b);
+        k.push_back((uint16_t)c);
+        parent.push_back(p);
+    }
+};
+}  // namespace
+
+std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<const TerrainVolume> vol,
+                                                            bool collapse) {
+    std::unique_ptr<GigaVoxelsOctTree> t(new GigaVoxelsOctTree());
+    t->vol_ = vol;
+    const int L = vol->depth();
+    t->depth_ = L;
+    std::vector<LevelNodes> lv((size_t)L + 1);
+    lv[0].push(0, 0, 0, kNoParent);
+    for (int d = 0; d <= L; ++d) {
+        LevelNodes& cur = lv[(size_t)d];
+        const size_t n = cur.size();
+        cur.cval.assign(n, 0);
+        cur.isc.assign(n, 0);
+        cur.first_child.assign(n, UINT32_MAX);
+        cur.nidx.assign(n, 0);
+#pragma omp parallel for schedule(dynamic, 256)
+        for (long q = 0; q < (long)n; ++q) {
+            uint32_t cv = 0;
+            bool c = classify_node(*vol, d, cur.i[(size_t)q], cur.j[(size_t)q], cur.k[(size_t)q], cv);
+            cur.isc[(size_t)q] = c ? 1 : 0;
+            cur.cval[(size_t)q] = cv;
+        }
+        if (d == L) break;
+        LevelNodes& nxt = lv[(size_t)d + 1];
+        for (size_t q = 0; q < n; ++q) {
+            if (collapse && cur.isc[q]) continue;
+            cur.first_child[q] = (uint32_t)nxt.size();
+            for (int c = 0; c < 8; ++c)
+                nxt.push(2 * cur.i[q] + (c & 1), 2 * cur.j[q] + ((c >> 1) & 1), 2 * cur.k[q] + (c >> 2),
+                         (uint32_t)q);
+        }
+    }
+    // Depth-first pre-order block numbering (BuildOctTreeChildren allocates a
+    // child's block right before recursing into it).
+    size_t blocks = 1;
+    {
+        std::vector<std::pair<int, uint32_t>> stack;
+        lv[0].nidx[0] = 0;
+        stack.push_back({0, 0u});
+        while (!stack.empty()) {
+            auto [d, q] = stack.back();
+            stack.pop_back();
+            uint32_t fc = lv[(size_t)d].first_child[q];
+            if (fc == UINT32_MAX) continue;
+            size_t B = blocks++;
+            LevelNodes& nxt = lv[(size_t)d + 1];
+            for (int c = 0; c < 8; ++c) nxt.nidx[fc + (uint32_t)c] = (uint32_t)(8 * B + (size_t)c);
+            for (int c = 7; c >= 0; --c) stack.push_back({d + 1, fc + (uint32_t)c});
+        }
+    }
+    const size_t num_nodes = 8 * blocks;
+    // OctTreeNodePool::create3DTexture grid dimensions (NodePool.cpp:98-116).
+    size_t cube_root = (size_t)std::pow((double)num_nodes, 1.0 / 3.0);
+    if (cube_root % 2 != 0) {
+        --cube_root;
+        if (cube_root == 0) cube_root = 2;
+    }
+    size_t dx = cube_root, dy = cube_root, dz = cube_root;
+    while (dx * dy * dz < num_nodes) dx += 2;
+    if (dx > 1022 || dy > 1022 || dz > 1022)
+        throw std::runtime_error("node pool exceeds the 10-bit grid of the node encoding");
+    t->pool_dim_[0] = (int)dx;
+    t->pool_dim_[1] = (int)dy;
+    t->pool_dim_[2] = (int)dz;
+
+    t->level_.assign(num_nodes, -1);
+    t->ci_.assign(num_nodes, 0);
+    t->cj_.assign(num_nodes, 0);
+    t->ck_.assign(num_nodes, 0);
+    t->parent_.assign(num_nodes, kNoParent);
+    t->word0_.assign(num_nodes, 0);
+    t->word1_.assign(num_nodes, 0);
+    const size_t bx = dx / 2, by = dy / 2;
+    size_t nonconst = 0;
+    for (int d = 0; d <= L; ++d) {
+        const LevelNodes& cur = lv[(size_t)d];
+        for (size_t q = 0; q < cur.size(); ++q) {
+            uint32_t n = cur.nidx[q];
+            t->level_[n] = (int8_t)d;
+            t->ci_[n] = cur.i[q];
+            t->cj_[n] = cur.j[q];
+            t->ck_[n] = cur.k[q];
+            t->parent_[n] = d == 0 ? kNoParent : lv[(size_t)d - 1].nidx[cur.parent[q]];
+            uint32_t w0 = 0, w1 = 0;
+            if (cur.isc[q]) {
+                w0 |= kConstantBit;
+                w1 = cur.cval[q];
+            } else {
+                ++nonconst;
+            }
+            if (cur.first_child[q] != UINT32_MAX) {
+                size_t B = lv[(size_t)d + 1].nidx[cur.first_child[q]] / 8;
+                uint32_t x = (uint32_t)(2 * (B % bx));
+                uint32_t y = (uint32_t)(2 * ((B / bx) % by));
+                uint32_t z = (uint32_t)(2 * (B / (bx * by)));
+                w0 |= pack10(x, y, z);
+            }
+            t->word0_[n] = w0;
+            t->word1_[n] = w1;
+        }
+    }
+    t->nonconst_ = nonconst;
+    return t;
+}
+
+void GigaVoxelsOctTree::grid_of(uint32_t n, uint32_t& x, uint32_t& y, uint32_t& z) const {
+    const uint32_t bx = (uint32_t)pool_dim_[0] / 2, by = (uint32_t)pool_dim_[1] / 2;
+    uint32_t k = n >> 3, c = n & 7u;
+    x = 2 * (k % bx) + (c & 1u);
+    y = 2 * ((k / bx) % by) + ((c >> 1) & 1u);
+    z = 2 * (k / (bx * by)) + (c >> 2);
+}
+
+uint32_t GigaVoxelsOctTree::index_of(uint32_t x, uint32_t y, uint32_t z) const {
+    if (x >= (uint32_t)pool_dim_[0] || y >= (uint32_t)pool_dim_[1] || z >= (uint32_t)pool_dim_[2])
+        return kNoParent;
+    const uint32_t bx = (uint32_t)pool_dim_[0] / 2, by = (uint32_t)pool_dim_[1] / 2;
+    uint64_t k = ((uint64_t)(z / 2) * by + (y / 2)) * bx + (x / 2);
+    uint64_t n = 8 * k + ((x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2));
+    if (n >= level_.size()) return kNoParent;
+    return (uint32_t)n;
+}
+
+void GigaVoxelsOctTree::words_grid(uint32_t* out) const {
+    const size_t cells = (size_t)pool_dim_[0] * pool_dim_[1] * pool_dim_[2];
+    std::memset(out, 0, cells * 2 * sizeof(uint32_t));
+    for (size_t n = 0; n < level_.size(); ++n) {
+        uint32_t x, y, z;
+        grid_of((uint32_t)n, x, y, z);
+        size_t g = ((size_t)z * pool_dim_[1] + y) * pool_dim_[0] + x;
+        out[2 * g] = word0_[n];
+        out[2 * g + 1] = word1_[n];
+    }
+}
+
+void GigaVoxelsOctTree::produce_brick_rgba8(uint32_t n, uint32_t* out) const {
+    const int d = level_[n];
+    const int m = depth_ - d;
+    const MipLevel& M = vol_->mip(m);
+    const int dim = M.dim;
+    const int x0 = 8 * ci_[n] - 1, y0 = 8 * cj_[n] - 1, z0 = 8 * ck_[n] - 1;
+    for (int by = 0; by < 10; ++by) {
+        const int y = y0 + by;
+        for (int bx = 0; bx < 10; ++bx) {
+            const int x = x0 + bx;
+            if (x < 0 || y < 0 || x >= dim || y >= dim) {
+                for (int bz = 0; bz < 10; ++bz) out[(bz * 10 + by) * 10 + bx] = 0u;
+                continue;
+            }
+            const size_t c = (size_t)y * dim + x;
+            const int s = M.s[c], e = s + M.r[c];
+            const uint32_t* run = M.data.empty() ? nullptr : M.data.data() + M.off[c];
+            for (int bz = 0; bz < 10; ++bz) {
+                const int z = z0 + bz;
+                uint32_t v;
+                if (z < 0 || z >= dim) v = 0u;
+                else if (z < s) v = band_colour(vol_->band(m, z));
+                else if (z < e) v = run[z - s];
+                else v = 0u;
+                out[(bz * 10 + by) * 10 + bx] = v;
+            }
+        }
+    }
+}
+
+size_t texel_bytes(int fmt) {
+    switch (fmt) {
+        case VV_FMT_RGBA8: return 4;
+        case VV_FMT_FP16: return 8;
+        case VV_FMT_BF16: return 8;
+        case VV_FMT_FP32: return 16;
+        default: return 0;
+    }
+}
+
+uint16_t float_to_half_rn(float f) {
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    const uint32_t sign = (x >> 16) & 0x8000u;
+    const uint32_t ax = x & 0x7FFFFFFFu;
+    if (ax >= 0x7F800000u) return (uint16_t)(sign | (ax > 0x7F800000u ? 0x7E00u : 0x7C00u));
+    if (ax >= 0x477FF000u) return (uint16_t)(sign | 0x7C00u);
+    if (ax < 0x38800000u) {
+        const int e = (int)(ax >> 23);
+        if (e < 102) return (uint16_t)sign;
+        const uint32_t mant = (ax & 0x7FFFFFu) | 0x800000u;
+        const int shift = 126 - e;
+        uint32_t q = mant >> shift;
+        const uint32_t rem = mant & ((1u << shift) - 1u), half = 1u << (shift - 1);
+        if (rem > half || (rem == half && (q & 1u))) ++q;
+        return (uint16_t)(sign | q);
+    }
+    const uint32_t e = (ax >> 23) - 127u + 15u;
+    uint32_t q = (e << 10) | ((ax & 0x7FFFFFu) >> 13);
+    const uint32_t rem = ax & 0x1FFFu;
+    if (rem > 0x1000u || (rem == 0x1000u && (q & 1u))) ++q;
+    return (uint16_t)(sign | q);
+}
+
+uint16_t float_to_bf16_rn(float f) {
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    if ((x & 0x7FFFFFFFu) > 0x7F800000u) return (uint16_t)((x >> 16) | 0x40u);
+    x += 0x7FFFu + ((x >> 16) & 1u);
+    return (uint16_t)(x >> 16);
+}
+
+void convert_texel(uint32_t v, int fmt, void* dst) {
+    float c[4];
+    for (int ch = 0; ch < 4; ++ch) c[ch] = (float)((v >> (8 * ch)) & 255u) / 255.0f;
+    switch (fmt) {
+        case VV_FMT_RGBA8: std::memcpy(dst, &v, 4); break;
+        case VV_FMT_FP16: {
+            uint16_t h[4];
+            for (int ch = 0; ch < 4; ++ch) h[ch] = float_to_half_rn(c[ch]);
+            std::memcpy(dst, h, 8);
+            break;
+        }
+        case VV_FMT_BF16: {
+            uint16_t h[4];
+            for (int ch = 0; ch < 4; ++ch) h[ch] = float_to_bf16_rn(c[ch]);
+            std::memcpy(dst, h, 8);
+            break;
+        }
+        case VV_FMT_FP32: std::memcpy(dst, c, 16); break;
+        default: break;
+    }
+}
+
+void GigaVoxelsOctTree::produce_brick(uint32_t n, int fmt, void* out) const {
+    uint32_t tmp[VV_BRICK_TEXELS];
+    produce_brick_rgba8(n, tmp);
+    const size_t tb = texel_bytes(fmt);
+    unsigned char* o = (unsigned char*)out;
+    for (int t = 0; t < VV_BRICK_TEXELS; ++t) convert_texel(tmp[t], fmt, o + (size_t)t * tb);
+}
+
+}  // namespace vv

@@ -1,0 +1,413 @@
+// renderer.cpp - GigaVoxels renderer frame protocol and page-request service.
+#include "renderer.h"
+
+#include "ctx.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace vv {
+
+namespace {
+
+struct D3 {
+    double x, y, z;
+};
+D3 d3(const float* a) { return D3{a[0], a[1], a[2]}; }
+D3 operator+(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+D3 operator-(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+D3 operator*(D3 a, double s) { return D3{a.x * s, a.y * s, a.z * s}; }
+double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+D3 cross(D3 a, D3 b) { return D3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+D3 unit(D3 a) { return a * (1.0 / std::sqrt(dot(a, a))); }
+
+// ComputePerspective (Camera.cpp:74-89): ymax = near * tanf(fovy * pi / 360).
+void frustum_extent(const vv_camera& cam, double& xmax, double& ymax) {
+    const double PI = 3.14159265358979323846;
+    ymax = (double)cam.near_dist * (double)std::tan((float)((double)cam.fov_y_deg * PI / 360.0));
+    const float aspect = (float)cam.width / (float)cam.height;
+    xmax = ymax * (double)aspect;
+}
+
+}  // namespace
+
+float camera_pixel_size(const vv_camera& cam) {
+    // Unproject window points (W/2,H/2) and (W/2+1,H/2+1) on the near plane and
+    // take 1 - cos of the angle between the two eye rays.  In eye space the
+    // points are (x_ndc*xmax, y_ndc*ymax, -near).
+    double xmax, ymax;
+    frustum_extent(cam, xmax, ymax);
+    const double n = cam.near_dist;
+    D3 a{0.0, 0.0, -n};
+    D3 b{(2.0 / cam.width) * xmax, (2.0 / cam.height) * ymax, -n};
+    return (float)(1.0 - dot(unit(a), unit(b)));
+}
+
+void make_jitter(uint32_t seed, int size, uint8_t* out) {
+    for (int i = 0; i < size * size; ++i) {
+        uint32_t h = lattice_hash((uint32_t)i, 0x51ED27u, seed ^ 0xA5A5A5A5u);
+        // rand()/RAND_MAX scaled to 255, zero bumped to one (GLUtils.cpp:478-485)
+        float f = (float)(h >> 8) * (1.0f / 16777215.0f);
+        unsigned char v = (unsigned char)(255.0f * f);
+        if (v == 0) v = 1;
+        out[i] = v;
+    }
+}
+
+void compute_uniforms(int depth, bool root_is_constant, const vv_camera& cam, const int slots[3],
+                      float lod_scalar, float alpha_stop, vv_uniforms& u) {
+    std::memset(&u, 0, sizeof(u));
+    // The volume box is [0,1]^3: translation 0.5, scale 1 (:1655-1672).
+    const float trans = 0.5f, scale = 1.0f;
+    for (int a = 0; a < 3; ++a) {
+        u.vol_extent_min[a] = ((0.0f - trans) / scale) + 0.5f;
+        u.vol_extent_max[a] = ((1.0f - trans) / scale) + 0.5f;
+        u.camera_position[a] = ((cam.position[a] - trans) / scale) + 0.5f;
+    }
+    D3 look = unit(d3(cam.look)), up = unit(d3(cam.up));
+    D3 left = unit(cross(up, look));  // vox::Camera keeps left = up x look
+    const float upf[3] = {(float)up.x, (float)up.y, (float)up.z};
+    const float leftf[3] = {(float)left.x, (float)left.y, (float)left.z};
+    std::memcpy(u.camera_up, upf, sizeof(upf));
+    std::memcpy(u.camera_left, leftf, sizeof(leftf));
+    // RayStepSize = getRayStepSize() * 0.5 with getRayStepSize = one leaf
+    // voxel (GigaVoxelsReader.cpp:430-440; GigaVoxelsRenderer.cpp:1705).
+    const int N = 8 << depth;
+    const float leaf = (1.0f / (float)N) / (1.0f - 0.0f);
+    const float rs = leaf * 0.5f;
+    u.ray_step_size = rs;
+    // BrickStepVector (:1728-1751)
+    const float pow2 = std::pow(2.0f, (float)depth);
+    const float bd[3] = {8.0f, 8.0f, 8.0f};
+    for (int a = 0; a < 3; ++a) {
+        float root_step = (scale * rs) * pow2;
+        float root_voxel = scale / bd[a];
+        float ratio = root_step / root_voxel;
+        float pool_dim = (float)(slots[a] * 10);
+        float pool_voxel = 1.0f / pool_dim;
+        u.brick_step_vector[a] = pool_voxel * ratio;
+        u.brick_dimension[a] = bd[a];
+        u.brick_pool_dimension[a] = pool_dim;
+    }
+    u.root_voxel_half_size = (1.0f / 8.0f) * 0.5f;  // (:1780-1787)
+    u.pixel_size = camera_pixel_size(cam);
+    u.lod_scalar = lod_scalar;
+    u.alpha_stop = alpha_stop;
+    u.oct_tree_depth_minus_one = depth;
+    u.max_nodes_to_push = 12 * ((cam.frame % 2) + 1);  // (:1813-1816)
+    u.root_node_is_constant = root_is_constant ? 1 : 0;
+    u.jitter_tex_size = 32;
+    u.width = cam.width;
+    u.height = cam.height;
+    const D3 C = d3(cam.position);
+    u.camera_inside = (C.x > 0.0 && C.x < 1.0 && C.y > 0.0 && C.y < 1.0 && C.z > 0.0 && C.z < 1.0) ? 1 : 0;
+    double xmax, ymax;
+    frustum_extent(cam, xmax, ymax);
+    D3 right = left * -1.0;
+    D3 O = C + look * (double)cam.near_dist - right * xmax - up * ymax;
+    D3 dx = right * (2.0 * xmax / cam.width), dy = up * (2.0 * ymax / cam.height);
+    const double o[3] = {O.x, O.y, O.z}, ddx[3] = {dx.x, dx.y, dx.z}, ddy[3] = {dy.x, dy.y, dy.z};
+    for (int a = 0; a < 3; ++a) {
+        u.near_origin[a] = (float)o[a];
+        u.near_dx[a] = (float)ddx[a];
+        u.near_dy[a] = (float)ddy[a];
+    }
+}
+
+void SlotLRU::init(uint32_t n) {
+    n_ = n;
+    prev_.resize(n);
+    next_.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        prev_[i] = i == 0 ? UINT32_MAX : i - 1;
+        next_[i] = i + 1 == n ? UINT32_MAX : i + 1;
+    }
+    head_ = 0;
+    tail_ = n ? n - 1 : 0;
+}
+
+void SlotLRU::touch(uint32_t s) {
+    if (s == tail_) return;
+    // unlink
+    uint32_t p = prev_[s], q = next_[s];
+    if (p != UINT32_MAX) next_[p] = q;
+    else head_ = q;
+    if (q != UINT32_MAX) prev_[q] = p;
+    // append
+    prev_[s] = tail_;
+    next_[s] = UINT32_MAX;
+    next_[tail_] = s;
+    tail_ = s;
+}
+
+GigaVoxelsRenderer::GigaVoxelsRenderer(vv_ctx* ctx, vv_octree*, const GigaVoxelsOctTree* tree,
+                                       const vv_renderer_desc& d)
+    : ctx_(ctx), tree_(tree), d_(d) {}
+
+GigaVoxelsRenderer::~GigaVoxelsRenderer() {
+    if (ctx_) vv_ctx_synchronize(ctx_);
+    void* bufs[] = {d_color, d_usage, d_mask, d_requests, d_count};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (h_stage_) cudaFreeHost(h_stage_);
+}
+
+int GigaVoxelsRenderer::init() {
+    const size_t tb = texel_bytes(d_.fmt);
+    if (!tb) return VV_ERR_ARG;
+    texel_bytes_ = tb;
+    size_t want;
+    if (d_.pool_bytes > 0) want = (size_t)d_.pool_bytes / (VV_BRICK_TEXELS * tb);
+    else want = tree_->nonconst_count() + 1;
+    if (want < 1) want = 1;
+    // BrickPool::init slot grid (GigaVoxelsBrickPool.cpp:75-87)
+    size_t cr = (size_t)std::pow((double)want, 1.0 / 3.0);
+    if (cr < 1) cr = 1;
+    size_t sx = cr, sy = cr, sz = cr;
+    while (sx * sy * sz < want) ++sx;
+    if (sx > 102 || sy > 102 || sz > 102) return VV_ERR_ARG;
+    slots_[0] = (int)sx;
+    slots_[1] = (int)sy;
+    slots_[2] = (int)sz;
+    total_slots_ = (uint32_t)(sx * sy * sz);
+    int rc = vv_brickpool_create(ctx_, slots_[0], slots_[1], slots_[2], d_.fmt);
+    if (rc) return rc;
+    const size_t nn = tree_->node_count();
+    w0_.resize(nn);
+    w1_.resize(nn);
+    for (size_t i = 0; i < nn; ++i) {
+        w0_[i] = tree_->word0((uint32_t)i);
+        w1_[i] = tree_->word1((uint32_t)i);
+    }
+    const int* pd = tree_->pool_dim();
+    std::vector<uint32_t> words((size_t)pd[0] * pd[1] * pd[2] * 2);
+    tree_->words_grid(words.data());
+    rc = vv_nodepool_upload(ctx_, 0, words.data(), pd[0], pd[1], pd[2]);
+    if (rc) return rc;
+    std::vector<uint8_t> jit(32 * 32);
+    make_jitter(d_.jitter_seed, 32, jit.data());
+    rc = vv_set_jitter(ctx_, jit.data(), 32);
+    if (rc) return rc;
+    lru_.init(total_slots_);
+    slot_node_.assign(total_slots_, -1);
+    node_slot_.assign(nn, -1);
+    touched_mark_.assign(nn, 0);
+    seen_mark_.assign(nn, 0);
+    // BrickPool::initBricks (GigaVoxelsBrickPool.cpp:270-354): the root
+    // brick, or every brick when the pool holds them all.
+    if (d_.preload_all) {
+        for (size_t n = 0; n < nn; ++n)
+            if (tree_->level((uint32_t)n) >= 0 && !tree_->is_constant((uint32_t)n)) {
+                if (pending_nodes_.size() >= total_slots_) break;
+                rc = upload_nodes((uint32_t)n);
+                if (rc) return rc;
+            }
+    } else if (!tree_->is_constant(0)) {
+        rc = upload_nodes(0);
+        if (rc) return rc;
+    }
+    rc = flush_uploads();
+    uploaded_ = 0;
+    return rc;
+}
+
+int GigaVoxelsRenderer::alloc_frame(int w, int h) {
+    if (w == width && h == height && d_color) return VV_OK;
+    void** bufs[] = {(void**)&d_color, (void**)&d_usage, (void**)&d_mask, (void**)&d_requests, (void**)&d_count};
+    vv_ctx_synchronize(ctx_);
+    for (void** b : bufs)
+        if (*b) {
+            cudaFree(*b);
+            *b = nullptr;
+        }
+    const size_t np = (size_t)w * h;
+    cap_ = d_.request_cap > 0 ? d_.request_cap : (int)np;
+    if (cudaMalloc((void**)&d_color, np * 16) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMalloc((void**)&d_usage, np * 48) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMalloc((void**)&d_mask, np * 4) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMalloc((void**)&d_requests, (size_t)cap_ * 16) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMalloc((void**)&d_count, 4) != cudaSuccess) return VV_ERR_OOM;
+    width = w;
+    height = h;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::draw(const vv_camera& cam) {
+    int rc = alloc_frame(cam.width, cam.height);
+    if (rc) return rc;
+    compute_uniforms(tree_->depth(), tree_->is_constant(0), cam, slots_, d_.lod_scalar, d_.alpha_stop, last_u_);
+    vv_frame_out o;
+    std::memset(&o, 0, sizeof(o));
+    o.color = d_color;
+    o.usage = d_usage;
+    o.mask = d_mask;
+    o.requests = d_requests;
+    o.request_count = d_count;
+    o.request_cap = cap_;
+    o.compress_max_push = 4 * ((cam.frame % 3) + 1);  // (GigaVoxelsRenderer.cpp:2093-2098)
+    o.passes = VV_PASS_ALL;
+    frame_ = cam.frame;
+    return vv_render(ctx_, 0, &last_u_, &o);
+}
+
+int GigaVoxelsRenderer::upload_nodes(uint32_t n) {
+    // BrickPool::update body (GigaVoxelsBrickPool.cpp:583-629): evict the
+    // LRU front, upload into its slot, move it to the back.
+    const uint32_t s = lru_.front();
+    const int32_t old = slot_node_[s];
+    if (old >= 0) {
+        node_slot_[(size_t)old] = -1;
+        w0_[(size_t)old] &= ~kBrickResidentBit;
+        if (!touched_mark_[(size_t)old]) {
+            touched_mark_[(size_t)old] = 1;
+            touched_.push_back((uint32_t)old);
+        }
+        ++evictions_;
+        --resident_;
+    }
+    slot_node_[s] = (int32_t)n;
+    node_slot_[n] = (int32_t)s;
+    const uint32_t sx = s % (uint32_t)slots_[0], sy = (s / (uint32_t)slots_[0]) % (uint32_t)slots_[1],
+                   sz = s / ((uint32_t)slots_[0] * (uint32_t)slots_[1]);
+    // uploadBrick (:800-810): pointer = slot origin + border
+    w1_[n] = pack10(sx * 10 + 1, sy * 10 + 1, sz * 10 + 1);
+    w0_[n] |= kBrickResidentBit;
+    if (!touched_mark_[n]) {
+        touched_mark_[n] = 1;
+        touched_.push_back(n);
+    }
+    lru_.touch(s);
+    pending_nodes_.push_back(n);
+    pending_slots_.push_back(s);
+    ++uploaded_;
+    ++uploaded_total_;
+    ++resident_;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::flush_uploads() {
+    const size_t n = pending_nodes_.size();
+    int rc = VV_OK;
+    if (n) {
+        const size_t bb = VV_BRICK_TEXELS * texel_bytes_;
+        const size_t bytes = n * bb;
+        if (h_stage_cap_ < bytes) {
+            if (h_stage_) cudaFreeHost(h_stage_);
+            h_stage_ = nullptr;
+            h_stage_cap_ = 0;
+            if (cudaMallocHost(&h_stage_, bytes) != cudaSuccess) return VV_ERR_OOM;
+            h_stage_cap_ = bytes;
+        }
+        unsigned char* st = (unsigned char*)h_stage_;
+        const int fmt = d_.fmt;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(d_.producer_threads > 0 ? d_.producer_threads : omp_get_max_threads())
+        for (long i = 0; i < (long)n; ++i) tree_->produce_brick(pending_nodes_[(size_t)i], fmt, st + (size_t)i * bb);
+        rc = vv_upload_bricks(ctx_, pending_slots_.data(), (int32_t)n, h_stage_);
+        if (rc) return rc;
+    }
+    if (!touched_.empty()) {
+        std::vector<vv_node_patch> patches;
+        patches.reserve(touched_.size());
+        for (uint32_t t : touched_) {
+            vv_node_patch q;
+            tree_->grid_of(t, q.x, q.y, q.z);
+            q.word0 = w0_[t];
+            q.word1 = w1_[t];
+            patches.push_back(q);
+            touched_mark_[t] = 0;
+        }
+        touched_.clear();
+        rc = vv_nodepool_patch(ctx_, 0, patches.data(), (int32_t)patches.size());
+        if (rc) return rc;
+    }
+    pending_nodes_.clear();
+    pending_slots_.clear();
+    return rc;
+}
+
+int GigaVoxelsRenderer::update() {
+    if (!d_count) return VV_ERR_STATE;
+    uploaded_ = 0;
+    uint32_t count = 0;
+    if (cudaMemcpyAsync(&count, d_count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    active_ = count;
+    const uint32_t n = std::min<uint32_t>(count, (uint32_t)cap_);
+    req_count_ = n;
+    host_requests_.resize((size_t)n * 4);
+    if (n) {
+        if (cudaMemcpyAsync(host_requests_.data(), d_requests, (size_t)n * 16, cudaMemcpyDeviceToHost,
+                            ctx_->stream) != cudaSuccess)
+            return VV_ERR_CUDA;
+        if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    }
+    // NodeUsageListProcessor::run (GigaVoxelsOctTree.cpp:430-657): decode the
+    // ids, keep the unique nodes in first-seen order, touch resident bricks,
+    // queue non-constant non-resident nodes for upload.
+    if (++seen_epoch_ == 0) {
+        std::fill(seen_mark_.begin(), seen_mark_.end(), 0u);
+        seen_epoch_ = 1;
+    }
+    std::vector<uint32_t> upload;
+    for (size_t i = 0; i < host_requests_.size(); ++i) {
+        const uint32_t id = host_requests_[i];
+        if (id == 0u) continue;
+        const uint32_t x = ((id >> 20) & 0x3FFu) - 1u, y = ((id >> 10) & 0x3FFu) - 1u, z = (id & 0x3FFu) - 1u;
+        const uint32_t nidx = tree_->index_of(x, y, z);
+        if (nidx == kNoParent || tree_->level(nidx) < 0) continue;
+        if (seen_mark_[nidx] == seen_epoch_) continue;
+        seen_mark_[nidx] = seen_epoch_;
+        if (node_slot_[nidx] >= 0) lru_.touch((uint32_t)node_slot_[nidx]);
+        else if (!tree_->is_constant(nidx)) upload.push_back(nidx);
+    }
+    // GigaVoxelsOctTree::update touches the root every frame (:1821-1850).
+    if (node_slot_[0] >= 0) lru_.touch((uint32_t)node_slot_[0]);
+    // BrickPool::update (GigaVoxelsBrickPool.cpp:561-682), including the
+    // upload of a non-resident non-constant parent (:629-673).
+    for (uint32_t nidx : upload) {
+        if (node_slot_[nidx] >= 0) continue;
+        int rc = upload_nodes(nidx);
+        if (rc) return rc;
+        const uint32_t par = tree_->parent(nidx);
+        if (par != kNoParent && !tree_->is_constant(par) && node_slot_[par] < 0) {
+            rc = upload_nodes(par);
+            if (rc) return rc;
+        }
+    }
+    return flush_uploads();
+}
+
+void GigaVoxelsRenderer::stats(vv_renderer_stats& s) const {
+    s.frame = frame_;
+    s.requests = req_count_;
+    s.active_pixels = active_;
+    s.bricks_uploaded = uploaded_;
+    s.bricks_uploaded_total = uploaded_total_;
+    s.resident_bricks = resident_;
+    s.evictions_total = evictions_;
+    s.pool_slots = (int32_t)total_slots_;
+}
+
+void GigaVoxelsRenderer::residency(std::vector<uint32_t>& xyz, std::vector<uint32_t>& slot) const {
+    xyz.clear();
+    slot.clear();
+    for (uint32_t s = 0; s < total_slots_; ++s) {
+        if (slot_node_[s] < 0) continue;
+        uint32_t x, y, z;
+        tree_->grid_of((uint32_t)slot_node_[s], x, y, z);
+        xyz.push_back(x);
+        xyz.push_back(y);
+        xyz.push_back(z);
+        slot.push_back(s);
+    }
+}
+
+}  // namespace vv
