@@ -72,8 +72,12 @@ typedef enum vv_fmt {
  * GigaVoxelsRenderer::drawVolume does (GigaVoxelsRenderer.cpp:1630-1816).
  * The second block replaces rasterisation of the volume box
  * (GigaVoxels.vert:11-19) and of the near-plane quad (NearPlaneQuad.vert:11-20):
- * pixel (px,py) (origin bottom-left, as gl_FragCoord) looks through the
- * near-plane point near_origin + (px+0.5)*near_dx + (py+0.5)*near_dy. */
+ * pixel (px,py) (origin bottom-left, as gl_FragCoord) looks along
+ * d = near_origin + (px+0.5)*near_dx + (py+0.5)*near_dy, the vector from the
+ * camera to the pixel's near-plane point (camera-relative, so that small near
+ * distances keep full float precision).  A camera outside the volume box
+ * starts the ray at the box entry camera + t*d; a camera inside starts it at
+ * the near-plane point camera + d. */
 typedef struct vv_uniforms {
     float ray_step_size;           /* RayStepSize                          */
     float brick_step_vector[3];    /* BrickStepVector                      */
@@ -204,6 +208,18 @@ int vv_set_jitter(vv_ctx* ctx, const uint8_t* table, int32_t size);
 int vv_render(vv_ctx* ctx, int32_t tree, const vv_uniforms* u,
               const vv_frame_out* out);
 
+/* Kernel timing: with profiling on, vv_render records CUDA events around the
+ * ray cast and around the selection/compaction passes on the context stream
+ * (the reference kept QElapsedTimer pass timers, GigaVoxelsRenderer.cpp:858-903).
+ * vv_ctx_last_times waits for the last draw and returns its two durations. */
+int vv_ctx_set_profiling(vv_ctx* ctx, int32_t on);
+int vv_ctx_last_times(vv_ctx* ctx, float* raycast_ms, float* compact_ms);
+/* Footprint of one draw: the number of distinct node-pool entries and
+ * brick-pool slots the ray cast of `u` reads (a counting variant of the same
+ * kernel; used for the algorithmic bytes of the roofline). */
+int vv_measure_footprint(vv_ctx* ctx, int32_t tree, const vv_uniforms* u,
+                         int64_t* nodes, int64_t* bricks);
+
 /* ---- host data model: terrain octree (GigaVoxelsOctTree) ----------------- */
 
 typedef struct vv_octree vv_octree;
@@ -332,6 +348,11 @@ int vv_renderer_frame_buffers(vv_renderer* r, float** color, uint32_t** usage,
                               uint32_t** request_count);
 /* Copy the last frame's colour (H*W*4 floats) to host memory. */
 int vv_renderer_read_color(vv_renderer* r, float* host_rgba);
+/* Copy the last frame's node-usage lists (H*W*12 words) and selection mask
+ * (H*W words) to host memory; NULL skips a buffer.  This is the readback of
+ * GigaVoxelsOctTree::updateNodeUsageListProcessor (GigaVoxelsOctTree.cpp:1852-1985)
+ * for the raw lists, kept for checking. */
+int vv_renderer_read_lists(vv_renderer* r, uint32_t* host_usage, uint32_t* host_mask);
 /* Host copy of the compacted request list of the last update (n x 4 words). */
 int vv_renderer_last_requests(const vv_renderer* r, uint32_t* out, int32_t cap,
                               int32_t* n);

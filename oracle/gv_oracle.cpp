@@ -363,19 +363,19 @@ struct Shader {
     // ray (GigaVoxels.vert) or the near-plane point (NearPlaneQuad.vert).
     bool RayPosition(int px, int py, vec3<T>& out) const {
         const T fx = (T)px + (T)0.5, fy = (T)py + (T)0.5;
-        vec3<T> P;
+        // camera-to-near-plane vector of this pixel
+        vec3<T> d;
         const float* o = U->near_origin;
         const float* dx = U->near_dx;
         const float* dy = U->near_dy;
-        P.x = (T)o[0] + fx * (T)dx[0] + fy * (T)dy[0];
-        P.y = (T)o[1] + fx * (T)dx[1] + fy * (T)dy[1];
-        P.z = (T)o[2] + fx * (T)dx[2] + fy * (T)dy[2];
+        d.x = (T)o[0] + fx * (T)dx[0] + fy * (T)dy[0];
+        d.y = (T)o[1] + fx * (T)dx[1] + fy * (T)dy[1];
+        d.z = (T)o[2] + fx * (T)dx[2] + fy * (T)dy[2];
+        const vec3<T> C = CameraPosition;
         if (U->camera_inside) {
-            out = P;
+            out = C + d;
             return true;
         }
-        const vec3<T> C = CameraPosition;
-        const vec3<T> d = P - C;
         const T da[3] = {d.x, d.y, d.z}, ca[3] = {C.x, C.y, C.z};
         const T mn[3] = {VolExtentMin.x, VolExtentMin.y, VolExtentMin.z};
         const T mx[3] = {VolExtentMax.x, VolExtentMax.y, VolExtentMax.z};

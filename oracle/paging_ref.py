@@ -1,0 +1,106 @@
+"""Restatement of the page-request service policy.  TEST INFRASTRUCTURE.
+
+NodeUsageListProcessor::run (VoxViz/GigaVoxels/GigaVoxelsOctTree.cpp:430-657)
+decodes the compacted list, keeps each node once, touches resident bricks
+and queues non-constant, non-resident nodes; BrickPool::update
+(VoxViz/GigaVoxels/GigaVoxelsBrickPool.cpp:561-682) uploads each queued node
+into the least recently used slot and also its parent when the parent is
+non-constant and not resident; GigaVoxelsOctTree::update touches the root
+every frame (GigaVoxelsOctTree.cpp:1821-1850).
+
+The reference runs this on worker threads with tryLock, so its order is not
+reproducible.  The policy both sides implement is the synchronous one:
+unique nodes in first-seen order of the list, touches in that order, then the
+root, then uploads in that order; the LRU list starts with the empty slots in
+slot-id order.  This module derives the tree from the node words alone.
+"""
+from __future__ import annotations
+
+from collections import OrderedDict
+
+import numpy as np
+
+RESIDENT = 0x80000000
+CONSTANT = 0x40000000
+
+
+class PagingRef:
+    def __init__(self, words: np.ndarray, slots: tuple[int, int, int]):
+        self.words = np.array(words, dtype=np.uint32, copy=True)  # (dz, dy, dx, 2)
+        self.sx, self.sy, self.sz = slots
+        self.total = self.sx * self.sy * self.sz
+        self.lru: OrderedDict[int, None] = OrderedDict((s, None) for s in range(self.total))
+        self.slot_node: dict[int, tuple] = {}
+        self.node_slot: dict[tuple, int] = {}
+        self.parent: dict[tuple, tuple] = {}
+        self.valid: set[tuple] = {(0, 0, 0)}
+        self._derive_tree()
+
+    def _derive_tree(self) -> None:
+        stack = [(0, 0, 0)]
+        while stack:
+            n = stack.pop()
+            w0 = int(self.words[n[2], n[1], n[0], 0])
+            c = ((w0 >> 20) & 1023, (w0 >> 10) & 1023, w0 & 1023)
+            if c == (0, 0, 0):
+                continue
+            for k in range(8):
+                ch = (c[0] + (k & 1), c[1] + ((k >> 1) & 1), c[2] + (k >> 2))
+                self.parent[ch] = n
+                self.valid.add(ch)
+                stack.append(ch)
+
+    def is_constant(self, n) -> bool:
+        return bool(int(self.words[n[2], n[1], n[0], 0]) & CONSTANT)
+
+    def _upload(self, n) -> None:
+        s = next(iter(self.lru))
+        old = self.slot_node.get(s)
+        if old is not None:
+            del self.node_slot[old]
+            self.words[old[2], old[1], old[0], 0] &= np.uint32(~RESIDENT & 0xFFFFFFFF)
+        self.slot_node[s] = n
+        self.node_slot[n] = s
+        x, y, z = s % self.sx, (s // self.sx) % self.sy, s // (self.sx * self.sy)
+        self.words[n[2], n[1], n[0], 1] = ((x * 10 + 1) << 20) | ((y * 10 + 1) << 10) | (z * 10 + 1)
+        self.words[n[2], n[1], n[0], 0] |= np.uint32(RESIDENT)
+        self.lru.move_to_end(s)
+        self.uploaded.append(n)
+
+    def init(self, preload_all: bool) -> None:
+        self.uploaded = []
+        if preload_all:
+            raise NotImplementedError("the paging checks start from the root brick only")
+        if not self.is_constant((0, 0, 0)):
+            self._upload((0, 0, 0))
+
+    def update(self, requests: np.ndarray) -> list:
+        """Service one frame's compacted list (n x 4 words); returns uploads."""
+        self.uploaded = []
+        seen = set()
+        queue = []
+        for v in np.asarray(requests, dtype=np.uint32).reshape(-1):
+            v = int(v)
+            if v == 0:
+                continue
+            n = (((v >> 20) & 1023) - 1, ((v >> 10) & 1023) - 1, (v & 1023) - 1)
+            if n not in self.valid or n in seen:
+                continue
+            seen.add(n)
+            if n in self.node_slot:
+                self.lru.move_to_end(self.node_slot[n])
+            elif not self.is_constant(n):
+                queue.append(n)
+        if (0, 0, 0) in self.node_slot:
+            self.lru.move_to_end(self.node_slot[(0, 0, 0)])
+        for n in queue:
+            if n in self.node_slot:
+                continue
+            self._upload(n)
+            p = self.parent.get(n)
+            if p is not None and not self.is_constant(p) and p not in self.node_slot:
+                self._upload(p)
+        return list(self.uploaded)
+
+    def residency(self) -> dict:
+        return dict(self.node_slot)

@@ -1,0 +1,90 @@
+"""GPU ray cast against the FP32 oracle on the same inputs: node-usage lists
+(node indices, LOD choices, traversal order) bit-exact, colour within 1/255
+(in practice identical: both sides run the same binary32 operations)."""
+import numpy as np
+import pytest
+
+import voxviz_b200 as vv
+from tests import helpers
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1.0 / 255.0
+
+
+@pytest.fixture(scope="module")
+def cfg1():
+    sc = helpers.Scene(seed=1, depth=5, collapse=True, fmt="rgba8")
+    return sc, helpers.GpuScene(sc)
+
+
+@pytest.mark.parametrize("view_seed,frame", [(3, 0), (5, 1), (11, 2), (17, 3)])
+def test_config1_view_matches_oracle(cfg1, view_seed, frame):
+    sc, g = cfg1
+    u = sc.uniforms(sc.view(view_seed, 512, 512, frame=frame))
+    got = g.render(u, max_push=4 * (frame % 3 + 1))
+    ref = helpers.oracle_frame(u, sc.oracle_scene(), max_push=4 * (frame % 3 + 1))
+    assert got["status"] == 0 and ref["status"] == 0
+    assert np.array_equal(got["usage"], ref["usage"])
+    err = np.abs(got["color"] - ref["color"])
+    assert err.max() <= TOL, err.max()
+    assert (err > 0).mean() < 1e-3
+    assert np.array_equal(got["mask"], ref["mask"])
+    assert got["count"] == ref["count"]
+    assert np.array_equal(got["requests"], ref["requests"])
+
+
+@pytest.mark.parametrize("alpha_stop", [0.995, 0.5])
+def test_alpha_stop_parameter(cfg1, alpha_stop):
+    sc, g = cfg1
+    u = sc.uniforms(sc.view(7, 256, 192), alpha=alpha_stop)
+    got = g.render(u)
+    ref = helpers.oracle_frame(u, sc.oracle_scene())
+    assert np.array_equal(got["usage"], ref["usage"])
+    assert np.abs(got["color"] - ref["color"]).max() <= TOL
+
+
+def test_full_tree_and_camera_inside():
+    sc = helpers.Scene(seed=4, depth=4, collapse=False)
+    g = helpers.GpuScene(sc)
+    from voxviz_b200 import scene
+    cams = scene.camera_path(2, sc.heights, 8, 200, 120)
+    for cam in cams[::3]:
+        u = sc.uniforms(cam)
+        assert u.camera_inside == 1
+        got = g.render(u)
+        ref = helpers.oracle_frame(u, sc.oracle_scene())
+        assert np.array_equal(got["usage"], ref["usage"])
+        assert np.abs(got["color"] - ref["color"]).max() <= TOL
+        assert np.array_equal(got["requests"], ref["requests"])
+
+
+@pytest.mark.parametrize("fmt", ["fp16", "bf16", "fp32"])
+def test_float_brick_formats_match_oracle(fmt):
+    sc = helpers.Scene(seed=1, depth=5, fmt=fmt)
+    g = helpers.GpuScene(sc)
+    u = sc.uniforms(sc.view(3, 384, 256))
+    got = g.render(u)
+    ref = helpers.oracle_frame(u, sc.oracle_scene())
+    assert np.array_equal(got["usage"], ref["usage"])
+    assert np.abs(got["color"] - ref["color"]).max() <= TOL
+
+
+def test_error_vs_fp64_oracle_reported_bounds(cfg1):
+    sc, g = cfg1
+    u = sc.uniforms(sc.view(3, 512, 512))
+    got = g.render(u)
+    ref64 = helpers.oracle_frame(u, sc.oracle_scene(), precision=64)
+    err = np.abs(got["color"].astype(np.float64) - ref64["color"])
+    rms = float(np.sqrt((err ** 2).mean()))
+    assert rms < TOL, rms
+    assert (err.max(-1) > TOL).mean() < 0.03
+
+
+def test_miss_only_view_is_empty(cfg1):
+    sc, g = cfg1
+    look, up = vv.look_at([0.5, 0.5, 1.5], [0.5, 0.5, 3.0])  # looking away from the volume
+    u = sc.uniforms(vv.make_camera([0.5, 0.5, 1.5], look, up, 64, 48))
+    got = g.render(u)
+    assert not got["color"].any() and not got["usage"].any()
+    assert got["count"] == 0 and got["requests"].shape[0] == 0

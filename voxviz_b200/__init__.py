@@ -254,6 +254,21 @@ class Context:
         size = int(round(np.sqrt(t.size)))
         self._ck(lib().vv_set_jitter(self._h, _ptr(t), size), "jitter")
 
+    def set_profiling(self, on: bool = True) -> None:
+        self._ck(lib().vv_ctx_set_profiling(self._h, 1 if on else 0), "profiling")
+
+    def last_times(self) -> tuple[float, float]:
+        """(ray-cast ms, selection+compaction ms) of the last profiled draw."""
+        a, b = C.c_float(), C.c_float()
+        self._ck(lib().vv_ctx_last_times(self._h, C.byref(a), C.byref(b)), "last times")
+        return a.value, b.value
+
+    def footprint(self, u: Uniforms, tree: int = 0) -> tuple[int, int]:
+        """(distinct node-pool entries, distinct brick slots) one draw reads."""
+        n, b = C.c_int64(), C.c_int64()
+        self._ck(lib().vv_measure_footprint(self._h, tree, C.byref(u), C.byref(n), C.byref(b)), "footprint")
+        return n.value, b.value
+
     def render(self, u: Uniforms, color=0, usage=0, mask=0, requests=0, request_count=0, request_cap=0,
                compress_max_push=4, passes=VV_PASS_ALL, tree: int = 0) -> None:
         """One draw; every buffer argument is a device pointer (int) or 0."""
@@ -281,6 +296,8 @@ class Renderer:
         self.ctx = ctx
         self.octree = octree
         self.fmt = fmt_code(fmt)
+        ctx._node_dims = tuple(octree.info.pool_dim)
+        ctx.fmt = self.fmt
 
     def close(self) -> None:
         if self._h:
@@ -312,11 +329,21 @@ class Renderer:
         self._ck(lib().vv_renderer_frame_buffers(self._h, *[C.byref(p) for p in ptrs]), "frame buffers")
         return dict(zip(["color", "usage", "mask", "requests", "request_count"], [p.value for p in ptrs]))
 
-    def read_color(self) -> np.ndarray:
-        u = self.last_uniforms()
-        out = np.zeros((u.height, u.width, 4), dtype=np.float32)
+    def read_color(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Last frame's colour (H,W,4) float32, into `out` (e.g. pinned) if given."""
+        if out is None:
+            u = self.last_uniforms()
+            out = np.zeros((u.height, u.width, 4), dtype=np.float32)
         self._ck(lib().vv_renderer_read_color(self._h, _ptr(out)), "read color")
         return out
+
+    def read_lists(self):
+        """(usage (H,W,12), mask (H,W)) of the last frame, uint32."""
+        u = self.last_uniforms()
+        usage = np.zeros((u.height, u.width, 12), dtype=np.uint32)
+        mask = np.zeros((u.height, u.width), dtype=np.uint32)
+        self._ck(lib().vv_renderer_read_lists(self._h, _ptr(usage), _ptr(mask)), "read lists")
+        return usage, mask
 
     def last_requests(self) -> np.ndarray:
         n = C.c_int32()

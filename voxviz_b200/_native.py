@@ -173,6 +173,10 @@ SIGNATURES = {
     "vv_brickpool_device_ptr": (C.c_int, [P, C.POINTER(P), C.POINTER(C.c_size_t)]),
     "vv_set_jitter": (C.c_int, [P, P, C.c_int32]),
     "vv_render": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(FrameOut)]),
+    "vv_ctx_set_profiling": (C.c_int, [P, C.c_int32]),
+    "vv_ctx_last_times": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "vv_measure_footprint": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64)]),
     "vv_octree_build_terrain": (C.c_int, [C.POINTER(TerrainDesc), C.POINTER(P)]),
     "vv_octree_destroy": (None, [P]),
     "vv_octree_get_info": (C.c_int, [P, C.POINTER(OctreeInfo)]),
@@ -192,6 +196,7 @@ SIGNATURES = {
     "vv_renderer_get_stats": (C.c_int, [P, C.POINTER(RendererStats)]),
     "vv_renderer_frame_buffers": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "vv_renderer_read_color": (C.c_int, [P, P]),
+    "vv_renderer_read_lists": (C.c_int, [P, P, P]),
     "vv_renderer_last_requests": (C.c_int, [P, P, C.c_int32, i32p]),
     "vv_renderer_residency": (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),
     "vv_renderer_last_uniforms": (C.c_int, [P, C.POINTER(Uniforms)]),

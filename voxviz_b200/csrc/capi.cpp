@@ -203,6 +203,18 @@ int vv_renderer_read_color(vv_renderer* r, float* host_rgba) {
     return VV_OK;
 }
 
+int vv_renderer_read_lists(vv_renderer* r, uint32_t* host_usage, uint32_t* host_mask) {
+    if (!r || !r->impl->d_usage) return VV_ERR_ARG;
+    const size_t np = (size_t)r->impl->width * r->impl->height;
+    cudaStream_t s = r->ctx->stream;
+    if (host_usage && cudaMemcpyAsync(host_usage, r->impl->d_usage, np * 48, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (host_mask && cudaMemcpyAsync(host_mask, r->impl->d_mask, np * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return VV_ERR_CUDA;
+    return VV_OK;
+}
+
 int vv_renderer_last_requests(const vv_renderer* r, uint32_t* out, int32_t cap, int32_t* n) {
     if (!r || !n) return VV_ERR_ARG;
     const auto& q = r->impl->last_requests();

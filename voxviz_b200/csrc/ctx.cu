@@ -134,6 +134,8 @@ int vv_ctx_destroy(vv_ctx* c) {
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->h_stage) cudaFreeHost(c->h_stage);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
     delete c;
     return VV_OK;
 }
@@ -334,6 +336,8 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         if (rc) return rc;
         usage = (uint4*)c->d_usage;
     }
+    c->timed = c->profiling;
+    if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
     if (passes & VV_PASS_RAYCAST) {
         RaycastParams p;
         std::memset(&p, 0, sizeof(p));
@@ -353,7 +357,11 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         p.max_iter = vv_max_iterations(u);
         VV_CUDA(c, launch_raycast(c->fmt, p, c->stream));
     }
-    if (!(passes & (VV_PASS_SELECT | VV_PASS_COMPACT))) return VV_OK;
+    if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+    if (!(passes & (VV_PASS_SELECT | VV_PASS_COMPACT))) {
+        if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
+        return VV_OK;
+    }
 
     // level dims of the histopyramid (GigaVoxelsRenderer.cpp:1967-2046)
     CompactParams cp;
@@ -387,7 +395,10 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         mask = c->d_mask;
     }
     VV_CUDA(c, launch_select(usage, mask, c->d_counts, W, H, c->stream));
-    if (!(passes & VV_PASS_COMPACT)) return VV_OK;
+    if (!(passes & VV_PASS_COMPACT)) {
+        if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
+        return VV_OK;
+    }
     cp.counts = c->d_counts;
     cp.offsets = c->d_offsets;
     cp.usage = usage;
@@ -397,6 +408,68 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
     cp.cap = out->requests ? out->request_cap : 0;
     cp.max_push = out->compress_max_push > 0 ? out->compress_max_push : 4;
     VV_CUDA(c, launch_compact(cp, c->stream));
+    if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
+    return VV_OK;
+}
+
+int vv_ctx_set_profiling(vv_ctx* c, int32_t on) {
+    if (!c) return VV_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (on && !c->ev[0])
+        for (auto& e : c->ev) VV_CUDA(c, cudaEventCreate(&e));
+    c->profiling = on != 0;
+    c->timed = false;
+    return VV_OK;
+}
+
+int vv_ctx_last_times(vv_ctx* c, float* raycast_ms, float* compact_ms) {
+    if (!c) return VV_ERR_ARG;
+    if (!c->timed) return fail(c, VV_ERR_STATE, "no profiled draw");
+    cudaSetDevice(c->device);
+    VV_CUDA(c, cudaEventSynchronize(c->ev[2]));
+    float a = 0.f, b = 0.f;
+    VV_CUDA(c, cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+    VV_CUDA(c, cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
+    if (raycast_ms) *raycast_ms = a;
+    if (compact_ms) *compact_ms = b;
+    return VV_OK;
+}
+
+int vv_measure_footprint(vv_ctx* c, int32_t tree, const vv_uniforms* u, int64_t* nodes, int64_t* bricks) {
+    if (!c || !u || tree < 0 || tree >= VV_MAX_TREES) return fail(c, VV_ERR_ARG, "bad footprint arguments");
+    const DeviceTree& t = c->trees[tree];
+    if (!t.nodes || !c->bricks) return fail(c, VV_ERR_STATE, "pools not ready");
+    if (u->jitter_tex_size != c->jitter_size) return fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
+    cudaSetDevice(c->device);
+    const size_t nwords = (t.cells + 31) / 32, bwords = ((size_t)c->total_slots + 31) / 32;
+    uint32_t* bits = nullptr;
+    VV_CUDA(c, cudaMalloc(&bits, (nwords + bwords) * 4));
+    cudaMemsetAsync(bits, 0, (nwords + bwords) * 4, c->stream);
+    RaycastParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.u = *u;
+    p.nodes = t.nodes;
+    for (int a = 0; a < 3; ++a) {
+        p.node_dim[a] = t.dim[a];
+        p.slots[a] = c->slots[a];
+    }
+    p.bricks = c->bricks;
+    p.jitter = c->d_jitter;
+    p.status = c->d_status;
+    p.max_iter = vv_max_iterations(u);
+    p.node_touch = bits;
+    p.brick_touch = bits + nwords;
+    cudaError_t e = launch_raycast(c->fmt, p, c->stream);
+    std::vector<uint32_t> h(nwords + bwords);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), bits, h.size() * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(bits);
+    if (e != cudaSuccess) return cuda_fail(c, e, "footprint");
+    int64_t n = 0, b = 0;
+    for (size_t i = 0; i < nwords; ++i) n += __builtin_popcount(h[i]);
+    for (size_t i = 0; i < bwords; ++i) b += __builtin_popcount(h[nwords + i]);
+    if (nodes) *nodes = n;
+    if (bricks) *bricks = b;
     return VV_OK;
 }
 

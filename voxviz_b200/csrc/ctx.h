@@ -55,4 +55,8 @@ struct vv_ctx {
     size_t grid_words_cap = 0;
     void* h_stage = nullptr;
     size_t h_stage_cap = 0;
+    // profiling
+    bool profiling = false;
+    bool timed = false;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
 };

@@ -119,7 +119,9 @@ __device__ __forceinline__ Axis axis_taps(float u, float N, int n) {
     return a;
 }
 
-template <int FMT>
+__device__ __forceinline__ void touch(uint32_t* bits, uint32_t i) { atomicOr(bits + (i >> 5), 1u << (i & 31u)); }
+
+template <int FMT, bool COUNT>
 __device__ __forceinline__ float4 sample_brick(const RaycastParams& p, F3 uvw) {
     const float* N = p.u.brick_pool_dimension;
     const int nx = p.slots[0] * 10, ny = p.slots[1] * 10, nz = p.slots[2] * 10;
@@ -140,6 +142,13 @@ __device__ __forceinline__ float4 sample_brick(const RaycastParams& p, F3 uvw) {
     float4 v101 = Texel<FMT>::load(pool, idx(ax.s1, ax.l1, ay.s0, ay.l0, az.s1, az.l1));
     float4 v011 = Texel<FMT>::load(pool, idx(ax.s0, ax.l0, ay.s1, ay.l1, az.s1, az.l1));
     float4 v111 = Texel<FMT>::load(pool, idx(ax.s1, ax.l1, ay.s1, ay.l1, az.s1, az.l1));
+    if (COUNT) {
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t sx = (uint32_t)((k & 1) ? ax.s1 : ax.s0), sy = (uint32_t)((k & 2) ? ay.s1 : ay.s0),
+                           sz = (uint32_t)((k & 4) ? az.s1 : az.s0);
+            touch(p.brick_touch, (sz * SY + sy) * SX + sx);
+        }
+    }
     float4 c00 = lerp4(v000, v100, ax.f);
     float4 c10 = lerp4(v010, v110, ax.f);
     float4 c01 = lerp4(v001, v101, ax.f);
@@ -184,6 +193,7 @@ __device__ __forceinline__ bool inside_box(F3 p, F3 mn, F3 mx) {
     return p.x > mn.x && p.y > mn.y && p.z > mn.z && mx.x > p.x && mx.y > p.y && mx.z > p.z;
 }
 
+template <bool COUNT>
 __device__ __forceinline__ uint2 fetch_node(const RaycastParams& p, uint32_t x, uint32_t y, uint32_t z,
                                             bool& ok) {
     if (x >= (uint32_t)p.node_dim[0] || y >= (uint32_t)p.node_dim[1] || z >= (uint32_t)p.node_dim[2]) {
@@ -193,12 +203,13 @@ __device__ __forceinline__ uint2 fetch_node(const RaycastParams& p, uint32_t x, 
     const uint32_t bx = (uint32_t)p.node_dim[0] >> 1, by = (uint32_t)p.node_dim[1] >> 1;
     uint32_t blk = ((z >> 1) * by + (y >> 1)) * bx + (x >> 1);
     uint32_t idx = blk * 8u + ((x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2));
+    if (COUNT) touch(p.node_touch, idx);
     return __ldg(p.nodes + idx);
 }
 
 }  // namespace
 
-template <int FMT>
+template <int FMT, bool COUNT>
 __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ RaycastParams p) {
     const vv_uniforms& u = p.u;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -220,13 +231,12 @@ __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ Ra
     F3 pos;
     {
         const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
-        F3 P = f3(u.near_origin[0] + fx * u.near_dx[0] + fy * u.near_dy[0],
-                  u.near_origin[1] + fx * u.near_dx[1] + fy * u.near_dy[1],
-                  u.near_origin[2] + fx * u.near_dx[2] + fy * u.near_dy[2]);
+        const F3 d = f3(u.near_origin[0] + fx * u.near_dx[0] + fy * u.near_dy[0],
+                        u.near_origin[1] + fx * u.near_dx[1] + fy * u.near_dy[1],
+                        u.near_origin[2] + fx * u.near_dx[2] + fy * u.near_dy[2]);
         if (u.camera_inside) {
-            pos = P;
+            pos = add(C, d);
         } else {
-            const F3 d = sub(P, C);
             const float da[3] = {d.x, d.y, d.z}, ca[3] = {C.x, C.y, C.z};
             const float mn[3] = {vmin.x, vmin.y, vmin.z}, mx[3] = {vmax.x, vmax.y, vmax.z};
             float tenter = -INFINITY, texit = INFINITY;
@@ -276,7 +286,7 @@ __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ Ra
 
             bool ok = true;
             uint32_t nptr_x = 0, nptr_y = 0, nptr_z = 0;
-            const uint2 root = fetch_node(p, 0, 0, 0, ok);
+            const uint2 root = fetch_node<COUNT>(p, 0, 0, 0, ok);
             uint2 node = root;
             F3 ext_min = vmin, ext_max = vmax;
             float node_size = 1.0f;
@@ -355,7 +365,7 @@ __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ Ra
                                 pos = add(pos, muls(dir, (float)rem * step));
                                 break;
                             }
-                            float4 src = sample_brick<FMT>(p, bpos);
+                            float4 src = sample_brick<FMT, COUNT>(p, bpos);
                             src.w = 1.0f - (1.0f - src.w);
                             const float k = 1.0f - dst.w;
                             dst = make_float4(k * src.x + dst.x, k * src.y + dst.y, k * src.z + dst.z,
@@ -402,7 +412,7 @@ __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ Ra
                     ext_min = add(ext_min, muls(f3((float)ox, (float)oy, (float)oz), node_size));
                     ext_max = sub(ext_max, muls(f3(1.0f - (float)ox, 1.0f - (float)oy, 1.0f - (float)oz), node_size));
                     vhalf = vhalf * 0.5f;
-                    node = fetch_node(p, nptr_x, nptr_y, nptr_z, ok);
+                    node = fetch_node<COUNT>(p, nptr_x, nptr_y, nptr_z, ok);
                     if (!ok) {
                         set_status(p.status, VV_ERR_BOUNDS);
                         break;
@@ -423,13 +433,18 @@ __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ Ra
 cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s) {
     dim3 block(128);
     dim3 grid((unsigned)((p.u.width + 15) / 16), (unsigned)((p.u.height + 7) / 8));
+    const bool count = p.node_touch && p.brick_touch;
+#define VV_LAUNCH(F)                                                           \
+    if (count) raycast_kernel<F, true><<<grid, block, 0, s>>>(p);              \
+    else raycast_kernel<F, false><<<grid, block, 0, s>>>(p);
     switch (fmt) {
-        case VV_FMT_RGBA8: raycast_kernel<VV_FMT_RGBA8><<<grid, block, 0, s>>>(p); break;
-        case VV_FMT_FP16: raycast_kernel<VV_FMT_FP16><<<grid, block, 0, s>>>(p); break;
-        case VV_FMT_BF16: raycast_kernel<VV_FMT_BF16><<<grid, block, 0, s>>>(p); break;
-        case VV_FMT_FP32: raycast_kernel<VV_FMT_FP32><<<grid, block, 0, s>>>(p); break;
+        case VV_FMT_RGBA8: VV_LAUNCH(VV_FMT_RGBA8) break;
+        case VV_FMT_FP16: VV_LAUNCH(VV_FMT_FP16) break;
+        case VV_FMT_BF16: VV_LAUNCH(VV_FMT_BF16) break;
+        case VV_FMT_FP32: VV_LAUNCH(VV_FMT_FP32) break;
         default: return cudaErrorInvalidValue;
     }
+#undef VV_LAUNCH
     return cudaGetLastError();
 }
 

@@ -20,6 +20,8 @@ struct RaycastParams {
     uint4* usage;            // [H*W*3] (12 uint32 per pixel)
     int* status;             // sticky device status word
     int max_iter;            // bound on outer-loop iterations per ray
+    uint32_t* node_touch;    // footprint mode: bit per node (block-linear index)
+    uint32_t* brick_touch;   // footprint mode: bit per brick-pool slot
 };
 
 // Pyramid/compaction launch state.

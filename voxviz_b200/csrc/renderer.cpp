@@ -112,7 +112,8 @@ void compute_uniforms(int depth, bool root_is_constant, const vv_camera& cam, co
     double xmax, ymax;
     frustum_extent(cam, xmax, ymax);
     D3 right = left * -1.0;
-    D3 O = C + look * (double)cam.near_dist - right * xmax - up * ymax;
+    // camera-relative near-plane corner of window coordinate (0,0)
+    D3 O = look * (double)cam.near_dist - right * xmax - up * ymax;
     D3 dx = right * (2.0 * xmax / cam.width), dy = up * (2.0 * ymax / cam.height);
     const double o[3] = {O.x, O.y, O.z}, ddx[3] = {dx.x, dx.y, dx.z}, ddy[3] = {dy.x, dy.y, dy.z};
     for (int a = 0; a < 3; ++a) {

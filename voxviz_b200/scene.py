@@ -78,7 +78,7 @@ def terrain_height(heights: np.ndarray, x: float, y: float) -> float:
     return float(heights[j, i]) / n
 
 
-def seeded_view(seed: int, heights: np.ndarray, width: int, height: int, frame: int = 0, near: float = 1e-3):
+def seeded_view(seed: int, heights: np.ndarray, width: int, height: int, frame: int = 0, near: float = 0.05):
     """A seeded pinhole camera above the terrain looking at it."""
     rng = np.random.default_rng(seed)
     theta = rng.uniform(0, 2 * math.pi)
@@ -96,7 +96,7 @@ def _catmull_rom(p0, p1, p2, p3, t):
     return 0.5 * ((2 * p1) + (-p0 + p2) * t + (2 * p0 - 5 * p1 + 4 * p2 - p3) * t2 + (-p0 + 3 * p1 - 3 * p2 + p3) * t3)
 
 
-def camera_path(seed: int, heights: np.ndarray, frames: int, width: int, height: int, near: float = 1e-4,
+def camera_path(seed: int, heights: np.ndarray, frames: int, width: int, height: int, near: float = 0.005,
                 waypoints: int = 6):
     """A seeded low-altitude flight: a Catmull-Rom spline through seeded
     waypoints 1.05-1.3x the local terrain height, looking forward and down."""
