@@ -171,6 +171,8 @@ int vv_nodepool_patch(vv_ctx* ctx, int32_t tree, const vv_node_patch* patches,
                       int32_t n);
 /* Read the node pool back in reference texture order (for checking). */
 int vv_nodepool_download(vv_ctx* ctx, int32_t tree, uint32_t* words);
+/* Grid dimensions of octree slot `tree` (0,0,0 if none was uploaded). */
+int vv_nodepool_info(const vv_ctx* ctx, int32_t tree, int32_t dims[3]);
 
 /* ---- brick pool ----------------------------------------------------------- */
 
@@ -190,6 +192,8 @@ int vv_upload_bricks_device(vv_ctx* ctx, const uint32_t* slots_dev, int32_t n,
                             const void* texels_dev);
 /* Read the whole pool back (slot-major, brick-linear) into host memory. */
 int vv_brickpool_download(vv_ctx* ctx, void* texels);
+/* Slots per axis and format of the brick pool (0 slots if none exists). */
+int vv_brickpool_info(const vv_ctx* ctx, int32_t slots[3], int32_t* fmt);
 /* Device address of the pool texels (for callers that manage data on device). */
 int vv_brickpool_device_ptr(vv_ctx* ctx, void** ptr, size_t* bytes);
 

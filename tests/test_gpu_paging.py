@@ -24,7 +24,6 @@ def test_paged_camera_path_matches_oracle_and_policy(fmt):
     slots = scene.slot_grid(pool_bricks)
     ctx = vv.Context(0)
     r = vv.Renderer(ctx, o, fmt=fmt, pool_bytes=pool_bytes, preload_all=False, alpha_stop=0.99, jitter_seed=7)
-    ctx._node_dims = tuple(o.info.pool_dim)
     sim = PagingRef(o.node_words(), slots)
     sim.init(False)
     jit = vv.make_jitter(7)

@@ -29,12 +29,11 @@ def test_loop_bound_sets_timeout_status_and_matches_oracle():
 def test_out_of_range_patch_and_slot_are_reported():
     sc = helpers.Scene(seed=1, depth=3)
     g = helpers.GpuScene(sc)
-    before = g.ctx.download_nodes() if hasattr(g.ctx, "_node_dims") else None
+    before = g.ctx.download_nodes()
     g.ctx.patch_nodes(np.array([[5000, 0, 0, 1, 2]], dtype=np.uint32))
     g.ctx.synchronize()
     assert g.ctx.device_status() == vv._native.VV_ERR_BOUNDS
-    if before is not None:
-        assert np.array_equal(g.ctx.download_nodes(), before)
+    assert np.array_equal(g.ctx.download_nodes(), before)
     total = sc.slots[0] * sc.slots[1] * sc.slots[2]
     g.ctx.upload_bricks(np.array([total + 3], dtype=np.uint32), np.zeros((1, 4000), dtype=np.uint8))
     assert g.ctx.device_status() == vv._native.VV_ERR_BOUNDS

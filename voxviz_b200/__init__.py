@@ -182,8 +182,24 @@ class Context:
         h = C.c_void_p()
         _check(lib().vv_ctx_create(C.byref(p), C.byref(h)), what="ctx create")
         self._h = h
-        self.fmt = VV_FMT_RGBA8
-        self.slots = (0, 0, 0)
+
+    @property
+    def slots(self) -> tuple[int, int, int]:
+        """Brick-pool slots per axis (0,0,0 before vv_brickpool_create)."""
+        s, f = (C.c_int32 * 3)(), C.c_int32()
+        self._ck(lib().vv_brickpool_info(self._h, s, C.byref(f)), "brick pool info")
+        return int(s[0]), int(s[1]), int(s[2])
+
+    @property
+    def fmt(self) -> int:
+        s, f = (C.c_int32 * 3)(), C.c_int32()
+        self._ck(lib().vv_brickpool_info(self._h, s, C.byref(f)), "brick pool info")
+        return int(f.value)
+
+    def node_dims(self, tree: int = 0) -> tuple[int, int, int]:
+        d = (C.c_int32 * 3)()
+        self._ck(lib().vv_nodepool_info(self._h, tree, d), "node pool info")
+        return int(d[0]), int(d[1]), int(d[2])
 
     def close(self) -> None:
         if self._h:
@@ -218,10 +234,11 @@ class Context:
         w = np.ascontiguousarray(words, dtype=np.uint32)
         dz, dy, dx = w.shape[:3]
         self._ck(lib().vv_nodepool_upload(self._h, tree, _ptr(w), dx, dy, dz), "node upload")
-        self._node_dims = (dx, dy, dz)
 
     def download_nodes(self, tree: int = 0) -> np.ndarray:
-        dx, dy, dz = self._node_dims
+        dx, dy, dz = self.node_dims(tree)
+        if dx == 0:
+            raise VVError(N.VV_ERR_STATE, "node pool not uploaded")
         out = np.zeros((dz, dy, dx, 2), dtype=np.uint32)
         self._ck(lib().vv_nodepool_download(self._h, tree, _ptr(out)), "node download")
         return out
@@ -234,17 +251,19 @@ class Context:
     def create_brickpool(self, slots: Sequence[int], fmt="rgba8") -> None:
         f = fmt_code(fmt)
         self._ck(lib().vv_brickpool_create(self._h, int(slots[0]), int(slots[1]), int(slots[2]), f), "brick pool")
-        self.fmt = f
-        self.slots = tuple(int(s) for s in slots)
 
     def upload_bricks(self, slot_ids: np.ndarray, texels: np.ndarray) -> None:
         s = np.ascontiguousarray(slot_ids, dtype=np.uint32)
         t = np.ascontiguousarray(texels)
-        assert t.nbytes == s.size * 1000 * TEXEL_BYTES[self.fmt]
+        if t.nbytes != s.size * 1000 * TEXEL_BYTES[self.fmt]:
+            raise VVError(N.VV_ERR_ARG, "texels must hold 1000 texels per slot id in the pool's format")
         self._ck(lib().vv_upload_bricks(self._h, _ptr(s), s.size, _ptr(t)), "brick upload")
 
     def download_bricks(self) -> np.ndarray:
-        n = self.slots[0] * self.slots[1] * self.slots[2]
+        sx, sy, sz = self.slots
+        n = sx * sy * sz
+        if n == 0:
+            raise VVError(N.VV_ERR_STATE, "brick pool not created")
         out = np.zeros((n, 1000 * TEXEL_BYTES[self.fmt]), dtype=np.uint8)
         self._ck(lib().vv_brickpool_download(self._h, _ptr(out)), "brick download")
         return out
@@ -296,8 +315,6 @@ class Renderer:
         self.ctx = ctx
         self.octree = octree
         self.fmt = fmt_code(fmt)
-        ctx._node_dims = tuple(octree.info.pool_dim)
-        ctx.fmt = self.fmt
 
     def close(self) -> None:
         if self._h:

@@ -170,6 +170,8 @@ SIGNATURES = {
     "vv_upload_bricks": (C.c_int, [P, P, C.c_int32, P]),
     "vv_upload_bricks_device": (C.c_int, [P, P, C.c_int32, P]),
     "vv_brickpool_download": (C.c_int, [P, P]),
+    "vv_brickpool_info": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "vv_nodepool_info": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int32)]),
     "vv_brickpool_device_ptr": (C.c_int, [P, C.POINTER(P), C.POINTER(C.c_size_t)]),
     "vv_set_jitter": (C.c_int, [P, P, C.c_int32]),
     "vv_render": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(FrameOut)]),

@@ -295,6 +295,19 @@ int vv_brickpool_download(vv_ctx* c, void* texels) {
     return VV_OK;
 }
 
+int vv_brickpool_info(const vv_ctx* c, int32_t slots[3], int32_t* fmt) {
+    if (!c || !slots) return VV_ERR_ARG;
+    for (int a = 0; a < 3; ++a) slots[a] = c->bricks ? c->slots[a] : 0;
+    if (fmt) *fmt = c->fmt;
+    return VV_OK;
+}
+
+int vv_nodepool_info(const vv_ctx* c, int32_t tree, int32_t dims[3]) {
+    if (!c || !dims || tree < 0 || tree >= VV_MAX_TREES) return VV_ERR_ARG;
+    for (int a = 0; a < 3; ++a) dims[a] = c->trees[tree].nodes ? c->trees[tree].dim[a] : 0;
+    return VV_OK;
+}
+
 int vv_brickpool_device_ptr(vv_ctx* c, void** ptr, size_t* bytes) {
     if (!c || !ptr) return VV_ERR_ARG;
     *ptr = c->bricks;
