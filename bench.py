@@ -118,14 +118,19 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+RAYCAST_VERSION = "v1"  # bumped whenever the ray-cast kernel changes; the ncu capture must match
+
+
 def ncu_traffic():
-    """Per-launch DRAM bytes of the ray cast from the committed ncu summary, if any."""
+    """Per-launch DRAM bytes of the ray cast from the committed ncu summary,
+    when it was captured on the current kernel version."""
     p = ROOT / "profiles" / "raycast_paged_1080p_traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text())
+            d = json.loads(p.read_text())
         except ValueError:
             return None
+        return d if d.get("kernel_version") == RAYCAST_VERSION else None
     return None
 
 
@@ -265,13 +270,18 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = rays / (float(te.item()) / 1e3) / 1e6
+    # check frame: the next frame of the path drawn on the current pools (no
+    # update after it), so the downloaded pools are exactly what it read
+    r.draw(cams[frame % PATH_FRAMES])
+    chk_ray_ms, _ = ctx.last_times()
     ctx.set_profiling(False)
-    # roofline of the ray cast on the last timed frame
-    u_last = timed_u[-1]
+    u_last = r.last_uniforms()
+    # roofline of the ray cast: algorithmic bytes of the check frame (same
+    # path, same pools) over the mean launch duration of the timed region
     nodes, bricks = ctx.footprint(u_last)
     alg_bytes = 8 * nodes + 4000 * bricks + WIDTH * HEIGHT * (16 + 48)
     peak, peak_kind = measured_peaks()
-    achieved = alg_bytes / (ray_ms[-1] / 1e3) / 1e9
+    achieved = alg_bytes / (float(np.mean(ray_ms)) / 1e3) / 1e9
     traffic = ncu_traffic()
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
@@ -287,7 +297,10 @@ def run_ours(args):
                      "kernel": "raycast_kernel<RGBA8>",
                      "algorithmic_bytes": {"per_launch": int(alg_bytes), "nodes_touched": int(nodes),
                                            "bricks_touched": int(bricks),
-                                           "formula": "8*nodes + 4000*bricks + W*H*(16 colour + 48 usage)"}},
+                                           "formula": "8*nodes + 4000*bricks + W*H*(16 colour + 48 usage)",
+                                           "measured_on": "check frame after the timed region",
+                                           "check_frame_raycast_ms": round(chk_ray_ms, 3)},
+                     "traffic_source": (traffic or {}).get("source")},
         "kernels": {"raycast_ms_mean": round(float(np.mean(ray_ms)), 3),
                     "raycast_mrays_s": round(WIDTH * HEIGHT / (np.mean(ray_ms) / 1e3) / 1e6, 1),
                     "select_compact_ms_mean": round(float(np.mean(cmp_ms)), 3)},
@@ -305,7 +318,7 @@ def run_ours(args):
         jit = vv.make_jitter(JITTER_SEED)
         slots = tuple(int(v) // 10 for v in u_last.brick_pool_dimension)
         out["parity"] = parity_sample(r, ctx, u_last, words, pool, slots, 0, jit)
-        out["cpu_baseline"] = cpu_baseline(timed_u[-4:], words, pool, slots, 0, jit, args.cpu_seconds)
+        out["cpu_baseline"] = cpu_baseline([u_last] + timed_u[-3:], words, pool, slots, 0, jit, args.cpu_seconds)
     if rank == 0:
         print(json.dumps(out), flush=True)
     r.close()
