@@ -224,6 +224,7 @@ def run_ours(args):
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ray_ms, cmp_ms, uploads, requests = [], [], 0, 0
+    host_ms = {"ms_readback": 0.0, "ms_policy": 0.0, "ms_produce": 0.0, "ms_upload": 0.0}
     timed_u = []
     ev0.record()
     for _ in range(args.steps):
@@ -235,6 +236,8 @@ def run_ours(args):
         st = r.stats()
         uploads += st["bricks_uploaded"]
         requests += st["requests"]
+        for k in host_ms:
+            host_ms[k] += st[k]
         timed_u.append(r.last_uniforms())
         frame += 1
     ev1.record()
@@ -306,6 +309,7 @@ def run_ours(args):
                     "select_compact_ms_mean": round(float(np.mean(cmp_ms)), 3)},
         "paging": {"bricks_uploaded_per_frame": round(uploads / args.steps, 1),
                    "requests_per_frame": round(requests / args.steps, 1), "converge_draws": converge,
+                   "host_ms_per_frame": {k[3:]: round(v / args.steps, 3) for k, v in host_ms.items()},
                    "resident": r.stats()["resident_bricks"], "pool_slots": r.stats()["pool_slots"]},
         "clocks": clk, "gpu_launches": None, "setup_s": round(setup_s, 1),
     }

@@ -332,6 +332,11 @@ typedef struct vv_renderer_stats {
     int64_t resident_bricks;
     int64_t evictions_total;
     int32_t pool_slots;
+    /* host wall time of the last update, milliseconds */
+    float ms_readback;         /* request count + list read-back            */
+    float ms_policy;           /* decode, dedupe, LRU                        */
+    float ms_produce;          /* brick production on the host cores         */
+    float ms_upload;           /* brick upload + node patches                */
 } vv_renderer_stats;
 
 /* vox::Renderer lifecycle of the "gv" renderer (VoxVizCore/Renderer.h:20-110,

@@ -146,6 +146,10 @@ class RendererStats(C.Structure):
         ("resident_bricks", C.c_int64),
         ("evictions_total", C.c_int64),
         ("pool_slots", C.c_int32),
+        ("ms_readback", C.c_float),
+        ("ms_policy", C.c_float),
+        ("ms_produce", C.c_float),
+        ("ms_upload", C.c_float),
     ]
 
 

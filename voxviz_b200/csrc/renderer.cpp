@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -309,11 +310,15 @@ int GigaVoxelsRenderer::flush_uploads() {
         }
         unsigned char* st = (unsigned char*)h_stage_;
         const int fmt = d_.fmt;
+        const auto t0 = std::chrono::steady_clock::now();
 #pragma omp parallel for schedule(dynamic, 16) num_threads(d_.producer_threads > 0 ? d_.producer_threads : omp_get_max_threads())
         for (long i = 0; i < (long)n; ++i) tree_->produce_brick(pending_nodes_[(size_t)i], fmt, st + (size_t)i * bb);
+        const auto t1 = std::chrono::steady_clock::now();
+        ms_produce_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
         rc = vv_upload_bricks(ctx_, pending_slots_.data(), (int32_t)n, h_stage_);
         if (rc) return rc;
     }
+    const auto t2 = std::chrono::steady_clock::now();
     if (!touched_.empty()) {
         std::vector<vv_node_patch> patches;
         patches.reserve(touched_.size());
@@ -331,15 +336,18 @@ int GigaVoxelsRenderer::flush_uploads() {
     }
     pending_nodes_.clear();
     pending_slots_.clear();
+    ms_upload_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t2).count();
     return rc;
 }
 
 int GigaVoxelsRenderer::update() {
     if (!d_count) return VV_ERR_STATE;
     uploaded_ = 0;
+    ms_produce_ = 0.0f;
     uint32_t count = 0;
     if (cudaMemcpyAsync(&count, d_count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    const auto t0 = std::chrono::steady_clock::now();  // the draw has finished here
     active_ = count;
     const uint32_t n = std::min<uint32_t>(count, (uint32_t)cap_);
     req_count_ = n;
@@ -350,6 +358,8 @@ int GigaVoxelsRenderer::update() {
             return VV_ERR_CUDA;
         if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     }
+    const auto t1 = std::chrono::steady_clock::now();
+    ms_readback_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
     // NodeUsageListProcessor::run (GigaVoxelsOctTree.cpp:430-657): decode the
     // ids, keep the unique nodes in first-seen order, touch resident bricks,
     // queue non-constant non-resident nodes for upload.
@@ -383,6 +393,7 @@ int GigaVoxelsRenderer::update() {
             if (rc) return rc;
         }
     }
+    ms_policy_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
     return flush_uploads();
 }
 
@@ -395,6 +406,10 @@ void GigaVoxelsRenderer::stats(vv_renderer_stats& s) const {
     s.resident_bricks = resident_;
     s.evictions_total = evictions_;
     s.pool_slots = (int32_t)total_slots_;
+    s.ms_readback = ms_readback_;
+    s.ms_policy = ms_policy_;
+    s.ms_produce = ms_produce_;
+    s.ms_upload = ms_upload_;
 }
 
 void GigaVoxelsRenderer::residency(std::vector<uint32_t>& xyz, std::vector<uint32_t>& slot) const {

@@ -86,6 +86,7 @@ private:
     int64_t frame_ = -1;
     int32_t frame_for_compress_ = 0;
     int64_t req_count_ = 0, active_ = 0, uploaded_ = 0, uploaded_total_ = 0, evictions_ = 0, resident_ = 0;
+    float ms_readback_ = 0.f, ms_policy_ = 0.f, ms_produce_ = 0.f, ms_upload_ = 0.f;
     void* h_stage_ = nullptr;            // pinned brick staging
     size_t h_stage_cap_ = 0;
 };
