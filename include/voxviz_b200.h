@@ -224,6 +224,36 @@ int vv_ctx_last_times(vv_ctx* ctx, float* raycast_ms, float* compact_ms);
 int vv_measure_footprint(vv_ctx* ctx, int32_t tree, const vv_uniforms* u,
                          int64_t* nodes, int64_t* bricks);
 
+/* ---- page-request compaction without allocation ------------------------- */
+
+/* This entry point has no counterpart in the reference.  It is for callers
+ * that cannot call cudaMalloc: code that runs inside an allocator or a
+ * memory-pool callback, a real-time render thread that must not block on the
+ * driver's allocator, or a process whose device memory is owned by a
+ * framework that forbids side allocations.  It needs no vv_ctx.
+ *
+ * Given a frame's node-usage lists (`usage`, width*height*12 words on the
+ * device, as vv_render writes them) it writes the selection mask (`mask`,
+ * width*height words), the compacted page requests (`requests`,
+ * request_cap*4 words) and the active-pixel count (`request_count`, 1 word,
+ * may be NULL) on `cuda_stream` - the same results as vv_render with
+ * VV_PASS_SELECT | VV_PASS_COMPACT.  Inputs and outputs are the caller's; the
+ * histopyramid lives in a 16 MiB file-scope device array that every GPU
+ * loading the library holds until exit, so width*height may not exceed
+ * VV_NOALLOC_MAX_PIXELS (2^21, enough for 1920x1080); larger frames return
+ * VV_ERR_ARG.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current); make that first
+ * call before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (different streams, or different host threads on the
+ * same device) race and must be serialised by the caller.  It calls no
+ * cudaMalloc, cudaFree or allocating library routine.  Errors: VV_ERR_ARG,
+ * VV_ERR_CUDA; the message is in vv_last_error(NULL). */
+#define VV_NOALLOC_MAX_PIXELS (1 << 21)
+int vv_compact_requests_noalloc(const uint32_t* usage, uint32_t* mask, int32_t width,
+                                int32_t height, uint32_t* requests, uint32_t* request_count,
+                                int32_t request_cap, int32_t compress_max_push,
+                                void* cuda_stream);
+
 /* ---- host data model: terrain octree (GigaVoxelsOctTree) ----------------- */
 
 typedef struct vv_octree vv_octree;

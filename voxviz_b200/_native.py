@@ -179,6 +179,7 @@ SIGNATURES = {
     "vv_brickpool_device_ptr": (C.c_int, [P, C.POINTER(P), C.POINTER(C.c_size_t)]),
     "vv_set_jitter": (C.c_int, [P, P, C.c_int32]),
     "vv_render": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(FrameOut)]),
+    "vv_compact_requests_noalloc": (C.c_int, [P, P, C.c_int32, C.c_int32, P, P, C.c_int32, C.c_int32, P]),
     "vv_ctx_set_profiling": (C.c_int, [P, C.c_int32]),
     "vv_ctx_last_times": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "vv_measure_footprint": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(C.c_int64),

@@ -490,6 +490,8 @@ int vv_measure_footprint(vv_ctx* c, int32_t tree, const vv_uniforms* u, int64_t*
 
 namespace vv {
 
+void set_thread_error(const std::string& msg) { g_global_error = msg; }
+
 int vv_max_iterations(const vv_uniforms* u) {
     // Every leaf segment advances the ray by at least one half-voxel step of
     // the leaf level and a descent has at most depth+1 fetches, so a ray

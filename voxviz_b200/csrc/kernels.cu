@@ -595,6 +595,24 @@ __global__ void copy_total_kernel(const uint32_t* top, uint32_t* dst) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *dst = *top;
 }
 
+cudaError_t launch_pyramid_levels(uint32_t* counts, uint32_t* offsets, const int* lw, const int* lh,
+                                  const long long* loff, int first, int levels, cudaStream_t s) {
+    dim3 block(32, 4);
+    for (int l = first; l + 1 < levels; ++l) {
+        const int cw = lw[l + 1], ch = lh[l + 1];
+        dim3 grid((unsigned)((cw + 31) / 32), (unsigned)((ch + 3) / 4));
+        pyramid_up_kernel<<<grid, block, 0, s>>>(counts + loff[l], counts + loff[l + 1], lw[l], lh[l], cw, ch);
+    }
+    cudaError_t e = cudaMemsetAsync(offsets + loff[levels - 1], 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    for (int l = levels - 2; l >= first; --l) {
+        dim3 grid((unsigned)((lw[l] + 31) / 32), (unsigned)((lh[l] + 3) / 4));
+        pyramid_down_kernel<<<grid, block, 0, s>>>(counts + loff[l], offsets + loff[l], offsets + loff[l + 1], lw[l],
+                                                   lh[l], lw[l + 1], lh[l + 1]);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_compact(const CompactParams& p, cudaStream_t s) {
     dim3 block(32, 4);
     for (int l = 0; l + 1 < p.levels; ++l) {

@@ -44,6 +44,11 @@ cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s);
 cudaError_t launch_select(const uint4* usage, uint32_t* mask, uint32_t* level0, int w, int h,
                           cudaStream_t s);
 cudaError_t launch_compact(const CompactParams& p, cudaStream_t s);
+// Histopyramid up-sweep from level `first` to the top and down-sweep of the
+// exclusive offsets back to level `first` (level arrays at counts/offsets +
+// loff[l], dims lw[l] x lh[l]).
+cudaError_t launch_pyramid_levels(uint32_t* counts, uint32_t* offsets, const int* lw, const int* lh,
+                                  const long long* loff, int first, int levels, cudaStream_t s);
 cudaError_t launch_node_upload(const uint32_t* grid_words, uint2* nodes, const int dim[3],
                                cudaStream_t s);
 cudaError_t launch_node_download(const uint2* nodes, uint32_t* grid_words, const int dim[3],
