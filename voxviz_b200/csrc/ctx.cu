@@ -1,6 +1,7 @@
 // ctx.cu - device context, pools and the render entry point of the C ABI.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -41,12 +42,17 @@ size_t fmt_texel_bytes(int fmt) {
 }
 
 // Grow a device buffer to at least `bytes`.
+cudaError_t launch_raycast_any(vv_ctx* c, const RaycastParams& p) { return launch_raycast(c->fmt, p, c->stream); }
+
+// Grow a device buffer to at least `bytes` (geometrically, so that a run of
+// slowly growing requests does not re-allocate every call).
 int ensure(vv_ctx* c, void** ptr, size_t* cap, size_t bytes, const char* what) {
     if (*cap >= bytes && *ptr) return VV_OK;
+    const size_t grown = *cap * 2;
     if (*ptr) cudaFree(*ptr);
     *ptr = nullptr;
     *cap = 0;
-    size_t want = std::max(bytes, (size_t)256);
+    size_t want = std::max(std::max(bytes, grown), (size_t)256);
     cudaError_t e = cudaMalloc(ptr, want);
     if (e != cudaSuccess) {
         *ptr = nullptr;
@@ -58,10 +64,11 @@ int ensure(vv_ctx* c, void** ptr, size_t* cap, size_t bytes, const char* what) {
 
 int ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes) {
     if (*cap >= bytes && *ptr) return VV_OK;
+    const size_t grown = *cap * 2;
     if (*ptr) cudaFreeHost(*ptr);
     *ptr = nullptr;
     *cap = 0;
-    size_t want = std::max(bytes, (size_t)4096);
+    size_t want = std::max(std::max(bytes, grown), (size_t)4096);
     cudaError_t e = cudaMallocHost(ptr, want);
     if (e != cudaSuccess) {
         *ptr = nullptr;
@@ -368,7 +375,7 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         p.usage = usage;
         p.status = c->d_status;
         p.max_iter = vv_max_iterations(u);
-        VV_CUDA(c, launch_raycast(c->fmt, p, c->stream));
+        VV_CUDA(c, launch_raycast_any(c, p));
     }
     if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
     if (!(passes & (VV_PASS_SELECT | VV_PASS_COMPACT))) {
@@ -472,7 +479,7 @@ int vv_measure_footprint(vv_ctx* c, int32_t tree, const vv_uniforms* u, int64_t*
     p.max_iter = vv_max_iterations(u);
     p.node_touch = bits;
     p.brick_touch = bits + nwords;
-    cudaError_t e = launch_raycast(c->fmt, p, c->stream);
+    cudaError_t e = launch_raycast_any(c, p);
     std::vector<uint32_t> h(nwords + bwords);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), bits, h.size() * 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

@@ -163,6 +163,41 @@ __device__ __forceinline__ float4 sample_brick(const RaycastParams& p, F3 uvw) {
     return c;
 }
 
+// Trilinear sample when all 8 taps lie in the brick-pool slot whose first
+// texel per axis is base[]; returns false (and nothing) otherwise.  Same
+// arithmetic as sample_brick: only the texel addressing is shorter.
+template <int FMT>
+__device__ __forceinline__ bool sample_in_slot(const RaycastParams& p, F3 uvw, const int base[3], uint32_t slot_texel0,
+                                               float4& out) {
+    const float* N = p.u.brick_pool_dimension;
+    const float ta[3] = {uvw.x * N[0] - 0.5f, uvw.y * N[1] - 0.5f, uvw.z * N[2] - 0.5f};
+    float f[3];
+    int l[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float fi = floorf(ta[a]);
+        f[a] = ta[a] - fi;
+        l[a] = (int)fi - base[a];
+    }
+    if ((unsigned)l[0] > 8u || (unsigned)l[1] > 8u || (unsigned)l[2] > 8u) return false;
+    const uint32_t i000 = slot_texel0 + (uint32_t)((l[2] * 10 + l[1]) * 10 + l[0]);
+    const void* pool = p.bricks;
+    const float4 v000 = Texel<FMT>::load(pool, i000), v100 = Texel<FMT>::load(pool, i000 + 1u);
+    const float4 v010 = Texel<FMT>::load(pool, i000 + 10u), v110 = Texel<FMT>::load(pool, i000 + 11u);
+    const float4 v001 = Texel<FMT>::load(pool, i000 + 100u), v101 = Texel<FMT>::load(pool, i000 + 101u);
+    const float4 v011 = Texel<FMT>::load(pool, i000 + 110u), v111 = Texel<FMT>::load(pool, i000 + 111u);
+    const float4 c0 = lerp4(lerp4(v000, v100, f[0]), lerp4(v010, v110, f[0]), f[1]);
+    const float4 c1 = lerp4(lerp4(v001, v101, f[0]), lerp4(v011, v111, f[0]), f[1]);
+    float4 c = lerp4(c0, c1, f[2]);
+    if (Texel<FMT>::kScale != 1.0f) {
+        const float k = Texel<FMT>::kScale;
+        c = make_float4(c.x * k, c.y * k, c.z * k, c.w * k);
+    }
+    out = c;
+    return true;
+}
+
+
 // ComputeMinRayBoxIntersection (GigaVoxelsNoLighting.frag:124-180): exit
 // time over the planes facing away from the ray, 4.0 if none, t == 0 ignored.
 __device__ __forceinline__ float min_exit(F3 p, F3 d, F3 mn, F3 mx) {
@@ -297,108 +332,38 @@ __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ Ra
             int depth = 0, brick_depth = 0;
             int nl_count = 0, pushed = 0;
             int iter = 0;
+            // Segment-synchronous ("while-while") form: the descent to the
+            // stopping node is its own loop, then the segment is marched.  Lanes of
+            // a warp descend together and march together, which keeps far more of
+            // them converged than alternating single levels with whole segments.
+            bool failed = false;
             while (inside) {
-                if (++iter > p.max_iter) {
-                    set_status(p.status, VV_ERR_TIMEOUT);
-                    break;
-                }
-                const bool is_const = (node.x & kConstant) != 0u;
-                const bool loaded = (node.x & kResident) != 0u;
-                if (loaded) {
-                    cur_brick = node;
-                    cur_brp = rbp;
-                    brick_depth = depth;
-                }
-                // ComputeVoxelSize (:429-441) * LodScalar
-                float proj;
-                {
-                    const F3 uh = muls(up, vhalf), lh = muls(left, vhalf);
-                    const F3 ll = normalize3(sub(add(sub(pos, uh), lh), C));
-                    const F3 ur = normalize3(sub(sub(add(pos, uh), lh), C));
-                    proj = (1.0f - dot3(ll, ur)) * u.lod_scalar;
-                }
-                const uint32_t cx = (node.x >> 20) & 0x3FFu, cy = (node.x >> 10) & 0x3FFu, cz = node.x & 0x3FFu;
-                if ((!is_const && !loaded) || u.pixel_size > proj || (cx == 0u && cy == 0u && cz == 0u)) {
-                    if (is_const) {
-                        // TraverseConstant (:230-282)
-                        const float ratio = ldexpf(1.0f, L - depth);
-                        const float step = RS * ratio;
-                        const float4 cv = make_float4((float)(node.y & 255u) / 255.0f,
-                                                      (float)((node.y >> 8) & 255u) / 255.0f,
-                                                      (float)((node.y >> 16) & 255u) / 255.0f,
-                                                      (float)(node.y >> 24) / 255.0f);
-                        const float t = min_exit(pos, dir, ext_min, ext_max);
-                        int n = (int)(t / step) + 1;
-                        if (cv.w < 0.005f) {
-                            pos = add(pos, muls(dir, (float)n * step));
-                        } else {
-                            const F3 wstep = muls(dir, step);
-                            const float sa = 1.0f - pow_pow2(1.0f - cv.w, L - depth);
-                            const float4 src = make_float4(cv.x * ratio, cv.y * ratio, cv.z * ratio, sa);
-                            for (int i = 0; i < n; ++i) {
-                                pos = add(pos, wstep);
-                                if (dst.w > astop) {
-                                    const int rem = n - (i + 1);
-                                    pos = add(pos, muls(dir, (float)rem * step));
-                                    break;
-                                }
-                                const float k = 1.0f - dst.w;
-                                dst = make_float4(k * src.x + dst.x, k * src.y + dst.y, k * src.z + dst.z,
-                                                  k * src.w + dst.w);
-                            }
-                        }
-                    } else {
-                        // TraverseBrick (:311-359) over the most recently found brick
-                        const uint32_t bw = cur_brick.y;
-                        const F3 bptr = f3((float)((bw >> 20) & 0x3FFu) / pdim.x, (float)((bw >> 10) & 0x3FFu) / pdim.y,
-                                           (float)(bw & 0x3FFu) / pdim.z);
-                        F3 bpos = add(bptr, divv(mul(cur_brp, bdim), pdim));
-                        const float ratio = ldexpf(1.0f, L - brick_depth);
-                        const F3 wstep = muls(muls(dir, RS), ratio);
-                        const float t = min_exit(pos, dir, ext_min, ext_max);
-                        const float step = RS * ratio;
-                        const int n = (int)(t / step) + 1;
-                        for (int i = 0; i < n; ++i) {
-                            pos = add(pos, wstep);
-                            if (dst.w > astop) {
-                                const int rem = n - (i + 1);
-                                pos = add(pos, muls(dir, (float)rem * step));
-                                break;
-                            }
-                            float4 src = sample_brick<FMT, COUNT>(p, bpos);
-                            src.w = 1.0f - (1.0f - src.w);
-                            const float k = 1.0f - dst.w;
-                            dst = make_float4(k * src.x + dst.x, k * src.y + dst.y, k * src.z + dst.z,
-                                              k * src.w + dst.w);
-                            bpos = add(bpos, brick_step);
-                        }
+                // ---- descent from the root to the node that stops it (:563-622, :722-746)
+                bool is_const, loaded;
+                for (;;) {
+                    if (++iter > p.max_iter) {
+                        set_status(p.status, VV_ERR_TIMEOUT);
+                        failed = true;
+                        break;
                     }
-                    // AddToNodeUsageList (:454-488)
-                    if (nl_count >= start_push && nl_count < stop_push && pushed < u.max_nodes_to_push) {
-                        ++pushed;
-                        const uint32_t bits = ((nptr_x + 1u) << 20) | ((nptr_y + 1u) << 10) | (nptr_z + 1u);
-#pragma unroll
-                        for (int i = 0; i < 12; ++i)
-                            if (i == list_slot) usage[i] = bits;
-                        list_slot = list_slot == 11 ? 0 : list_slot + 1;
+                    is_const = (node.x & kConstant) != 0u;
+                    loaded = (node.x & kResident) != 0u;
+                    if (loaded) {
+                        cur_brick = node;
+                        cur_brp = rbp;
+                        brick_depth = depth;
                     }
-                    if (dst.w > astop && (is_const || loaded)) break;
-                    // restart from the root (:688-720); the node pointer keeps its value
-                    node = root;
-                    ext_min = vmin;
-                    ext_max = vmax;
-                    node_size = 1.0f;
-                    vhalf = u.root_voxel_half_size;
-                    rbp = pos;
-                    cur_brp = pos;
-                    cur_brick = root;
-                    depth = 0;
-                    brick_depth = 0;
-                    inside = inside_box(pos, vmin, vmax);
-                    ++nl_count;
-                    if (nl_count >= 48) nl_count = 0;
-                } else {
-                    // descend (:722-746)
+                    const uint32_t cx = (node.x >> 20) & 0x3FFu, cy = (node.x >> 10) & 0x3FFu, cz = node.x & 0x3FFu;
+                    if ((!is_const && !loaded) || (cx == 0u && cy == 0u && cz == 0u)) break;
+                    // ComputeVoxelSize (:429-441) * LodScalar, only when the other
+                    // two stop conditions do not decide (it has no side effects)
+                    {
+                        const F3 uh = muls(up, vhalf), lh = muls(left, vhalf);
+                        const F3 ll = normalize3(sub(add(sub(pos, uh), lh), C));
+                        const F3 ur = normalize3(sub(sub(add(pos, uh), lh), C));
+                        const float proj = (1.0f - dot3(ll, ur)) * u.lod_scalar;
+                        if (u.pixel_size > proj) break;
+                    }
                     const F3 boff = muls(rbp, 2.0f);
                     const uint32_t ox = boff.x >= 1.0f ? 1u : 0u;
                     const uint32_t oy = boff.y >= 1.0f ? 1u : 0u;
@@ -415,9 +380,102 @@ __global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ Ra
                     node = fetch_node<COUNT>(p, nptr_x, nptr_y, nptr_z, ok);
                     if (!ok) {
                         set_status(p.status, VV_ERR_BOUNDS);
+                        failed = true;
                         break;
                     }
                 }
+                if (failed) break;
+                // ---- the leaf segment
+                if (is_const) {
+                    // TraverseConstant (:230-282)
+                    const float ratio = ldexpf(1.0f, L - depth);
+                    const float step = RS * ratio;
+                    const float aw = (float)(node.y >> 24) / 255.0f;
+                    const float t = min_exit(pos, dir, ext_min, ext_max);
+                    const int n = (int)(t / step) + 1;
+                    if (aw < 0.005f) {
+                        pos = add(pos, muls(dir, (float)n * step));
+                    } else {
+                        const F3 wstep = muls(dir, step);
+                        const float sa = 1.0f - pow_pow2(1.0f - aw, L - depth);
+                        const float4 src = make_float4((float)(node.y & 255u) / 255.0f * ratio,
+                                                       (float)((node.y >> 8) & 255u) / 255.0f * ratio,
+                                                       (float)((node.y >> 16) & 255u) / 255.0f * ratio, sa);
+                        for (int i = 0; i < n; ++i) {
+                            pos = add(pos, wstep);
+                            if (dst.w > astop) {
+                                const int rem = n - (i + 1);
+                                pos = add(pos, muls(dir, (float)rem * step));
+                                break;
+                            }
+                            const float k = 1.0f - dst.w;
+                            dst = make_float4(k * src.x + dst.x, k * src.y + dst.y, k * src.z + dst.z,
+                                              k * src.w + dst.w);
+                        }
+                    }
+                } else {
+                    // TraverseBrick (:311-359) over the most recently found brick
+                    const uint32_t bw = cur_brick.y;
+                    const F3 bptr = f3((float)((bw >> 20) & 0x3FFu) / pdim.x, (float)((bw >> 10) & 0x3FFu) / pdim.y,
+                                       (float)(bw & 0x3FFu) / pdim.z);
+                    F3 bpos = add(bptr, divv(mul(cur_brp, bdim), pdim));
+                    const float ratio = ldexpf(1.0f, L - brick_depth);
+                    const F3 wstep = muls(muls(dir, RS), ratio);
+                    const float t = min_exit(pos, dir, ext_min, ext_max);
+                    const float step = RS * ratio;
+                    const int n = (int)(t / step) + 1;
+                    // taps inside this brick's slot skip the general texel addressing
+                    int base[3] = {(int)((bw >> 20) & 0x3FFu) - 1, (int)((bw >> 10) & 0x3FFu) - 1,
+                                   (int)(bw & 0x3FFu) - 1};
+                    uint32_t slot_texel0 = 0u;
+                    if (base[0] >= 0 && base[1] >= 0 && base[2] >= 0 && base[0] % 10 == 0 && base[1] % 10 == 0 &&
+                        base[2] % 10 == 0 && base[0] < p.slots[0] * 10 && base[1] < p.slots[1] * 10 &&
+                        base[2] < p.slots[2] * 10) {
+                        slot_texel0 = (((uint32_t)base[2] / 10u * (uint32_t)p.slots[1] + (uint32_t)base[1] / 10u) *
+                                           (uint32_t)p.slots[0] + (uint32_t)base[0] / 10u) * 1000u;
+                    } else {
+                        base[0] = base[1] = base[2] = -100000;
+                    }
+                    for (int i = 0; i < n; ++i) {
+                        pos = add(pos, wstep);
+                        if (dst.w > astop) {
+                            const int rem = n - (i + 1);
+                            pos = add(pos, muls(dir, (float)rem * step));
+                            break;
+                        }
+                        float4 src;
+                        if (COUNT || !sample_in_slot<FMT>(p, bpos, base, slot_texel0, src))
+                            src = sample_brick<FMT, COUNT>(p, bpos);
+                        src.w = 1.0f - (1.0f - src.w);
+                        const float k = 1.0f - dst.w;
+                        dst = make_float4(k * src.x + dst.x, k * src.y + dst.y, k * src.z + dst.z, k * src.w + dst.w);
+                        bpos = add(bpos, brick_step);
+                    }
+                }
+                // AddToNodeUsageList (:454-488)
+                if (nl_count >= start_push && nl_count < stop_push && pushed < u.max_nodes_to_push) {
+                    ++pushed;
+                    const uint32_t bits = ((nptr_x + 1u) << 20) | ((nptr_y + 1u) << 10) | (nptr_z + 1u);
+#pragma unroll
+                    for (int i = 0; i < 12; ++i)
+                        if (i == list_slot) usage[i] = bits;
+                    list_slot = list_slot == 11 ? 0 : list_slot + 1;
+                }
+                if (dst.w > astop && (is_const || loaded)) break;
+                // restart from the root (:688-720); the node pointer keeps its value
+                node = root;
+                ext_min = vmin;
+                ext_max = vmax;
+                node_size = 1.0f;
+                vhalf = u.root_voxel_half_size;
+                rbp = pos;
+                cur_brp = pos;
+                cur_brick = root;
+                depth = 0;
+                brick_depth = 0;
+                inside = inside_box(pos, vmin, vmax);
+                ++nl_count;
+                if (nl_count >= 48) nl_count = 0;
             }
         }
     }
