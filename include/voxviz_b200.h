@@ -351,6 +351,9 @@ typedef struct vv_renderer_desc {
     uint32_t jitter_seed;
     int32_t max_width, max_height;
     int32_t producer_threads;  /* host brick producers (0 = all cores)      */
+    int32_t device_paging;     /* 1: de-duplicate requests and produce bricks
+                                  on the GPU (same policy and results; the
+                                  host keeps only the LRU list)             */
 } vv_renderer_desc;
 
 typedef struct vv_renderer_stats {

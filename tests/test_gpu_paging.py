@@ -14,8 +14,9 @@ from tests import helpers
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("fmt", ["rgba8", "fp16"])
-def test_paged_camera_path_matches_oracle_and_policy(fmt):
+@pytest.mark.parametrize("fmt,device_paging", [("rgba8", False), ("fp16", False), ("rgba8", True),
+                                               ("bf16", True)])
+def test_paged_camera_path_matches_oracle_and_policy(fmt, device_paging):
     depth, W, H, frames = 6, 256, 160, 12
     o = helpers.octree(seed=3, depth=depth)
     f = vv.fmt_code(fmt)
@@ -23,7 +24,8 @@ def test_paged_camera_path_matches_oracle_and_policy(fmt):
     pool_bytes = pool_bricks * 1000 * vv.TEXEL_BYTES[f]
     slots = scene.slot_grid(pool_bricks)
     ctx = vv.Context(0)
-    r = vv.Renderer(ctx, o, fmt=fmt, pool_bytes=pool_bytes, preload_all=False, alpha_stop=0.99, jitter_seed=7)
+    r = vv.Renderer(ctx, o, fmt=fmt, pool_bytes=pool_bytes, preload_all=False, alpha_stop=0.99, jitter_seed=7,
+                    device_paging=device_paging)
     sim = PagingRef(o.node_words(), slots)
     sim.init(False)
     jit = vv.make_jitter(7)

@@ -304,10 +304,11 @@ class Renderer:
 
     def __init__(self, ctx: Context, octree: Octree, fmt="rgba8", pool_bytes: int = 0, preload_all: bool = True,
                  request_cap: int = 0, lod_scalar: float = 1.0, alpha_stop: float = 0.99, jitter_seed: int = 7,
-                 producer_threads: int = 0):
+                 producer_threads: int = 0, device_paging: bool = False):
         d = N.RendererDesc(fmt=fmt_code(fmt), pool_bytes=pool_bytes, preload_all=1 if preload_all else 0,
                            request_cap=request_cap, lod_scalar=lod_scalar, alpha_stop=alpha_stop,
-                           jitter_seed=jitter_seed, max_width=0, max_height=0, producer_threads=producer_threads)
+                           jitter_seed=jitter_seed, max_width=0, max_height=0, producer_threads=producer_threads,
+                           device_paging=1 if device_paging else 0)
         h = C.c_void_p()
         _check(lib().vv_renderer_create(ctx.handle, octree.handle, C.byref(d), C.byref(h)), ctx.handle,
                "renderer create")

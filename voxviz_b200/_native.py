@@ -133,6 +133,7 @@ class RendererDesc(C.Structure):
         ("max_width", C.c_int32),
         ("max_height", C.c_int32),
         ("producer_threads", C.c_int32),
+        ("device_paging", C.c_int32),
     ]
 
 

@@ -217,7 +217,9 @@ int vv_renderer_read_lists(vv_renderer* r, uint32_t* host_usage, uint32_t* host_
 
 int vv_renderer_last_requests(const vv_renderer* r, uint32_t* out, int32_t cap, int32_t* n) {
     if (!r || !n) return VV_ERR_ARG;
-    const auto& q = r->impl->last_requests();
+    std::vector<uint32_t> q;
+    const int rc = const_cast<vv_renderer*>(r)->impl->last_requests(q);
+    if (rc) return rc;
     const int32_t cnt = (int32_t)(q.size() / 4);
     *n = cnt;
     if (out) std::memcpy(out, q.data(), (size_t)std::min(cnt, cap) * 16);

@@ -1,0 +1,225 @@
+// production.cu - GPU brick production and request de-duplication.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstring>
+
+#include "../../include/voxviz_b200.h"
+#include "production.h"
+#include "terrain.h"
+
+namespace vv {
+
+DeviceTerrain::~DeviceTerrain() {
+    for (void* p : allocs_) cudaFree(p);
+}
+
+void* DeviceTerrain::alloc_copy(const void* src, size_t bytes, cudaError_t& e) {
+    if (e != cudaSuccess) return nullptr;
+    void* p = nullptr;
+    e = cudaMalloc(&p, bytes ? bytes : 4);
+    if (e != cudaSuccess) return nullptr;
+    allocs_.push_back(p);
+    bytes_ += bytes;
+    if (bytes) e = cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    return p;
+}
+
+cudaError_t DeviceTerrain::upload(const TerrainVolume& vol) {
+    cudaError_t e = cudaSuccess;
+    v_.depth = vol.depth();
+    for (int b = 0; b < 8; ++b) v_.band[b] = band_colour(b);
+    for (int m = 0; m <= vol.depth(); ++m) {
+        const MipLevel& L = vol.mip(m);
+        DeviceMipLevel& d = v_.lv[m];
+        d.dim = L.dim;
+        d.s = (const uint16_t*)alloc_copy(L.s.data(), L.s.size() * sizeof(uint16_t), e);
+        if (m == 0) {  // the leaf level has no explicit voxels
+            d.r = nullptr;
+            d.off = nullptr;
+            d.data = nullptr;
+            continue;
+        }
+        d.r = (const uint16_t*)alloc_copy(L.r.data(), L.r.size() * sizeof(uint16_t), e);
+        std::vector<uint32_t> off32(L.off.size());
+        for (size_t i = 0; i < off32.size(); ++i) off32[i] = (uint32_t)L.off[i];
+        d.off = (const uint32_t*)alloc_copy(off32.data(), off32.size() * sizeof(uint32_t), e);
+        d.data = (const uint32_t*)alloc_copy(L.data.data(), L.data.size() * sizeof(uint32_t), e);
+    }
+    return e;
+}
+
+namespace {
+
+template <int FMT>
+__device__ __forceinline__ void store_texel(void* pool, size_t i, uint32_t v) {
+    if (FMT == VV_FMT_RGBA8) {
+        ((uint32_t*)pool)[i] = v;
+        return;
+    }
+    // the same v/255 values as the host producer, rounded to nearest even
+    const float c0 = (float)(v & 255u) / 255.0f, c1 = (float)((v >> 8) & 255u) / 255.0f;
+    const float c2 = (float)((v >> 16) & 255u) / 255.0f, c3 = (float)(v >> 24) / 255.0f;
+    if (FMT == VV_FMT_FP32) {
+        ((float4*)pool)[i] = make_float4(c0, c1, c2, c3);
+    } else if (FMT == VV_FMT_FP16) {
+        const uint32_t a = (uint32_t)__half_as_ushort(__float2half_rn(c0)) |
+                           ((uint32_t)__half_as_ushort(__float2half_rn(c1)) << 16);
+        const uint32_t b = (uint32_t)__half_as_ushort(__float2half_rn(c2)) |
+                           ((uint32_t)__half_as_ushort(__float2half_rn(c3)) << 16);
+        ((uint2*)pool)[i] = make_uint2(a, b);
+    } else {
+        const uint32_t a = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(c0)) |
+                           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(c1)) << 16);
+        const uint32_t b = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(c2)) |
+                           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(c3)) << 16);
+        ((uint2*)pool)[i] = make_uint2(a, b);
+    }
+}
+
+// One CTA per brick.  Texel (bx,by,bz) of node (d; i,j,k) is the mip-level
+// (L-d) voxel (8i-1+bx, 8j-1+by, 8k-1+bz), transparent black outside the level.
+template <int FMT>
+__global__ void produce_kernel(const __grid_constant__ DeviceTerrainView t, const uint4* __restrict__ jobs,
+                               void* __restrict__ pool, long long total_slots, int* status) {
+    const uint4 job = jobs[blockIdx.x];
+    if ((long long)job.x >= total_slots || (int)job.y > t.depth) {
+        if (threadIdx.x == 0 && status) atomicCAS(status, 0, VV_ERR_BOUNDS);
+        return;
+    }
+    const int m = t.depth - (int)job.y;
+    const DeviceMipLevel L = t.lv[m];
+    const int i = (int)((job.z >> 20) & 1023u), j = (int)((job.z >> 10) & 1023u), k = (int)(job.z & 1023u);
+    const size_t base = (size_t)job.x * 1000u;
+    for (int q = threadIdx.x; q < 1000; q += blockDim.x) {
+        const int bz = q / 100, by = (q / 10) % 10, bx = q % 10;
+        const int x = 8 * i - 1 + bx, y = 8 * j - 1 + by, z = 8 * k - 1 + bz;
+        uint32_t v = 0u;
+        if (x >= 0 && y >= 0 && z >= 0 && x < L.dim && y < L.dim && z < L.dim) {
+            const size_t c = (size_t)y * L.dim + x;
+            const int s = L.s[c];
+            if (z < s) {
+                v = t.band[((z << m) >> t.depth) & 7];
+            } else if (L.r) {
+                const int r = L.r[c];
+                if (z < s + r) v = L.data[L.off[c] + (uint32_t)(z - s)];
+            }
+        }
+        store_texel<FMT>(pool, base + (size_t)q, v);
+    }
+}
+
+__device__ __forceinline__ bool decode_cell(uint32_t id, int dx, int dy, int dz, uint32_t& g) {
+    if (id == 0u) return false;
+    const uint32_t x = ((id >> 20) & 0x3FFu) - 1u, y = ((id >> 10) & 0x3FFu) - 1u, z = (id & 0x3FFu) - 1u;
+    if (x >= (uint32_t)dx || y >= (uint32_t)dy || z >= (uint32_t)dz) return false;
+    g = (z * (uint32_t)dy + y) * (uint32_t)dx + x;
+    return true;
+}
+
+__global__ void dedupe_first_kernel(const uint32_t* __restrict__ ids, int n, int dx, int dy, int dz,
+                                    uint32_t* __restrict__ first) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    uint32_t g;
+    if (decode_cell(ids[q], dx, dy, dz, g)) atomicMin(first + g, (uint32_t)q);
+}
+
+__global__ void __launch_bounds__(1024) dedupe_count_kernel(const uint32_t* __restrict__ ids, int n, int dx, int dy,
+                                                            int dz, const uint32_t* __restrict__ first,
+                                                            uint32_t* __restrict__ block_sums) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t g = 0;
+    const bool f = q < n && decode_cell(ids[q], dx, dy, dz, g) && first[g] == (uint32_t)q;
+    const int c = __syncthreads_count(f);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = (uint32_t)c;
+}
+
+// Exclusive scan of the block sums in place, total to *count (one CTA).
+__global__ void __launch_bounds__(1024) scan_sums_kernel(uint32_t* __restrict__ sums, int nb,
+                                                         uint32_t* __restrict__ count) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0u;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < nb; base += 1024) {
+        const int i = base + (int)threadIdx.x;
+        const uint32_t v = i < nb ? sums[i] : 0u;
+        uint32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = warp_tot[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_tot[lane] = w;  // inclusive
+        }
+        __syncthreads();
+        const uint32_t before = carry + (warp > 0 ? warp_tot[warp - 1] : 0u) + (x - v);
+        if (i < nb) sums[i] = before;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_tot[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = carry;
+}
+
+__global__ void __launch_bounds__(1024) dedupe_scatter_kernel(const uint32_t* __restrict__ ids, int n, int dx,
+                                                              int dy, int dz, uint32_t* __restrict__ first,
+                                                              const uint32_t* __restrict__ block_off,
+                                                              uint32_t* __restrict__ out) {
+    __shared__ uint32_t warp_cnt[32];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t g = 0;
+    const bool f = q < n && decode_cell(ids[q], dx, dy, dz, g) && first[g] == (uint32_t)q;
+    const unsigned b = __ballot_sync(0xFFFFFFFFu, f);
+    if (lane == 0) warp_cnt[warp] = (uint32_t)__popc(b);
+    __syncthreads();
+    if (f) {
+        uint32_t off = block_off[blockIdx.x];
+        for (int w = 0; w < warp; ++w) off += warp_cnt[w];
+        off += (uint32_t)__popc(b & ((1u << lane) - 1u));
+        out[off] = g;
+        first[g] = 0xFFFFFFFFu;  // ready for the next frame
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs, int n, void* pool, int fmt,
+                                  long long total_slots, int* status, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    switch (fmt) {
+        case VV_FMT_RGBA8: produce_kernel<VV_FMT_RGBA8><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
+        case VV_FMT_FP16: produce_kernel<VV_FMT_FP16><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
+        case VV_FMT_BF16: produce_kernel<VV_FMT_BF16><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
+        case VV_FMT_FP32: produce_kernel<VV_FMT_FP32><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dedupe(const uint32_t* requests, int n_entries, const int grid_dim[3], const DedupeBuffers& b,
+                          cudaStream_t s) {
+    const int n = 4 * n_entries;
+    if (n <= 0) return cudaMemsetAsync(b.count, 0, sizeof(uint32_t), s);
+    const int nb = (n + 1023) / 1024;
+    if ((size_t)nb > b.block_cap || (size_t)n > b.unique_cap) return cudaErrorInvalidValue;
+    dedupe_first_kernel<<<(n + 255) / 256, 256, 0, s>>>(requests, n, grid_dim[0], grid_dim[1], grid_dim[2], b.first);
+    dedupe_count_kernel<<<nb, 1024, 0, s>>>(requests, n, grid_dim[0], grid_dim[1], grid_dim[2], b.first,
+                                            b.block_sums);
+    scan_sums_kernel<<<1, 1024, 0, s>>>(b.block_sums, nb, b.count);
+    dedupe_scatter_kernel<<<nb, 1024, 0, s>>>(requests, n, grid_dim[0], grid_dim[1], grid_dim[2], b.first,
+                                              b.block_sums, b.unique);
+    return cudaGetLastError();
+}
+
+}  // namespace vv

@@ -160,6 +160,9 @@ GigaVoxelsRenderer::~GigaVoxelsRenderer() {
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h_stage_) cudaFreeHost(h_stage_);
+    void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, dd_.count, d_jobs_};
+    for (void* b : dbufs)
+        if (b) cudaFree(b);
 }
 
 int GigaVoxelsRenderer::init() {
@@ -182,6 +185,16 @@ int GigaVoxelsRenderer::init() {
     total_slots_ = (uint32_t)(sx * sy * sz);
     int rc = vv_brickpool_create(ctx_, slots_[0], slots_[1], slots_[2], d_.fmt);
     if (rc) return rc;
+    if (d_.device_paging) {
+        device_paging_ = true;
+        dterrain_ = std::make_unique<DeviceTerrain>();
+        if (dterrain_->upload(tree_->volume()) != cudaSuccess) return VV_ERR_OOM;
+        const int* g = tree_->pool_dim();
+        dd_.first_cells = (size_t)g[0] * g[1] * g[2];
+        if (cudaMalloc((void**)&dd_.first, dd_.first_cells * 4) != cudaSuccess) return VV_ERR_OOM;
+        if (cudaMemset(dd_.first, 0xFF, dd_.first_cells * 4) != cudaSuccess) return VV_ERR_CUDA;
+        if (cudaMalloc((void**)&dd_.count, 4) != cudaSuccess) return VV_ERR_OOM;
+    }
     const size_t nn = tree_->node_count();
     w0_.resize(nn);
     w1_.resize(nn);
@@ -298,27 +311,59 @@ int GigaVoxelsRenderer::upload_nodes(uint32_t n) {
 int GigaVoxelsRenderer::flush_uploads() {
     const size_t n = pending_nodes_.size();
     int rc = VV_OK;
-    if (n) {
+    ms_produce_ = 0.0f;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (n && device_paging_) {
+        // brick production on the GPU, straight into the slots
+        jobs_.resize(n);
+        for (size_t i = 0; i < n; ++i) {
+            const uint32_t node = pending_nodes_[i];
+            int ci, cj, ck;
+            tree_->origin(node, ci, cj, ck);
+            jobs_[i] = make_uint4(pending_slots_[i], (uint32_t)tree_->level(node),
+                                  ((uint32_t)ci << 20) | ((uint32_t)cj << 10) | (uint32_t)ck, 0u);
+        }
+        if (jobs_cap_ < n) {
+            if (d_jobs_) cudaFree(d_jobs_);
+            d_jobs_ = nullptr;
+            jobs_cap_ = std::max(n, 2 * jobs_cap_);
+            if (cudaMalloc((void**)&d_jobs_, jobs_cap_ * sizeof(uint4)) != cudaSuccess) {
+                jobs_cap_ = 0;
+                return VV_ERR_OOM;
+            }
+        }
+        if (cudaMemcpyAsync(d_jobs_, jobs_.data(), n * sizeof(uint4), cudaMemcpyHostToDevice, ctx_->stream) !=
+            cudaSuccess)
+            return VV_ERR_CUDA;
+        void* pool = nullptr;
+        size_t pool_bytes = 0;
+        vv_brickpool_device_ptr(ctx_, &pool, &pool_bytes);
+        if (launch_produce_bricks(dterrain_->view(), d_jobs_, (int)n, pool, d_.fmt, (long long)total_slots_,
+                                  ctx_->d_status, ctx_->stream) != cudaSuccess)
+            return VV_ERR_CUDA;
+    } else if (n) {
         const size_t bb = VV_BRICK_TEXELS * texel_bytes_;
         const size_t bytes = n * bb;
         if (h_stage_cap_ < bytes) {
+            // pinned memory is slow to allocate: grow geometrically, at least 4096 bricks
+            const size_t want = std::max(std::max(bytes, 2 * h_stage_cap_), 4096 * bb);
             if (h_stage_) cudaFreeHost(h_stage_);
             h_stage_ = nullptr;
             h_stage_cap_ = 0;
-            if (cudaMallocHost(&h_stage_, bytes) != cudaSuccess) return VV_ERR_OOM;
-            h_stage_cap_ = bytes;
+            if (cudaMallocHost(&h_stage_, want) != cudaSuccess) return VV_ERR_OOM;
+            h_stage_cap_ = want;
         }
         unsigned char* st = (unsigned char*)h_stage_;
         const int fmt = d_.fmt;
-        const auto t0 = std::chrono::steady_clock::now();
 #pragma omp parallel for schedule(dynamic, 16) num_threads(d_.producer_threads > 0 ? d_.producer_threads : omp_get_max_threads())
         for (long i = 0; i < (long)n; ++i) tree_->produce_brick(pending_nodes_[(size_t)i], fmt, st + (size_t)i * bb);
-        const auto t1 = std::chrono::steady_clock::now();
-        ms_produce_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
+        ms_produce_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    if (n && !device_paging_) {
         rc = vv_upload_bricks(ctx_, pending_slots_.data(), (int32_t)n, h_stage_);
         if (rc) return rc;
     }
-    const auto t2 = std::chrono::steady_clock::now();
     if (!touched_.empty()) {
         std::vector<vv_node_patch> patches;
         patches.reserve(touched_.size());
@@ -340,17 +385,15 @@ int GigaVoxelsRenderer::flush_uploads() {
     return rc;
 }
 
-int GigaVoxelsRenderer::update() {
-    if (!d_count) return VV_ERR_STATE;
-    uploaded_ = 0;
-    ms_produce_ = 0.0f;
-    uint32_t count = 0;
-    if (cudaMemcpyAsync(&count, d_count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
-    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
-    const auto t0 = std::chrono::steady_clock::now();  // the draw has finished here
-    active_ = count;
-    const uint32_t n = std::min<uint32_t>(count, (uint32_t)cap_);
-    req_count_ = n;
+// One distinct requested node, in first-seen order (NodeUsageListProcessor::run,
+// GigaVoxelsOctTree.cpp:509-523): touch its brick if resident, else queue a
+// non-constant node for upload.
+void GigaVoxelsRenderer::visit(uint32_t nidx, std::vector<uint32_t>& upload) {
+    if (node_slot_[nidx] >= 0) lru_.touch((uint32_t)node_slot_[nidx]);
+    else if (!tree_->is_constant(nidx)) upload.push_back(nidx);
+}
+
+int GigaVoxelsRenderer::update_host(uint32_t n, std::vector<uint32_t>& upload) {
     host_requests_.resize((size_t)n * 4);
     if (n) {
         if (cudaMemcpyAsync(host_requests_.data(), d_requests, (size_t)n * 16, cudaMemcpyDeviceToHost,
@@ -358,16 +401,11 @@ int GigaVoxelsRenderer::update() {
             return VV_ERR_CUDA;
         if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     }
-    const auto t1 = std::chrono::steady_clock::now();
-    ms_readback_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
-    // NodeUsageListProcessor::run (GigaVoxelsOctTree.cpp:430-657): decode the
-    // ids, keep the unique nodes in first-seen order, touch resident bricks,
-    // queue non-constant non-resident nodes for upload.
+    requests_on_host_ = true;
     if (++seen_epoch_ == 0) {
         std::fill(seen_mark_.begin(), seen_mark_.end(), 0u);
         seen_epoch_ = 1;
     }
-    std::vector<uint32_t> upload;
     for (size_t i = 0; i < host_requests_.size(); ++i) {
         const uint32_t id = host_requests_[i];
         if (id == 0u) continue;
@@ -376,16 +414,70 @@ int GigaVoxelsRenderer::update() {
         if (nidx == kNoParent || tree_->level(nidx) < 0) continue;
         if (seen_mark_[nidx] == seen_epoch_) continue;
         seen_mark_[nidx] = seen_epoch_;
-        if (node_slot_[nidx] >= 0) lru_.touch((uint32_t)node_slot_[nidx]);
-        else if (!tree_->is_constant(nidx)) upload.push_back(nidx);
+        visit(nidx, upload);
     }
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload) {
+    requests_on_host_ = false;
+    if (!n) return VV_OK;
+    const size_t ids = (size_t)n * 4, blocks = (ids + 1023) / 1024;
+    if (dd_.block_cap < blocks) {
+        if (dd_.block_sums) cudaFree(dd_.block_sums);
+        dd_.block_sums = nullptr;
+        dd_.block_cap = std::max(blocks, 2 * dd_.block_cap);
+        if (cudaMalloc((void**)&dd_.block_sums, dd_.block_cap * 4) != cudaSuccess) return VV_ERR_OOM;
+    }
+    if (dd_.unique_cap < ids) {
+        if (dd_.unique) cudaFree(dd_.unique);
+        dd_.unique = nullptr;
+        dd_.unique_cap = std::max(ids, 2 * dd_.unique_cap);
+        if (cudaMalloc((void**)&dd_.unique, dd_.unique_cap * 4) != cudaSuccess) return VV_ERR_OOM;
+    }
+    const int* pd = tree_->pool_dim();
+    if (launch_dedupe(d_requests, (int)n, pd, dd_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    uint32_t u = 0;
+    if (cudaMemcpyAsync(&u, dd_.count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    unique_host_.resize(u);
+    if (u) {
+        if (cudaMemcpyAsync(unique_host_.data(), dd_.unique, (size_t)u * 4, cudaMemcpyDeviceToHost, ctx_->stream) !=
+            cudaSuccess)
+            return VV_ERR_CUDA;
+        if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    }
+    const uint32_t dx = (uint32_t)pd[0], dy = (uint32_t)pd[1];
+    for (uint32_t g : unique_host_) {
+        const uint32_t nidx = tree_->index_of(g % dx, (g / dx) % dy, g / (dx * dy));
+        if (nidx == kNoParent || tree_->level(nidx) < 0) continue;
+        visit(nidx, upload);
+    }
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::update() {
+    if (!d_count) return VV_ERR_STATE;
+    uploaded_ = 0;
+    uint32_t count = 0;
+    if (cudaMemcpyAsync(&count, d_count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    const auto t0 = std::chrono::steady_clock::now();  // the draw has finished here
+    active_ = count;
+    const uint32_t n = std::min<uint32_t>(count, (uint32_t)cap_);
+    req_count_ = n;
+    std::vector<uint32_t> upload;
+    int rc = device_paging_ ? update_device(n, upload) : update_host(n, upload);
+    if (rc) return rc;
+    const auto t1 = std::chrono::steady_clock::now();
+    ms_readback_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
     // GigaVoxelsOctTree::update touches the root every frame (:1821-1850).
     if (node_slot_[0] >= 0) lru_.touch((uint32_t)node_slot_[0]);
     // BrickPool::update (GigaVoxelsBrickPool.cpp:561-682), including the
     // upload of a non-resident non-constant parent (:629-673).
     for (uint32_t nidx : upload) {
         if (node_slot_[nidx] >= 0) continue;
-        int rc = upload_nodes(nidx);
+        rc = upload_nodes(nidx);
         if (rc) return rc;
         const uint32_t par = tree_->parent(nidx);
         if (par != kNoParent && !tree_->is_constant(par) && node_slot_[par] < 0) {
@@ -395,6 +487,21 @@ int GigaVoxelsRenderer::update() {
     }
     ms_policy_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
     return flush_uploads();
+}
+
+int GigaVoxelsRenderer::last_requests(std::vector<uint32_t>& out) {
+    if (requests_on_host_) {
+        out = host_requests_;
+        return VV_OK;
+    }
+    out.resize((size_t)req_count_ * 4);
+    if (req_count_) {
+        if (cudaMemcpyAsync(out.data(), d_requests, (size_t)req_count_ * 16, cudaMemcpyDeviceToHost, ctx_->stream) !=
+            cudaSuccess)
+            return VV_ERR_CUDA;
+        if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    }
+    return VV_OK;
 }
 
 void GigaVoxelsRenderer::stats(vv_renderer_stats& s) const {

@@ -8,6 +8,7 @@
 
 #include "../../include/voxviz_b200.h"
 #include "octree.h"
+#include "production.h"
 
 namespace vv {
 
@@ -50,7 +51,9 @@ public:
     vv_ctx* ctx() { return ctx_; }
     const vv_uniforms& last_uniforms() const { return last_u_; }
     int slots(int a) const { return slots_[a]; }
-    const std::vector<uint32_t>& last_requests() const { return host_requests_; }
+    // The last compacted request list (host copy; read back from the device
+    // when the device-side service did not need it on the host).
+    int last_requests(std::vector<uint32_t>& out);
     void residency(std::vector<uint32_t>& xyz, std::vector<uint32_t>& slot) const;
 
     float* d_color = nullptr;
@@ -64,6 +67,9 @@ private:
     int alloc_frame(int w, int h);
     int upload_nodes(uint32_t node);     // upload the brick of node, evicting the LRU slot
     int flush_uploads();
+    int update_host(uint32_t n, std::vector<uint32_t>& upload);
+    int update_device(uint32_t n, std::vector<uint32_t>& upload);
+    void visit(uint32_t nidx, std::vector<uint32_t>& upload);
 
     vv_ctx* ctx_;
     const GigaVoxelsOctTree* tree_;
@@ -87,6 +93,15 @@ private:
     int32_t frame_for_compress_ = 0;
     int64_t req_count_ = 0, active_ = 0, uploaded_ = 0, uploaded_total_ = 0, evictions_ = 0, resident_ = 0;
     float ms_readback_ = 0.f, ms_policy_ = 0.f, ms_produce_ = 0.f, ms_upload_ = 0.f;
+    // device-side service
+    bool device_paging_ = false;
+    std::unique_ptr<DeviceTerrain> dterrain_;
+    DedupeBuffers dd_;
+    std::vector<uint32_t> unique_host_;
+    std::vector<uint4> jobs_;
+    uint4* d_jobs_ = nullptr;
+    size_t jobs_cap_ = 0;
+    bool requests_on_host_ = false;
     void* h_stage_ = nullptr;            // pinned brick staging
     size_t h_stage_cap_ = 0;
 };
