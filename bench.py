@@ -47,6 +47,10 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--workload", default="paged", choices=["paged", "precision", "fit"],
+                   help="paged: the 8192^3 paged terrain (default); precision: the 256^3 scene in four brick "
+                        "formats against the FP64 oracle; fit: the differentiable 2048^3 variant")
+    p.add_argument("--fit-steps", type=int, default=200)
     return p.parse_args()
 
 
@@ -118,7 +122,7 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-RAYCAST_VERSION = "v2"  # bumped whenever the ray-cast kernel changes; the ncu capture must match
+RAYCAST_VERSION = "v3"  # bumped whenever the ray-cast kernel changes; the ncu capture must match
 
 
 def ncu_traffic():
@@ -179,6 +183,46 @@ def parity_sample(r, ctx, u, words, pool, slots, fmt, jitter):
         n += e.size
     return {"rows_checked": sum(b - a for a, b in bands), "usage_bitexact_vs_fp32_oracle": exact,
             "err_vs_fp64": {"max": err_max, "rms": (sq / max(n, 1)) ** 0.5}}
+
+
+def fwd_bwd_leg(ctx, us, reps, per_ray=16):
+    """Checkpointing forward + adjoint of the L2 loss sum(colour^2) over the
+    given frames on the current pools: dL/d(texel) of every pool texel
+    (float4 per texel, zeroed each step).  Device-timed with CUDA events on
+    the stream both run on."""
+    import torch
+
+    import voxviz_b200 as vv
+
+    W, H = us[0].width, us[0].height
+    dev = torch.device("cuda", torch.cuda.current_device())
+    color = torch.empty((H, W, 4), dtype=torch.float32, device=dev)
+    nb = vv.Context.ckpt_bytes(W, H, per_ray)
+    ck = torch.empty(nb, dtype=torch.uint8, device=dev)
+    _, pool_bytes = ctx.brickpool_ptr()
+    texels = pool_bytes // vv.TEXEL_BYTES[ctx.fmt]
+    grad = torch.empty((texels, 4), dtype=torch.float32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd_ms, bwd_ms = [], []
+    for i in range(reps + 2):
+        u = us[i % len(us)]
+        ev[0].record()
+        ctx.forward_ckpt(u, color.data_ptr(), ck.data_ptr(), per_ray)
+        ev[1].record()
+        dl = color * 2.0
+        grad.zero_()
+        ctx.backward(u, dl.data_ptr(), ck.data_ptr(), per_ray, grad.data_ptr())
+        ev[2].record()
+        torch.cuda.synchronize()
+        if i >= 2:
+            fwd_ms.append(ev[0].elapsed_time(ev[1]))
+            bwd_ms.append(ev[1].elapsed_time(ev[2]))
+    status = ctx.device_status(clear=True)
+    f, b = float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
+    return {"fwd_mrays_s": round(W * H / (f / 1e3) / 1e6, 1), "fwd_bwd_mrays_s": round(W * H / ((f + b) / 1e3) / 1e6, 1),
+            "fwd_ms": round(f, 3), "bwd_ms": round(b, 3), "frames": len(us), "reps": reps, "per_ray_ckpts": per_ray,
+            "ckpt_bytes": nb, "grad_bytes": int(texels * 16), "status": status,
+            "loss": "sum(colour^2); bwd = elementwise dL/dc + grad zeroing + adjoint kernel"}
 
 
 def run_ours(args):
@@ -296,6 +340,7 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (float(np.mean(ray_ms)) / 1e3) / 1e9
     traffic = ncu_traffic()
+    fb = fwd_bwd_leg(ctx, timed_u[-16:], reps=min(16, args.steps))
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
@@ -325,6 +370,7 @@ def run_ours(args):
                    "requests_per_frame": round(requests / args.steps, 1), "converge_draws": converge,
                    "host_ms_per_frame": {k[3:]: round(v / args.steps, 3) for k, v in host_ms.items()},
                    "resident": r.stats()["resident_bricks"], "pool_slots": r.stats()["pool_slots"]},
+        "fwd_bwd": fb,
         "clocks": clk, "gpu_launches": None, "setup_s": round(setup_s, 1),
     }
     # our kernels per step: raycast + select + (levels-1) up + (levels-1) down + total + compact + patch + scatter
@@ -343,6 +389,256 @@ def run_ours(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+FIT_DEPTH, FIT_VIEWS, FIT_SIZE, FIT_SIGMA, FIT_LR = 8, 16, 512, 0.05, 5e-3
+FIT_POOL_BYTES = 6 << 30
+FIT_VIEW_SEED, FIT_NOISE_SEED, FIT_FD_SEED = 500, 11, 3
+
+
+def fit_subvolume_texels(octree, r, grad, slots, n, seed, box=64):
+    """`n` random pool texels (slot, texel, channel) with a non-zero gradient
+    whose voxel centres lie in a box^3 sub-volume of the leaf-level volume,
+    centred on the terrain surface at the volume's centre column."""
+    info = octree.info
+    L = info.depth
+    heights = octree.heights()
+    dim = info.volume_dim
+    c = np.array([dim // 2, dim // 2, int(heights[dim // 2, dim // 2])])
+    lo, hi = c - box // 2, c + box // 2
+    xyz, slot = r.residency()
+    cand = []
+    t = np.arange(1000)
+    tl = np.stack([t % 10, (t // 10) % 10, t // 100], axis=1)
+    for (x, y, z), s in zip(xyz, slot):
+        ni = octree.node_info(int(x), int(y), int(z))
+        scale = 1 << (L - ni.level)
+        o = np.array(list(ni.origin))
+        vox = (o + tl - 1 + 0.5) * scale  # texel centres in leaf voxels (border texels lie outside the node)
+        inside = np.all((vox >= lo) & (vox < hi), axis=1) & np.all((tl >= 1) & (tl <= 8), axis=1)
+        for ti in np.nonzero(inside)[0]:
+            cand.append((int(s), int(ti)))
+    if not cand:
+        return np.zeros((0, 3), dtype=np.int64), (lo.tolist(), hi.tolist())
+    cand = np.array(cand, dtype=np.int64)
+    g = grad[cand[:, 0], cand[:, 1]]  # (m, 4)
+    nz = np.argwhere(g != 0)
+    rng = np.random.default_rng(seed)
+    pick = nz[rng.choice(len(nz), size=min(n, len(nz)), replace=False)]
+    out = np.stack([cand[pick[:, 0], 0], cand[pick[:, 0], 1], pick[:, 1]], axis=1)
+    return out, (lo.tolist(), hi.tolist())
+
+
+def run_fit(args):
+    """Differentiable variant: fit brick contents to target views."""
+    import torch
+
+    import voxviz_b200 as vv
+    from voxviz_b200 import diff, scene
+
+    torch.cuda.set_device(0)
+    t_setup = time.perf_counter()
+    octree = vv.Octree.terrain(seed=TERRAIN_SEED, depth=FIT_DEPTH)
+    heights = octree.heights()
+    cams = [scene.seeded_view(FIT_VIEW_SEED + v, heights, FIT_SIZE, FIT_SIZE) for v in range(FIT_VIEWS)]
+    ctx = vv.Context(0)
+    r = vv.Renderer(ctx, octree, fmt="fp32", pool_bytes=FIT_POOL_BYTES, preload_all=False, alpha_stop=ALPHA_STOP,
+                    jitter_seed=JITTER_SEED, device_paging=True)
+    passes = scene.converge_views(r, cams)
+    st = r.stats()
+    slots = ctx.slots
+    us = [vv.compute_uniforms(octree.info, cam, slots, 1.0, ALPHA_STOP) for cam in cams]
+    clean = diff.pool_tensor_from_context(ctx)
+    diff.attach_pool(ctx, clean, slots)
+    gen = torch.Generator(device="cuda").manual_seed(FIT_NOISE_SEED)
+    noisy = (clean + FIT_SIGMA * torch.randn(clean.shape, generator=gen, device="cuda")).contiguous()
+    with torch.no_grad():
+        target = diff.render(noisy, ctx, slots, us)
+    del noisy
+    setup_s = time.perf_counter() - t_setup
+
+    def loss_sum64(c):
+        return ((c.double() - target.double()) ** 2).sum()
+
+    # ---- gradient checks at the starting point (param = clean bricks) ----
+    param = clean.clone().requires_grad_(True)
+    c0 = diff.render(param, ctx, slots, us)
+    l0 = loss_sum64(c0)
+    l0.backward()
+    grad = param.grad.detach()
+    status = diff.check_status(ctx)
+    gnp = grad.cpu().numpy()
+    picks, box = fit_subvolume_texels(octree, r, gnp, slots, 256, FIT_FD_SEED)
+    h = 1e-3
+    fd, an = [], []
+    with torch.no_grad():
+        base = param.detach()
+        flat = base.view(-1)
+        for s_, t_, ch in picks:
+            i = (int(s_) * 1000 + int(t_)) * 4 + int(ch)
+            old = float(flat[i])
+            flat[i] = old + h
+            l1 = loss_sum64(diff.render(base, ctx, slots, us))
+            flat[i] = old - h
+            l2 = loss_sum64(diff.render(base, ctx, slots, us))
+            flat[i] = old
+            fd.append(float((l1 - l2) / (2 * h)))
+            an.append(float(gnp[s_, t_, ch]))
+    fd, an = np.array(fd), np.array(an)
+    rel = np.abs(fd - an) / np.maximum(np.abs(fd), 1e-30)
+    fd_report = {"texels": int(len(picks)), "h": h, "subvolume_leaf_voxels": box,
+                 "rel_err_median": float(np.median(rel)) if len(rel) else None,
+                 "rel_err_p95": float(np.percentile(rel, 95)) if len(rel) else None,
+                 "rel_err_max": float(rel.max()) if len(rel) else None,
+                 "frac_within_1e-3": float((rel <= 1e-3).mean()) if len(rel) else None,
+                 "loss_reduction": "float64 on the GPU"}
+    # FP64 host gradient on row bands of two views
+    from oracle import gv_oracle as go
+    words = ctx.download_nodes()
+    pool_host = param.detach().cpu().numpy()
+    jit = vv.make_jitter(JITTER_SEED)
+    osc = go.Scene(words, pool_host.view(np.uint8).reshape(pool_host.shape[0], -1), slots, vv.VV_FMT_FP32, jit)
+    worst, checked = 0.0, 0
+    per_ray = diff.DEFAULT_PER_RAY
+    ck = torch.empty(vv.Context.ckpt_bytes(FIT_SIZE, FIT_SIZE, per_ray), dtype=torch.uint8, device="cuda")
+    col = torch.empty((FIT_SIZE, FIT_SIZE, 4), dtype=torch.float32, device="cuda")
+    for v in (0, 1):
+        r0, r1 = FIT_SIZE // 2, FIT_SIZE // 2 + 8
+        ctx.forward_ckpt(us[v], col.data_ptr(), ck.data_ptr(), per_ray)
+        dl = torch.zeros_like(col)
+        dl[r0:r1] = 2.0 * (col[r0:r1] - target[v, r0:r1])
+        g_gpu = torch.zeros_like(param)
+        ctx.backward(us[v], dl.data_ptr(), ck.data_ptr(), per_ray, g_gpu.data_ptr())
+        torch.cuda.synchronize()
+        ref = go.backward(us[v], osc, dl.cpu().numpy(), rows=(r0, r1))
+        got = g_gpu.cpu().numpy().astype(np.float64)
+        scale = np.abs(ref).max()
+        big = np.abs(ref) > 1e-3 * scale
+        worst = max(worst, float((np.abs(got - ref)[big] / np.abs(ref)[big]).max()))
+        checked += int(big.sum())
+        del ref, got
+    host_report = {"views": 2, "rows": "8 per view", "texels_compared": checked, "rel_err_max": worst,
+                   "criterion": "texels above 1e-3 of the largest gradient"}
+    # ---- the fit: Adam on every pool texel, L2 image loss ----
+    param.grad = None
+    opt = torch.optim.Adam([param], lr=FIT_LR, fused=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    fwd_ms, bwd_ms, adam_ms, losses = [], [], [], []
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for step in range(args.fit_steps):
+        ev[0].record()
+        c = diff.render(param, ctx, slots, us)
+        ev[1].record()
+        loss = ((c - target) ** 2).mean()
+        opt.zero_grad(set_to_none=False)
+        loss.backward()
+        ev[2].record()
+        opt.step()
+        ev[3].record()
+        losses.append(loss.detach())
+        torch.cuda.synchronize()
+        fwd_ms.append(ev[0].elapsed_time(ev[1]))
+        bwd_ms.append(ev[1].elapsed_time(ev[2]))
+        adam_ms.append(ev[2].elapsed_time(ev[3]))
+    t1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = t0.elapsed_time(t1)
+    status |= diff.check_status(ctx)
+    losses = [float(x) for x in losses]
+    rays = FIT_VIEWS * FIT_SIZE * FIT_SIZE
+    skip = min(3, max(0, args.fit_steps - 1))
+    f = float(np.mean(fwd_ms[skip:]))
+    b = float(np.mean(bwd_ms[skip:]))
+    a = float(np.mean(adam_ms[skip:]))
+    out = {
+        "workload": "fit", "metric": "Mrays/s fwd & fwd+bwd, 16x512^2 views, 2048^3 FP32 bricks",
+        "value": round(rays / ((f + b) / 1e3) / 1e6, 2), "unit": "Mrays/s (fwd+bwd)",
+        "fwd_mrays_s": round(rays / (f / 1e3) / 1e6, 2), "higher_is_better": True,
+        "ms": {"fwd": round(f, 3), "bwd": round(b, 3), "adam": round(a, 3),
+               "step_total_mean": round(total_ms / max(1, args.fit_steps), 3)},
+        "adam_steps": args.fit_steps, "lr": FIT_LR,
+        "loss": {"first": losses[0] if losses else None, "last": losses[-1] if losses else None,
+                 "at": {str(k): losses[k] for k in (0, 10, 50, 100, 199) if k < len(losses)}},
+        "grad_check_fd": fd_report, "grad_check_fp64_host": host_report, "status": status,
+        "config": {"workload": f"fBm terrain {octree.info.volume_dim}^3 (depth {FIT_DEPTH}), FP32 bricks, "
+                               f"{FIT_VIEWS} seeded {FIT_SIZE}x{FIT_SIZE} views, targets from bricks + N(0,{FIT_SIGMA})",
+                   "pool_slots": list(slots), "resident_bricks": st["resident_bricks"], "paging_passes": passes,
+                   "evictions": st["evictions_total"], "params": int(param.numel()), "data": "synthetic"},
+        "clocks": clk, "setup_s": round(setup_s, 1),
+    }
+    print(json.dumps(out), flush=True)
+    r.close()
+    ctx.close()
+
+
+def run_precision(args):
+    """The 256^3 scene in RGBA8 / FP16 / BF16 / FP32 brick pools, 64 seeded
+    512x512 views: Mrays/s, HBM GB/s and per-pixel error against the FP64
+    oracle (on the same stored bricks, and on the FP32 bricks)."""
+    import torch
+
+    import voxviz_b200 as vv
+    from voxviz_b200 import scene
+    from oracle import gv_oracle as go
+
+    torch.cuda.set_device(0)
+    octree = vv.Octree.terrain(seed=TERRAIN_SEED, depth=5)
+    heights = octree.heights()
+    jit = vv.make_jitter(JITTER_SEED)
+    views = 64
+    cams = [scene.seeded_view(3 + v, heights, 512, 512, frame=v) for v in range(views)]
+    peak, peak_kind = measured_peaks()
+    threads = go.cpu_count()
+    ref32 = None
+    rows = {}
+    order = ["fp32", "rgba8", "fp16", "bf16"]
+    for fmt in order:
+        f = vv.fmt_code(fmt)
+        words, pool, slots, xyz = scene.resident_scene(octree, f)
+        ctx = vv.Context(0)
+        ctx.upload_nodes(words)
+        ctx.create_brickpool(slots, f)
+        ctx.upload_bricks(np.arange(xyz.shape[0], dtype=np.uint32), pool[:xyz.shape[0]])
+        ctx.set_jitter(jit)
+        ctx.set_profiling(True)
+        color = torch.empty((512, 512, 4), dtype=torch.float32, device="cuda")
+        us = [vv.compute_uniforms(octree.info, c, slots, 1.0, ALPHA_STOP) for c in cams]
+        for u in us[:3]:
+            ctx.render(u, color=color.data_ptr(), passes=vv.VV_PASS_RAYCAST)
+        ms, gbs, imgs = [], [], []
+        for u in us:
+            ctx.render(u, color=color.data_ptr(), passes=vv.VV_PASS_RAYCAST)
+            ctx.synchronize()
+            a, _ = ctx.last_times()
+            nodes, bricks = ctx.footprint(u)
+            ms.append(a)
+            gbs.append((8 * nodes + 1000 * vv.TEXEL_BYTES[f] * bricks + 512 * 512 * 16) / (a / 1e3) / 1e9)
+            imgs.append(color.cpu().numpy().copy())
+        status = ctx.device_status(clear=True)
+        sc = go.Scene(words, pool, slots, f, jit)
+        own = [go.raycast(u, sc, 64, threads=threads, want_usage=False)[0] for u in us]
+        if fmt == "fp32":
+            ref32 = own
+        e_own = np.concatenate([np.abs(i.astype(np.float64) - o).ravel() for i, o in zip(imgs, own)])
+        e_32 = np.concatenate([np.abs(i.astype(np.float64) - o).ravel() for i, o in zip(imgs, ref32)])
+        rows[fmt] = {"mrays_s": round(512 * 512 / (float(np.mean(ms)) / 1e3) / 1e6, 1),
+                     "raycast_ms": round(float(np.mean(ms)), 4), "hbm_gbs_algorithmic": round(float(np.mean(gbs)), 1),
+                     "frac_of_peak": round(float(np.mean(gbs)) / peak, 4),
+                     "err_vs_fp64_same_bricks": {"max": float(e_own.max()), "rms": float(np.sqrt((e_own ** 2).mean()))},
+                     "err_vs_fp64_fp32_bricks": {"max": float(e_32.max()), "rms": float(np.sqrt((e_32 ** 2).mean()))},
+                     "status": status, "brick_bytes": 1000 * vv.TEXEL_BYTES[f]}
+        ctx.close()
+    out = {"workload": "precision", "metric": "Mrays/s, HBM GB/s and error vs FP64 per brick format",
+           "config": {"workload": "fBm terrain 256^3 (depth 5), 64 seeded 512x512 views, FP32 compositing",
+                      "peak_gbs": peak, "peak_source": peak_kind, "data": "synthetic"},
+           "formats": rows, "oracle_threads": threads}
+    print(json.dumps(out), flush=True)
 
 
 def run_reference(args):
@@ -396,6 +692,10 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "fit":
+        run_fit(args)
+    elif args.workload == "precision":
+        run_precision(args)
     else:
         run_ours(args)
 

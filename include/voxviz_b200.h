@@ -224,6 +224,29 @@ int vv_ctx_last_times(vv_ctx* ctx, float* raycast_ms, float* compact_ms);
 int vv_measure_footprint(vv_ctx* ctx, int32_t tree, const vv_uniforms* u,
                          int64_t* nodes, int64_t* bricks);
 
+/* ---- differentiable ray cast --------------------------------------------- */
+
+/* No counterpart in the reference: the adjoint of the ray cast with respect
+ * to the brick texels.  vv_render_forward_ckpt runs the ray cast of vv_render
+ * (colour only, identical values) and stores per-ray checkpoints (at a leaf
+ * segment start every >= 32 composited samples, at most `per_ray` per ray)
+ * into `ckpt`, a device buffer of vv_ckpt_bytes(width, height, per_ray)
+ * bytes.  vv_backward then ADDS dL/d(texel) to `grad_texels` (device, one
+ * float4 per pool texel, slot-major like the pool) given dL/d(colour)
+ * (`dl_dcolor`, device, float4 per pixel) for the same uniforms and pools.
+ * The gradient is with respect to the normalized texel value (v/255 for
+ * RGBA8); the forward's control flow is held fixed. */
+size_t vv_ckpt_bytes(int32_t width, int32_t height, int32_t per_ray);
+int vv_render_forward_ckpt(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, float* color,
+                           void* ckpt, int32_t per_ray);
+int vv_backward(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl_dcolor,
+                const void* ckpt, int32_t per_ray, float* grad_texels);
+/* Use caller-owned device memory (e.g. a torch tensor) as the brick pool:
+ * slots_x*slots_y*slots_z*1000 texels of `fmt` at `texels`; the context does
+ * not free it.  Replaces vv_brickpool_create for differentiable use. */
+int vv_brickpool_attach(vv_ctx* ctx, void* texels, int32_t slots_x, int32_t slots_y,
+                        int32_t slots_z, int32_t fmt);
+
 /* ---- page-request compaction without allocation ------------------------- */
 
 /* This entry point has no counterpart in the reference.  It is for callers

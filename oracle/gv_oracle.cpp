@@ -177,6 +177,13 @@ vec4<T> lerp4(const vec4<T>& a, const vec4<T>& b, T t) {
     return vec4<T>{glsl_lerp(a.r, b.r, t), glsl_lerp(a.g, b.g, t), glsl_lerp(a.b, b.b, t), glsl_lerp(a.a, b.a, t)};
 }
 
+struct SampleRec {
+    bool brick;
+    double src[4];
+    double T;
+    float bpos[3];
+};
+
 // Per-pixel shader state and body.
 template <typename T>
 struct Shader {
@@ -195,6 +202,7 @@ struct Shader {
     const uint8_t* jitter;
     int max_iter;
     int* status;
+    std::vector<SampleRec>* tape = nullptr;
 
     void init(const vv_uniforms* u) {
         U = u;
@@ -315,8 +323,25 @@ struct Shader {
             src.r *= sampleRatio;
             src.g *= sampleRatio;
             src.b *= sampleRatio;
+            record(false, src, dst, pos);
             composite(dst, src);
         }
+    }
+    // The adjoint's tape: every composited sample with the transmittance
+    // before it (and for brick samples the brick-pool coordinate).
+    void record(bool brick, const vec4<T>& src, const vec4<T>& dst, const vec3<T>& bpos) const {
+        if (!tape) return;
+        SampleRec r;
+        r.brick = brick;
+        r.src[0] = (double)src.r;
+        r.src[1] = (double)src.g;
+        r.src[2] = (double)src.b;
+        r.src[3] = (double)src.a;
+        r.T = (double)((T)1 - dst.a);
+        r.bpos[0] = (float)bpos.x;
+        r.bpos[1] = (float)bpos.y;
+        r.bpos[2] = (float)bpos.z;
+        tape->push_back(r);
     }
     static void composite(vec4<T>& dst, const vec4<T>& src) {
         T k = (T)1 - dst.a;
@@ -341,6 +366,7 @@ struct Shader {
             }
             vec4<T> src = texture(curBrickRayPos);
             src.a = (T)1 - pow_pow2((T)1 - src.a, 0);
+            record(true, src, dst, curBrickRayPos);
             composite(dst, src);
             curBrickRayPos += brickRayStep;
         }
@@ -640,6 +666,71 @@ int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, i
 }
 
 int oracle_max_iterations(const vv_uniforms* u) { return max_iterations(u); }
+
+// Adjoint of the binary32 ray cast in binary64: the forward runs exactly as
+// oracle_raycast(precision 32) and records its samples; the backward walks
+// them in reverse, g_k.a = g_{k+1}.a - dot(g_{k+1}, src_k), dL/dsrc_k =
+// g_{k+1} * T_k, and adds w_j * dL/dsrc_k to the 8 texels of each brick
+// sample (weights from the forward's float tap fractions).  grad holds 4
+// doubles per pool texel (slot-major, brick-linear), added to.
+int oracle_backward(const vv_uniforms* u, const oracle_scene* s, const float* dl_dcolor, double* grad, int row0,
+                    int row1) {
+    if (!u || !s || !dl_dcolor || !grad || row0 < 0 || row1 > u->height || row0 > row1) return VV_ERR_ARG;
+    Shader<float> sh;
+    sh.init(u);
+    sh.nodes = s->nodes;
+    for (int a = 0; a < 3; ++a) sh.ndim[a] = s->node_dim[a];
+    sh.brick.data = s->bricks;
+    sh.brick.fmt = s->fmt;
+    sh.brick.sx = s->slots[0];
+    sh.brick.sy = s->slots[1];
+    sh.brick.sz = s->slots[2];
+    sh.jitter = s->jitter;
+    sh.max_iter = max_iterations(u);
+    int st = 0;
+    sh.status = &st;
+    std::vector<SampleRec> tape;
+    sh.tape = &tape;
+    const int W = u->width;
+    const float N[3] = {u->brick_pool_dimension[0], u->brick_pool_dimension[1], u->brick_pool_dimension[2]};
+    const int n[3] = {s->slots[0] * 10, s->slots[1] * 10, s->slots[2] * 10};
+    for (int y = row0; y < row1; ++y)
+        for (int x = 0; x < W; ++x) {
+            tape.clear();
+            vec4<float> c;
+            uint32_t lst[12];
+            sh.main(x, y, c, lst);
+            const float* gp = dl_dcolor + 4 * ((size_t)y * W + x);
+            double g[4] = {gp[0], gp[1], gp[2], gp[3]};
+            for (size_t k = tape.size(); k-- > 0;) {
+                const SampleRec& r = tape[k];
+                if (r.brick) {
+                    const double d[4] = {g[0] * r.T, g[1] * r.T, g[2] * r.T, g[3] * r.T};
+                    int i0[3], i1[3];
+                    double f[3];
+                    for (int a = 0; a < 3; ++a) {
+                        float t = r.bpos[a] * N[a] - 0.5f;
+                        t = std::fmin(std::fmax(t, -1.0f), N[a]);
+                        const float fl = std::floor(t);
+                        f[a] = (double)(t - fl);
+                        const int kk = (int)fl;
+                        i0[a] = std::min(std::max(kk, 0), n[a] - 1);
+                        i1[a] = std::min(std::max(kk + 1, 0), n[a] - 1);
+                    }
+                    for (int t8 = 0; t8 < 8; ++t8) {
+                        const int bx = t8 & 1, by = (t8 >> 1) & 1, bz = t8 >> 2;
+                        const double w = (bx ? f[0] : 1.0 - f[0]) * (by ? f[1] : 1.0 - f[1]) * (bz ? f[2] : 1.0 - f[2]);
+                        const int ix = bx ? i1[0] : i0[0], iy = by ? i1[1] : i0[1], iz = bz ? i1[2] : i0[2];
+                        const size_t slot = ((size_t)(iz / 10) * s->slots[1] + (size_t)(iy / 10)) * s->slots[0] + (size_t)(ix / 10);
+                        const size_t ti = slot * 1000 + (size_t)((iz % 10) * 100 + (iy % 10) * 10 + (ix % 10));
+                        for (int ch = 0; ch < 4; ++ch) grad[4 * ti + ch] += w * d[ch];
+                    }
+                }
+                g[3] = g[3] - (g[0] * r.src[0] + g[1] * r.src[1] + g[2] * r.src[2] + g[3] * r.src[3]);
+            }
+        }
+    return st;
+}
 
 // GenerateSelectionMask.frag (:15-187): the red channel per pixel.
 int oracle_select(const uint32_t* usage, int w, int h, uint32_t* mask) {

@@ -22,6 +22,11 @@ typedef struct oracle_scene {
 int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
                    void* color, uint32_t* usage, int threads, int32_t* status);
 int oracle_max_iterations(const vv_uniforms* u);
+/* Adjoint of the binary32 ray cast with binary64 accumulation: ADDS
+ * dL/d(texel) (4 doubles per pool texel, slot-major) for rows [row0,row1)
+ * given dL/d(colour) (4 floats per pixel).  Single-threaded. */
+int oracle_backward(const vv_uniforms* u, const oracle_scene* s, const float* dl_dcolor, double* grad,
+                    int row0, int row1);
 int oracle_select(const uint32_t* usage, int w, int h, uint32_t* mask);
 int oracle_compress(const uint32_t* usage, const uint32_t* mask, int w, int h, int max_push, int cap,
                     uint32_t* out, uint32_t* total);

@@ -51,6 +51,9 @@ def load() -> C.CDLL:
                                    C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]
     lib.oracle_max_iterations.restype = C.c_int
     lib.oracle_max_iterations.argtypes = [C.POINTER(Uniforms)]
+    lib.oracle_backward.restype = C.c_int
+    lib.oracle_backward.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_void_p, C.c_void_p, C.c_int,
+                                    C.c_int]
     lib.oracle_select.restype = C.c_int
     lib.oracle_select.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     lib.oracle_compress.restype = C.c_int
@@ -95,6 +98,21 @@ def raycast(u, scene: Scene, precision: int = 32, rows=None, threads: int = 0, w
     if rc != 0:
         raise RuntimeError(f"oracle_raycast failed: {rc}")
     return color, usage, st.value
+
+
+def backward(u, scene: Scene, dl_dcolor: np.ndarray, rows=None, grad: np.ndarray | None = None) -> np.ndarray:
+    """dL/d(texel) in float64, shape (slots, 1000, 4), of the binary32 ray cast."""
+    lib = load()
+    r0, r1 = (0, u.height) if rows is None else rows
+    g = np.ascontiguousarray(dl_dcolor, dtype=np.float32)
+    assert g.shape == (u.height, u.width, 4)
+    n = int(np.prod(list(scene.s.slots)))
+    if grad is None:
+        grad = np.zeros((n, 1000, 4), dtype=np.float64)
+    rc = lib.oracle_backward(C.byref(u), C.byref(scene.s), _p(g), _p(grad), r0, r1)
+    if rc != 0:
+        raise RuntimeError(f"oracle_backward failed: {rc}")
+    return grad
 
 
 def select(usage: np.ndarray) -> np.ndarray:

@@ -296,6 +296,32 @@ class Context:
                      compress_max_push=compress_max_push, passes=passes)
         self._ck(lib().vv_render(self._h, tree, C.byref(u), C.byref(o)), "render")
 
+    # ---- differentiable ray cast (device pointers throughout) ----
+
+    def attach_bricks(self, texels_ptr: int, slots: Sequence[int], fmt="fp32") -> None:
+        """Use caller-owned device memory (1000 texels per slot) as the brick pool."""
+        self._ck(lib().vv_brickpool_attach(self._h, C.c_void_p(texels_ptr), int(slots[0]), int(slots[1]),
+                                           int(slots[2]), fmt_code(fmt)), "brick pool attach")
+
+    def brickpool_ptr(self) -> tuple[int, int]:
+        """(device pointer, bytes) of the current brick pool."""
+        p, n = C.c_void_p(), C.c_size_t()
+        self._ck(lib().vv_brickpool_device_ptr(self._h, C.byref(p), C.byref(n)), "brick pool pointer")
+        return int(p.value or 0), int(n.value)
+
+    @staticmethod
+    def ckpt_bytes(width: int, height: int, per_ray: int) -> int:
+        return int(lib().vv_ckpt_bytes(width, height, per_ray))
+
+    def forward_ckpt(self, u: Uniforms, color: int, ckpt: int, per_ray: int, tree: int = 0) -> None:
+        self._ck(lib().vv_render_forward_ckpt(self._h, tree, C.byref(u), C.c_void_p(color), C.c_void_p(ckpt),
+                                              per_ray), "forward with checkpoints")
+
+    def backward(self, u: Uniforms, dl_dcolor: int, ckpt: int, per_ray: int, grad_texels: int,
+                 tree: int = 0) -> None:
+        self._ck(lib().vv_backward(self._h, tree, C.byref(u), C.c_void_p(dl_dcolor), C.c_void_p(ckpt), per_ray,
+                                   C.c_void_p(grad_texels)), "backward")
+
 
 # -------------------------------------------------------------- renderer ---
 

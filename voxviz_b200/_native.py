@@ -182,6 +182,10 @@ SIGNATURES = {
     "vv_render": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(FrameOut)]),
     "vv_compact_requests_noalloc": (C.c_int, [P, P, C.c_int32, C.c_int32, P, P, C.c_int32, C.c_int32, P]),
     "vv_ctx_set_profiling": (C.c_int, [P, C.c_int32]),
+    "vv_ckpt_bytes": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
+    "vv_render_forward_ckpt": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32]),
+    "vv_backward": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32, P]),
+    "vv_brickpool_attach": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "vv_ctx_last_times": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "vv_measure_footprint": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int64)]),

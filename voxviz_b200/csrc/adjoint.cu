@@ -1,0 +1,215 @@
+// adjoint.cu - differentiable ray cast: checkpointing forward and adjoint.
+//
+// The forward composites  dst_{k+1} = dst_k + T_k * src_k,  T_k = 1 - dst_k.a
+// (GigaVoxelsNoLighting.frag:280,354).  Its adjoint with g = dL/d dst is
+//   dL/d src_k = g_{k+1} * T_k
+//   g_k.rgb    = g_{k+1}.rgb,   g_k.a = g_{k+1}.a - dot(g_{k+1}, src_k)
+// and a brick sample is the trilinear blend of 8 texels, so each texel gets
+// its blend weight times dL/d src_k.  Walking the samples backwards needs
+// T_k, which is not recoverable from the final colour once a sample is
+// opaque, so the forward stores a checkpoint at the start of a leaf segment
+// whenever 32 or more samples were composited since the last one; there the
+// walk restarts from the root, so a checkpoint is only the ray position,
+// dst, the iteration count, the sample index and the node pointer.  The
+// adjoint replays each chunk from its checkpoint (in pieces of at most 64
+// samples, the last piece first), keeps the samples of the piece in local
+// memory and back-propagates through them in reverse.  The control flow
+// (descent, step counts, early termination) is that of the forward and is
+// held fixed, as any reverse-mode derivative of this shader does.
+#include "raycast_common.cuh"
+
+namespace vv {
+
+using namespace rc;
+
+namespace {
+
+constexpr int kCkptEvery = 32;
+constexpr int kPiece = 64;
+
+struct Ckpt {
+    float4 a;  // pos.xyz, dst.x
+    float4 b;  // dst.yzw, iter (bits)
+    uint4 c;   // nsamples, nptr xyz
+};
+
+struct CkptVisitor {
+    Ckpt* out;
+    int cap, count, last;
+    int* status;
+    __device__ __forceinline__ bool segment_begin(const RayState& s) {
+        if ((count == 0 || s.nsamples - last >= kCkptEvery) && count < cap) {
+            Ckpt c;
+            c.a = make_float4(s.pos.x, s.pos.y, s.pos.z, s.dst.x);
+            c.b = make_float4(s.dst.y, s.dst.z, s.dst.w, __int_as_float(s.iter));
+            c.c = make_uint4((uint32_t)s.nsamples, s.nptr_x, s.nptr_y, s.nptr_z);
+            out[count++] = c;
+            last = s.nsamples;
+        }
+        return true;
+    }
+    __device__ __forceinline__ bool sample(int, const float4&, F3, float, int) { return true; }
+    __device__ __forceinline__ void segment_end(const RayState&, bool, bool) {}
+    __device__ __forceinline__ void fail(int code) { set_status(status, code); }
+};
+
+struct ReplayVisitor {
+    int first, last, n;
+    float4 src[kPiece];
+    float T[kPiece];
+    F3 bpos[kPiece];
+    bool brick[kPiece];
+    __device__ __forceinline__ bool segment_begin(const RayState& s) { return s.nsamples < last; }
+    __device__ __forceinline__ bool sample(int kind, const float4& v, F3 b, float t, int index) {
+        if (index >= first && n < kPiece) {
+            src[n] = v;
+            T[n] = t;
+            bpos[n] = b;
+            brick[n] = kind == kSampleBrick;
+            ++n;
+        }
+        return index + 1 < last;
+    }
+    __device__ __forceinline__ void segment_end(const RayState&, bool, bool) {}
+    __device__ __forceinline__ void fail(int) {}
+};
+
+// dL/d texel += w_j * d for the 8 taps of the sample at uvw (the addressing
+// of sample_brick, clamps included: clamped taps share a texel).
+__device__ __forceinline__ void scatter_texels(const RaycastParams& p, F3 uvw, float4 d, float4* grad) {
+    const float* N = p.u.brick_pool_dimension;
+    const Axis ax = axis_taps(uvw.x, N[0], p.slots[0] * 10);
+    const Axis ay = axis_taps(uvw.y, N[1], p.slots[1] * 10);
+    const Axis az = axis_taps(uvw.z, N[2], p.slots[2] * 10);
+    const uint32_t SX = (uint32_t)p.slots[0], SY = (uint32_t)p.slots[1];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int bx = t & 1, by = (t >> 1) & 1, bz = t >> 2;
+        const float w = (bx ? ax.f : 1.0f - ax.f) * (by ? ay.f : 1.0f - ay.f) * (bz ? az.f : 1.0f - az.f);
+        if (w == 0.0f) continue;
+        const int sx = bx ? ax.s1 : ax.s0, lx = bx ? ax.l1 : ax.l0;
+        const int sy = by ? ay.s1 : ay.s0, ly = by ? ay.l1 : ay.l0;
+        const int sz = bz ? az.s1 : az.s0, lz = bz ? az.l1 : az.l0;
+        const uint32_t slot = ((uint32_t)sz * SY + (uint32_t)sy) * SX + (uint32_t)sx;
+        const uint32_t i = slot * 1000u + (uint32_t)((lz * 10 + ly) * 10 + lx);
+        atomicAdd(grad + i, make_float4(w * d.x, w * d.y, w * d.z, w * d.w));
+    }
+}
+
+__device__ __forceinline__ void pixel_of(int& px, int& py) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    px = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
+    py = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+}
+
+}  // namespace
+
+template <int FMT>
+__global__ void __launch_bounds__(128) forward_ckpt_kernel(const __grid_constant__ RaycastParams p, int2* hdr,
+                                                           Ckpt* ckpt, int per_ray) {
+    int px, py;
+    pixel_of(px, py);
+    const vv_uniforms& u = p.u;
+    if (px >= u.width || py >= u.height) return;
+    const size_t pix = (size_t)py * u.width + px;
+    bool ok = true;
+    const WalkConsts k = walk_consts(p, fetch_node<false>(p, 0, 0, 0, ok));
+    CkptVisitor vis;
+    vis.out = ckpt + pix * (size_t)per_ray;
+    vis.cap = per_ray;
+    vis.count = 0;
+    vis.last = 0;
+    vis.status = p.status;
+    RayState s;
+    s.dst = make_float4(0.f, 0.f, 0.f, 0.f);
+    s.nsamples = 0;
+    F3 pos;
+    if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s)) walk<FMT, false>(p, k, s, vis);
+    if (p.color) p.color[pix] = s.dst;
+    hdr[pix] = make_int2(vis.count, s.nsamples);
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(128) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
+                                                       const Ckpt* ckpt, int per_ray, const float4* dl_dcolor,
+                                                       float4* grad) {
+    int px, py;
+    pixel_of(px, py);
+    const vv_uniforms& u = p.u;
+    if (px >= u.width || py >= u.height) return;
+    const size_t pix = (size_t)py * u.width + px;
+    const int2 h = hdr[pix];
+    const int C = h.x, total = h.y;
+    if (C == 0 || total == 0) return;
+    float4 g = dl_dcolor[pix];
+    if (g.x == 0.f && g.y == 0.f && g.z == 0.f && g.w == 0.f) return;
+    bool ok = true;
+    const WalkConsts k = walk_consts(p, fetch_node<false>(p, 0, 0, 0, ok));
+    RayState s0;
+    F3 pos;
+    if (!ray_origin(u, k, px, py, pos)) return;
+    ray_start(p, k, px, py, pos, s0);  // direction and brick step of this ray
+    const Ckpt* ck = ckpt + pix * (size_t)per_ray;
+    ReplayVisitor rv;
+    for (int c = C - 1; c >= 0; --c) {
+        const Ckpt cc = ck[c];
+        const int a = (int)cc.c.x, b = c + 1 < C ? (int)ck[c + 1].c.x : total;
+        for (int m = (b - a - 1) / kPiece; m >= 0; --m) {
+            RayState s = s0;
+            s.pos = f3(cc.a.x, cc.a.y, cc.a.z);
+            s.dst = make_float4(cc.a.w, cc.b.x, cc.b.y, cc.b.z);
+            s.iter = __float_as_int(cc.b.w);
+            s.nsamples = a;
+            s.nptr_x = cc.c.y;
+            s.nptr_y = cc.c.z;
+            s.nptr_z = cc.c.w;
+            rv.first = a + m * kPiece;
+            rv.last = min(b, rv.first + kPiece);
+            rv.n = 0;
+            walk<FMT, false>(p, k, s, rv);
+            for (int j = rv.n - 1; j >= 0; --j) {
+                const float t = rv.T[j];
+                const float4 sv = rv.src[j];
+                if (rv.brick[j]) scatter_texels(p, rv.bpos[j], make_float4(g.x * t, g.y * t, g.z * t, g.w * t), grad);
+                g.w = g.w - (g.x * sv.x + g.y * sv.y + g.z * sv.z + g.w * sv.w);
+            }
+        }
+    }
+}
+
+size_t ckpt_bytes(int w, int h, int per_ray) {
+    return (size_t)w * h * (sizeof(int2) + (size_t)per_ray * sizeof(Ckpt));
+}
+
+cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int per_ray, cudaStream_t s) {
+    const int W = p.u.width, H = p.u.height;
+    int2* hdr = (int2*)ckpt;
+    Ckpt* ck = (Ckpt*)((char*)ckpt + (size_t)W * H * sizeof(int2));
+    dim3 block(128), grid((unsigned)((W + 15) / 16), (unsigned)((H + 7) / 8));
+    switch (fmt) {
+        case VV_FMT_RGBA8: forward_ckpt_kernel<VV_FMT_RGBA8><<<grid, block, 0, s>>>(p, hdr, ck, per_ray); break;
+        case VV_FMT_FP16: forward_ckpt_kernel<VV_FMT_FP16><<<grid, block, 0, s>>>(p, hdr, ck, per_ray); break;
+        case VV_FMT_BF16: forward_ckpt_kernel<VV_FMT_BF16><<<grid, block, 0, s>>>(p, hdr, ck, per_ray); break;
+        case VV_FMT_FP32: forward_ckpt_kernel<VV_FMT_FP32><<<grid, block, 0, s>>>(p, hdr, ck, per_ray); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward(int fmt, const RaycastParams& p, const void* ckpt, int per_ray, const float4* dl_dcolor,
+                            float4* grad, cudaStream_t s) {
+    const int W = p.u.width, H = p.u.height;
+    const int2* hdr = (const int2*)ckpt;
+    const Ckpt* ck = (const Ckpt*)((const char*)ckpt + (size_t)W * H * sizeof(int2));
+    dim3 block(128), grid((unsigned)((W + 15) / 16), (unsigned)((H + 7) / 8));
+    switch (fmt) {
+        case VV_FMT_RGBA8: backward_kernel<VV_FMT_RGBA8><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
+        case VV_FMT_FP16: backward_kernel<VV_FMT_FP16><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
+        case VV_FMT_BF16: backward_kernel<VV_FMT_BF16><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
+        case VV_FMT_FP32: backward_kernel<VV_FMT_FP32><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace vv

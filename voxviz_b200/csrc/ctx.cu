@@ -135,7 +135,7 @@ int vv_ctx_destroy(vv_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (auto& t : c->trees)
         if (t.nodes) cudaFree(t.nodes);
-    if (c->bricks) cudaFree(c->bricks);
+    if (c->bricks && !c->bricks_external) cudaFree(c->bricks);
     void* bufs[] = {c->d_status, c->d_jitter, c->d_usage, c->d_mask, c->d_counts, c->d_offsets,
                     c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words};
     for (void* b : bufs)
@@ -244,9 +244,10 @@ int vv_brickpool_create(vv_ctx* c, int32_t sx, int32_t sy, int32_t sz, int32_t f
     cudaSetDevice(c->device);
     if (c->bricks) {
         VV_CUDA(c, cudaStreamSynchronize(c->stream));
-        cudaFree(c->bricks);
+        if (!c->bricks_external) cudaFree(c->bricks);
         c->bricks = nullptr;
     }
+    c->bricks_external = false;
     const long long total = (long long)sx * sy * sz;
     const size_t bytes = (size_t)total * VV_BRICK_TEXELS * tb;
     cudaError_t e = cudaMalloc(&c->bricks, bytes);
@@ -299,6 +300,86 @@ int vv_brickpool_download(vv_ctx* c, void* texels) {
     cudaSetDevice(c->device);
     VV_CUDA(c, cudaMemcpyAsync(texels, c->bricks, c->pool_bytes, cudaMemcpyDeviceToHost, c->stream));
     VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_brickpool_attach(vv_ctx* c, void* texels, int32_t sx, int32_t sy, int32_t sz, int32_t fmt) {
+    if (!c || !texels) return fail(c, VV_ERR_ARG, "bad attach arguments");
+    if (sx <= 0 || sy <= 0 || sz <= 0 || sx * 10 > 1023 || sy * 10 > 1023 || sz * 10 > 1023)
+        return fail(c, VV_ERR_ARG, "brick pool slots per axis must be in [1,102]");
+    const size_t tb = fmt_texel_bytes(fmt);
+    if (!tb) return fail(c, VV_ERR_ARG, "unknown brick format");
+    if (((uintptr_t)texels & 15u) != 0) return fail(c, VV_ERR_ARG, "attached pool must be 16-byte aligned");
+    cudaSetDevice(c->device);
+    // Launches already queued hold the old pointer by value; only an owned
+    // pool has to outlive them before it is freed.
+    if (c->bricks && !c->bricks_external) {
+        VV_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->bricks);
+    }
+    c->bricks = texels;
+    c->bricks_external = true;
+    c->slots[0] = sx;
+    c->slots[1] = sy;
+    c->slots[2] = sz;
+    c->total_slots = (long long)sx * sy * sz;
+    c->fmt = fmt;
+    c->brick_bytes = VV_BRICK_TEXELS * tb;
+    c->pool_bytes = (size_t)c->total_slots * VV_BRICK_TEXELS * tb;
+    return VV_OK;
+}
+
+size_t vv_ckpt_bytes(int32_t width, int32_t height, int32_t per_ray) {
+    if (width <= 0 || height <= 0 || per_ray <= 0) return 0;
+    return ckpt_bytes(width, height, per_ray);
+}
+
+// Shared set-up of the differentiable passes.
+static int diff_params(vv_ctx* c, int32_t tree, const vv_uniforms* u, RaycastParams& p) {
+    if (!c || !u || tree < 0 || tree >= VV_MAX_TREES) return fail(c, VV_ERR_ARG, "bad arguments");
+    const DeviceTree& t = c->trees[tree];
+    if (!t.nodes || !c->bricks) return fail(c, VV_ERR_STATE, "pools not ready");
+    if (u->width <= 0 || u->height <= 0) return fail(c, VV_ERR_ARG, "bad viewport");
+    if (u->jitter_tex_size != c->jitter_size) return fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
+    for (int a = 0; a < 3; ++a)
+        if (u->brick_pool_dimension[a] != (float)(c->slots[a] * 10))
+            return fail(c, VV_ERR_ARG, "brick_pool_dimension does not match the brick pool");
+    std::memset(&p, 0, sizeof(p));
+    p.u = *u;
+    p.nodes = t.nodes;
+    for (int a = 0; a < 3; ++a) {
+        p.node_dim[a] = t.dim[a];
+        p.slots[a] = c->slots[a];
+    }
+    p.bricks = c->bricks;
+    p.jitter = c->d_jitter;
+    p.status = c->d_status;
+    p.max_iter = vv_max_iterations(u);
+    return VV_OK;
+}
+
+int vv_render_forward_ckpt(vv_ctx* c, int32_t tree, const vv_uniforms* u, float* color, void* ckpt,
+                           int32_t per_ray) {
+    RaycastParams p;
+    int rc = diff_params(c, tree, u, p);
+    if (rc) return rc;
+    if (!ckpt || per_ray <= 0) return fail(c, VV_ERR_ARG, "checkpoint buffer required");
+    cudaSetDevice(c->device);
+    p.color = (float4*)color;
+    VV_CUDA(c, launch_forward_ckpt(c->fmt, p, ckpt, per_ray, c->stream));
+    return VV_OK;
+}
+
+int vv_backward(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* dl_dcolor, const void* ckpt,
+                int32_t per_ray, float* grad_texels) {
+    RaycastParams p;
+    int rc = diff_params(c, tree, u, p);
+    if (rc) return rc;
+    if (!ckpt || per_ray <= 0 || !dl_dcolor || !grad_texels) return fail(c, VV_ERR_ARG, "bad backward buffers");
+    if (((uintptr_t)grad_texels & 15u) != 0 || ((uintptr_t)dl_dcolor & 15u) != 0)
+        return fail(c, VV_ERR_ARG, "gradient buffers must be 16-byte aligned");
+    cudaSetDevice(c->device);
+    VV_CUDA(c, launch_backward(c->fmt, p, ckpt, per_ray, (const float4*)dl_dcolor, (float4*)grad_texels, c->stream));
     return VV_OK;
 }
 

@@ -28,6 +28,7 @@ struct vv_ctx {
     vv::DeviceTree trees[VV_MAX_TREES];
     // brick pool
     void* bricks = nullptr;
+    bool bricks_external = false;  // attached caller memory: never freed here
     int slots[3] = {0, 0, 0};
     long long total_slots = 0;
     int fmt = VV_FMT_RGBA8;

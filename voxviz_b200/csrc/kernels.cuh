@@ -41,6 +41,11 @@ struct CompactParams {
 };
 
 cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s);
+// Differentiable forward (colour + per-ray checkpoints) and its adjoint.
+size_t ckpt_bytes(int w, int h, int per_ray);
+cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int per_ray, cudaStream_t s);
+cudaError_t launch_backward(int fmt, const RaycastParams& p, const void* ckpt, int per_ray, const float4* dl_dcolor,
+                            float4* grad, cudaStream_t s);
 cudaError_t launch_select(const uint4* usage, uint32_t* mask, uint32_t* level0, int w, int h,
                           cudaStream_t s);
 cudaError_t launch_compact(const CompactParams& p, cudaStream_t s);

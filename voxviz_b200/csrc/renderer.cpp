@@ -160,6 +160,8 @@ GigaVoxelsRenderer::~GigaVoxelsRenderer() {
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h_stage_) cudaFreeHost(h_stage_);
+    if (h_small_) cudaFreeHost(h_small_);
+    if (h_unique_) cudaFreeHost(h_unique_);
     void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, dd_.count, d_jobs_};
     for (void* b : dbufs)
         if (b) cudaFree(b);
@@ -437,18 +439,29 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload)
     }
     const int* pd = tree_->pool_dim();
     if (launch_dedupe(d_requests, (int)n, pd, dd_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
-    uint32_t u = 0;
-    if (cudaMemcpyAsync(&u, dd_.count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    // read-backs land in pinned memory (pageable copies are staged and slow)
+    if (cudaMemcpyAsync(h_small_ + 1, dd_.count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
     if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
-    unique_host_.resize(u);
+    const uint32_t u = h_small_[1];
+    if (h_unique_cap_ < u) {
+        if (h_unique_) cudaFreeHost(h_unique_);
+        h_unique_ = nullptr;
+        h_unique_cap_ = std::max((size_t)u, 2 * h_unique_cap_);
+        if (cudaMallocHost((void**)&h_unique_, h_unique_cap_ * 4) != cudaSuccess) {
+            h_unique_cap_ = 0;
+            return VV_ERR_OOM;
+        }
+    }
     if (u) {
-        if (cudaMemcpyAsync(unique_host_.data(), dd_.unique, (size_t)u * 4, cudaMemcpyDeviceToHost, ctx_->stream) !=
+        if (cudaMemcpyAsync(h_unique_, dd_.unique, (size_t)u * 4, cudaMemcpyDeviceToHost, ctx_->stream) !=
             cudaSuccess)
             return VV_ERR_CUDA;
         if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     }
     const uint32_t dx = (uint32_t)pd[0], dy = (uint32_t)pd[1];
-    for (uint32_t g : unique_host_) {
+    for (uint32_t k = 0; k < u; ++k) {
+        const uint32_t g = h_unique_[k];
         const uint32_t nidx = tree_->index_of(g % dx, (g / dx) % dy, g / (dx * dy));
         if (nidx == kNoParent || tree_->level(nidx) < 0) continue;
         visit(nidx, upload);
@@ -459,9 +472,11 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload)
 int GigaVoxelsRenderer::update() {
     if (!d_count) return VV_ERR_STATE;
     uploaded_ = 0;
-    uint32_t count = 0;
-    if (cudaMemcpyAsync(&count, d_count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if (!h_small_ && cudaMallocHost((void**)&h_small_, 16) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMemcpyAsync(h_small_, d_count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
     if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    const uint32_t count = h_small_[0];
     const auto t0 = std::chrono::steady_clock::now();  // the draw has finished here
     active_ = count;
     const uint32_t n = std::min<uint32_t>(count, (uint32_t)cap_);

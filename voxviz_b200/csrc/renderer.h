@@ -97,7 +97,9 @@ private:
     bool device_paging_ = false;
     std::unique_ptr<DeviceTerrain> dterrain_;
     DedupeBuffers dd_;
-    std::vector<uint32_t> unique_host_;
+    uint32_t* h_small_ = nullptr;   // pinned: request count, distinct count
+    uint32_t* h_unique_ = nullptr;  // pinned: distinct node cells of the last frame
+    size_t h_unique_cap_ = 0;
     std::vector<uint4> jobs_;
     uint4* d_jobs_ = nullptr;
     size_t jobs_cap_ = 0;

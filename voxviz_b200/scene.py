@@ -135,3 +135,19 @@ def camera_path(seed: int, heights: np.ndarray, frames: int, width: int, height:
         look, up = look_at(eye, target)
         cams.append(make_camera(eye, look, up, width, height, frame=f, near=near))
     return cams
+
+
+def converge_views(renderer, cams, max_passes: int = 64) -> int:
+    """Draw every view and service its page requests until one whole pass
+    over the views uploads no brick (the paging fixed point of
+    GigaVoxelsRenderer::postDraw + BrickPool::update for that view set).
+    Returns the number of passes; raises if the pool cannot hold the set."""
+    for p in range(1, max_passes + 1):
+        uploaded = 0
+        for cam in cams:
+            renderer.draw(cam)
+            renderer.update()
+            uploaded += renderer.stats()["bricks_uploaded"]
+        if uploaded == 0:
+            return p
+    raise RuntimeError(f"paging did not converge in {max_passes} passes over {len(cams)} views")
