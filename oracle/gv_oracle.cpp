@@ -667,6 +667,106 @@ int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, i
 
 int oracle_max_iterations(const vv_uniforms* u) { return max_iterations(u); }
 
+namespace {
+
+// binary64 GL_LINEAR + CLAMP_TO_EDGE sample of `vals` at the binary32
+// texture coordinate bpos (the taps and weights of texture(), in double).
+void sample64(const BrickTexture<double>& bt, const float N[3], const float bpos[3], double out[4]) {
+    const int n[3] = {bt.sx * 10, bt.sy * 10, bt.sz * 10};
+    int i0[3], i1[3];
+    double w[3];
+    for (int a = 0; a < 3; ++a) {
+        double t = (double)bpos[a] * (double)N[a] - 0.5;
+        t = std::fmin(std::fmax(t, -1.0), (double)N[a]);
+        const double fl = std::floor(t);
+        w[a] = t - fl;
+        const int k = (int)fl;
+        i0[a] = std::min(std::max(k, 0), n[a] - 1);
+        i1[a] = std::min(std::max(k + 1, 0), n[a] - 1);
+    }
+    double acc[4] = {0, 0, 0, 0};
+    for (int t8 = 0; t8 < 8; ++t8) {
+        const int bx = t8 & 1, by = (t8 >> 1) & 1, bz = t8 >> 2;
+        const double wt = (bx ? w[0] : 1.0 - w[0]) * (by ? w[1] : 1.0 - w[1]) * (bz ? w[2] : 1.0 - w[2]);
+        const vec4<double> v = bt.fetch(bx ? i1[0] : i0[0], by ? i1[1] : i0[1], bz ? i1[2] : i0[2]);
+        acc[0] += wt * v.r;
+        acc[1] += wt * v.g;
+        acc[2] += wt * v.b;
+        acc[3] += wt * v.a;
+    }
+    const double k = bt.fmt == VV_FMT_RGBA8 ? 1.0 / 255.0 : 1.0;
+    for (int c = 0; c < 4; ++c) out[c] = acc[c] * k;
+}
+
+}  // namespace
+
+// The binary32 ray cast's sample sequence (descent, LOD choices, step
+// counts, sample positions, early termination: all taken from `traj`)
+// re-evaluated in binary64: brick samples are filtered in double from the
+// texels of `vals` (same pool layout) and every sample is composited in
+// double.  With vals == traj this isolates the arithmetic error of the
+// binary32 sampler and compositing; with vals a perturbed copy it is a
+// smooth function of the texels (the control flow is fixed), which is what
+// finite differences of the adjoint need.
+int oracle_fixed_path(const vv_uniforms* u, const oracle_scene* traj, const oracle_scene* vals, int row0, int row1,
+                      double* color, int threads) {
+    if (!u || !traj || !vals || !color || row0 < 0 || row1 > u->height || row0 > row1) return VV_ERR_ARG;
+    if (vals->slots[0] != traj->slots[0] || vals->slots[1] != traj->slots[1] || vals->slots[2] != traj->slots[2])
+        return VV_ERR_ARG;
+    Shader<float> base;
+    base.init(u);
+    base.nodes = traj->nodes;
+    for (int a = 0; a < 3; ++a) base.ndim[a] = traj->node_dim[a];
+    base.brick.data = traj->bricks;
+    base.brick.fmt = traj->fmt;
+    base.brick.sx = traj->slots[0];
+    base.brick.sy = traj->slots[1];
+    base.brick.sz = traj->slots[2];
+    base.jitter = traj->jitter;
+    base.max_iter = max_iterations(u);
+    int st = 0;
+    base.status = &st;
+    BrickTexture<double> bt;
+    bt.data = vals->bricks;
+    bt.fmt = vals->fmt;
+    bt.sx = vals->slots[0];
+    bt.sy = vals->slots[1];
+    bt.sz = vals->slots[2];
+    const float N[3] = {u->brick_pool_dimension[0], u->brick_pool_dimension[1], u->brick_pool_dimension[2]};
+    const int W = u->width;
+#ifdef _OPENMP
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel num_threads(nt)
+#endif
+    {
+        Shader<float> sh = base;
+        std::vector<SampleRec> tape;
+        sh.tape = &tape;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+        for (int y = row0; y < row1; ++y)
+            for (int x = 0; x < W; ++x) {
+                tape.clear();
+                vec4<float> c;
+                uint32_t lst[12];
+                sh.main(x, y, c, lst);
+                double d[4] = {0, 0, 0, 0};
+                for (const SampleRec& r : tape) {
+                    double s[4];
+                    if (r.brick) sample64(bt, N, r.bpos, s);
+                    else
+                        for (int k = 0; k < 4; ++k) s[k] = r.src[k];
+                    const double T = 1.0 - d[3];
+                    for (int k = 0; k < 4; ++k) d[k] = T * s[k] + d[k];
+                }
+                double* o = color + 4 * ((size_t)y * W + x);
+                for (int k = 0; k < 4; ++k) o[k] = d[k];
+            }
+    }
+    return st;
+}
+
 // Adjoint of the binary32 ray cast in binary64: the forward runs exactly as
 // oracle_raycast(precision 32) and records its samples; the backward walks
 // them in reverse, g_k.a = g_{k+1}.a - dot(g_{k+1}, src_k), dL/dsrc_k =

@@ -22,6 +22,11 @@ typedef struct oracle_scene {
 int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
                    void* color, uint32_t* usage, int threads, int32_t* status);
 int oracle_max_iterations(const vv_uniforms* u);
+/* The binary32 ray cast's sample sequence from `traj` re-evaluated in
+ * binary64 with texel values from `vals` (same layout): 4 doubles per pixel
+ * for rows [row0,row1) of a full-image buffer. */
+int oracle_fixed_path(const vv_uniforms* u, const oracle_scene* traj, const oracle_scene* vals, int row0,
+                      int row1, double* color, int threads);
 /* Adjoint of the binary32 ray cast with binary64 accumulation: ADDS
  * dL/d(texel) (4 doubles per pool texel, slot-major) for rows [row0,row1)
  * given dL/d(colour) (4 floats per pixel).  Single-threaded. */

@@ -54,6 +54,9 @@ def load() -> C.CDLL:
     lib.oracle_backward.restype = C.c_int
     lib.oracle_backward.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_void_p, C.c_void_p, C.c_int,
                                     C.c_int]
+    lib.oracle_fixed_path.restype = C.c_int
+    lib.oracle_fixed_path.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.POINTER(OracleScene), C.c_int,
+                                      C.c_int, C.c_void_p, C.c_int]
     lib.oracle_select.restype = C.c_int
     lib.oracle_select.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     lib.oracle_compress.restype = C.c_int
@@ -113,6 +116,19 @@ def backward(u, scene: Scene, dl_dcolor: np.ndarray, rows=None, grad: np.ndarray
     if rc != 0:
         raise RuntimeError(f"oracle_backward failed: {rc}")
     return grad
+
+
+def fixed_path(u, traj: Scene, vals: Scene | None = None, rows=None, threads: int = 0,
+               out: np.ndarray | None = None) -> np.ndarray:
+    """(H,W,4) float64: the binary32 sample sequence of `traj` composited in
+    binary64 with the texels of `vals` (default: traj's own)."""
+    lib = load()
+    r0, r1 = (0, u.height) if rows is None else rows
+    color = np.zeros((u.height, u.width, 4), dtype=np.float64) if out is None else out
+    rc = lib.oracle_fixed_path(C.byref(u), C.byref(traj.s), C.byref((vals or traj).s), r0, r1, _p(color), threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_fixed_path failed: {rc}")
+    return color
 
 
 def select(usage: np.ndarray) -> np.ndarray:

@@ -250,6 +250,8 @@ __device__ __forceinline__ uint2 fetch_node(const RaycastParams& p, uint32_t x, 
 //                                          false ends the walk after it
 //   void segment_end(const RayState&, bool is_const, bool loaded)
 //   void fail(int code)
+// STEPS unrolls the two march loops (samples issued per loop trip); the
+// results do not depend on it.
 
 struct WalkConsts {
     F3 C, vmin, vmax, up, left, bdim, pdim;
@@ -347,7 +349,7 @@ __device__ __forceinline__ bool ray_start(const RaycastParams& p, const WalkCons
     return inside_box(s.pos, k.vmin, k.vmax);
 }
 
-template <int FMT, bool COUNT, class V>
+template <int FMT, bool COUNT, class V, int STEPS = 1>
 __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis) {
     bool ok = true;
     for (;;) {
@@ -417,6 +419,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                 const float4 src = make_float4((float)(node.y & 255u) / 255.0f * ratio,
                                                (float)((node.y >> 8) & 255u) / 255.0f * ratio,
                                                (float)((node.y >> 16) & 255u) / 255.0f * ratio, sa);
+#pragma unroll(STEPS)
                 for (int i = 0; i < n; ++i) {
                     s.pos = add(s.pos, wstep);
                     if (s.dst.w > k.astop) {
@@ -453,6 +456,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             } else {
                 base[0] = base[1] = base[2] = -100000;
             }
+#pragma unroll(STEPS)
             for (int i = 0; i < n; ++i) {
                 s.pos = add(s.pos, wstep);
                 if (s.dst.w > k.astop) {
