@@ -247,6 +247,46 @@ int vv_backward(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl
 int vv_brickpool_attach(vv_ctx* ctx, void* texels, int32_t slots_x, int32_t slots_y,
                         int32_t slots_z, int32_t fmt);
 
+/* ---- batched persistent ray cast ----------------------------------------- */
+
+/* No counterpart in the reference (one drawVolume per octree per frame,
+ * GigaVoxelsRenderer.cpp:1584-1935): many views of many octrees in ONE
+ * launch.  A persistent grid pulls tile_w x tile_h pixel tiles of all views
+ * from a device work queue; each pixel runs exactly the vv_render ray cast
+ * of its view (colour and usage lists bit-identical to a per-view
+ * vv_render with VV_PASS_RAYCAST).  Every view names the context holding
+ * its octree's node pool (`tree`) and brick pool; all contexts must be on
+ * the launching context's device and share one brick format.  The launch
+ * runs on `ctx`'s stream and uses its scratch; the selection and
+ * compaction passes of a view run afterwards through vv_render with
+ * passes = VV_PASS_SELECT | VV_PASS_COMPACT on the same usage buffer. */
+typedef struct vv_batch_view {
+    vv_ctx* ctx;            /* context owning this view's pools           */
+    int32_t tree;           /* node pool index in that context            */
+    int32_t pad;
+    vv_uniforms u;          /* the view's uniforms (as for vv_render)     */
+    float* color;           /* device, 4 floats per pixel, or NULL        */
+    uint32_t* usage;        /* device, 12 words per pixel, or NULL        */
+} vv_batch_view;
+
+typedef struct vv_batch_config {
+    int32_t tile_w, tile_h;  /* pixel tile of one CTA: 8x8, 16x8, 16x16, 32x8 */
+    int32_t steps;           /* march samples per loop trip: 1, 2 or 4      */
+    int32_t ctas_per_sm;     /* resident CTAs per SM; 0 = occupancy limit   */
+} vv_batch_config;
+
+/* The compiled (tile_w, tile_h, steps) variants; returns their count and
+ * writes up to `cap` of them. */
+int32_t vv_batch_variants(vv_batch_config* out, int32_t cap);
+int vv_render_batch(vv_ctx* ctx, const vv_batch_view* views, int32_t n, const vv_batch_config* cfg);
+/* Times every compiled variant on this batch (one untimed launch, then
+ * `reps` timed launches each, CUDA events on ctx's stream) and returns the
+ * fastest in `best`.  `ms` (may be NULL) receives the mean launch time of
+ * each variant in vv_batch_variants order.  The views' outputs hold the
+ * last launch's results. */
+int vv_batch_autotune(vv_ctx* ctx, const vv_batch_view* views, int32_t n, int32_t reps,
+                      vv_batch_config* best, float* ms);
+
 /* ---- page-request compaction without allocation ------------------------- */
 
 /* This entry point has no counterpart in the reference.  It is for callers

@@ -34,6 +34,7 @@ STRUCTS = {
     "vv_uniforms": N.Uniforms, "vv_node_patch": N.NodePatch, "vv_frame_out": N.FrameOut, "vv_params": N.Params,
     "vv_terrain_desc": N.TerrainDesc, "vv_octree_info": N.OctreeInfo, "vv_node_info": N.NodeInfo,
     "vv_camera": N.Camera, "vv_renderer_desc": N.RendererDesc, "vv_renderer_stats": N.RendererStats,
+    "vv_batch_view": N.BatchView, "vv_batch_config": N.BatchConfig,
 }
 
 

@@ -25,8 +25,9 @@ from ._native import (FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_FP16, VV_FMT_F
                       VV_PASS_ALL, VV_PASS_COMPACT, VV_PASS_RAYCAST, VV_PASS_SELECT, Camera, FrameOut,
                       NodePatch, OctreeInfo, Uniforms, VVError)
 
-__all__ = ["Octree", "Context", "Renderer", "make_camera", "look_at", "compute_uniforms", "make_jitter",
-           "pixel_size", "lib", "VVError", "Uniforms", "Camera", "FMT_NAMES", "TEXEL_BYTES"]
+__all__ = ["Octree", "Context", "Renderer", "Batch", "batch_variants", "make_camera", "look_at",
+           "compute_uniforms", "make_jitter", "pixel_size", "lib", "VVError", "Uniforms", "Camera", "FMT_NAMES",
+           "TEXEL_BYTES"]
 
 
 def lib() -> C.CDLL:
@@ -321,6 +322,57 @@ class Context:
                  tree: int = 0) -> None:
         self._ck(lib().vv_backward(self._h, tree, C.byref(u), C.c_void_p(dl_dcolor), C.c_void_p(ckpt), per_ray,
                                    C.c_void_p(grad_texels)), "backward")
+
+
+# --------------------------------------------------------------- batches ---
+
+def batch_variants() -> list[tuple[int, int, int]]:
+    """The compiled (tile_w, tile_h, steps) variants of the batched launch."""
+    n = lib().vv_batch_variants(None, 0)
+    arr = (N.BatchConfig * n)()
+    lib().vv_batch_variants(arr, n)
+    return [(c.tile_w, c.tile_h, c.steps) for c in arr]
+
+
+class Batch:
+    """Many views of many octrees rendered by one persistent launch.
+
+    ``views`` holds (context, tree, uniforms, colour device pointer, usage
+    device pointer) tuples; the launch runs on ``ctx``'s stream."""
+
+    def __init__(self, ctx: Context, views: Sequence[tuple]):
+        self.ctx = ctx
+        self.n = len(views)
+        self._arr = (N.BatchView * self.n)()
+        self._keep = []
+        for i, (vctx, tree, u, color, usage) in enumerate(views):
+            self._arr[i].ctx = vctx.handle
+            self._arr[i].tree = tree
+            self._arr[i].u = u
+            self._arr[i].color = color or None
+            self._arr[i].usage = usage or None
+            self._keep.append(vctx)
+        self.config = N.BatchConfig(tile_w=16, tile_h=16, steps=1, ctas_per_sm=0)
+
+    def set_uniforms(self, i: int, u: Uniforms) -> None:
+        self._arr[i].u = u
+
+    def render(self, config: tuple[int, int, int] | None = None, ctas_per_sm: int = 0) -> None:
+        cfg = self.config if config is None else N.BatchConfig(tile_w=config[0], tile_h=config[1],
+                                                               steps=config[2], ctas_per_sm=ctas_per_sm)
+        _check(lib().vv_render_batch(self.ctx.handle, self._arr, self.n, C.byref(cfg)), self.ctx.handle,
+               "batched render")
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Time every compiled variant on this batch; keep and return the fastest."""
+        variants = batch_variants()
+        ms = (C.c_float * len(variants))()
+        best = N.BatchConfig()
+        _check(lib().vv_batch_autotune(self.ctx.handle, self._arr, self.n, reps, C.byref(best), ms),
+               self.ctx.handle, "batch autotune")
+        self.config = best
+        return {"best": (best.tile_w, best.tile_h, best.steps),
+                "ms": {f"{w}x{h}/s{s}": round(float(t), 4) for (w, h, s), t in zip(variants, ms)}}
 
 
 # -------------------------------------------------------------- renderer ---

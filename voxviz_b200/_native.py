@@ -154,6 +154,21 @@ class RendererStats(C.Structure):
     ]
 
 
+class BatchView(C.Structure):
+    _fields_ = [
+        ("ctx", C.c_void_p),
+        ("tree", C.c_int32),
+        ("pad", C.c_int32),
+        ("u", Uniforms),
+        ("color", C.c_void_p),
+        ("usage", C.c_void_p),
+    ]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("tile_w", C.c_int32), ("tile_h", C.c_int32), ("steps", C.c_int32), ("ctas_per_sm", C.c_int32)]
+
+
 P = C.c_void_p
 u32p = C.POINTER(C.c_uint32)
 i32p = C.POINTER(C.c_int32)
@@ -186,6 +201,10 @@ SIGNATURES = {
     "vv_render_forward_ckpt": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32]),
     "vv_backward": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32, P]),
     "vv_brickpool_attach": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "vv_batch_variants": (C.c_int32, [C.POINTER(BatchConfig), C.c_int32]),
+    "vv_render_batch": (C.c_int, [P, C.POINTER(BatchView), C.c_int32, C.POINTER(BatchConfig)]),
+    "vv_batch_autotune": (C.c_int, [P, C.POINTER(BatchView), C.c_int32, C.c_int32, C.POINTER(BatchConfig),
+                                    C.POINTER(C.c_float)]),
     "vv_ctx_last_times": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "vv_measure_footprint": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int64)]),

@@ -25,7 +25,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 HOST_CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
 
-CU_SOURCES = ["kernels.cu", "ctx.cu", "noalloc.cu", "production.cu", "adjoint.cu"]
+CU_SOURCES = ["kernels.cu", "ctx.cu", "noalloc.cu", "production.cu", "adjoint.cu", "batch.cu"]
 CPP_SOURCES = ["terrain.cpp", "octree.cpp", "renderer.cpp", "capi.cpp"]
 HEADERS = ["kernels.cuh", "ctx.h", "terrain.h", "octree.h", "renderer.h", "production.h", "raycast_common.cuh"]
 

@@ -80,6 +80,14 @@ int ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes) {
 
 }  // namespace
 
+namespace vv {
+int ctx_fail(vv_ctx* c, int code, const std::string& msg) { return fail(c, code, msg); }
+int ctx_ensure(vv_ctx* c, void** ptr, size_t* cap, size_t bytes, const char* what) {
+    return ensure(c, ptr, cap, bytes, what);
+}
+int ctx_ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes) { return ensure_host(c, ptr, cap, bytes); }
+}  // namespace vv
+
 extern "C" {
 
 int vv_abi_version(void) { return VV_ABI_VERSION; }
@@ -137,10 +145,12 @@ int vv_ctx_destroy(vv_ctx* c) {
         if (t.nodes) cudaFree(t.nodes);
     if (c->bricks && !c->bricks_external) cudaFree(c->bricks);
     void* bufs[] = {c->d_status, c->d_jitter, c->d_usage, c->d_mask, c->d_counts, c->d_offsets,
-                    c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words};
+                    c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words, c->d_batch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->h_batch) cudaFreeHost(c->h_batch);
+    if (c->batch_ev) cudaEventDestroy(c->batch_ev);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     delete c;

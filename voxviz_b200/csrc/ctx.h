@@ -18,6 +18,11 @@ struct DeviceTree {
 
 int vv_max_iterations(const vv_uniforms* u);
 
+// Error and scratch helpers of ctx.cu for the other translation units.
+int ctx_fail(vv_ctx* c, int code, const std::string& msg);
+int ctx_ensure(vv_ctx* c, void** ptr, size_t* cap, size_t bytes, const char* what);
+int ctx_ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes);
+
 }  // namespace vv
 
 struct vv_ctx {
@@ -56,6 +61,13 @@ struct vv_ctx {
     size_t grid_words_cap = 0;
     void* h_stage = nullptr;
     size_t h_stage_cap = 0;
+    // batched launch: per-view parameters (pinned staging -> device) + queue
+    void* h_batch = nullptr;
+    size_t h_batch_cap = 0;
+    void* d_batch = nullptr;
+    size_t d_batch_cap = 0;
+    cudaEvent_t batch_ev = nullptr;  // recorded after the staging copy
+    bool batch_ev_live = false;
     // profiling
     bool profiling = false;
     bool timed = false;

@@ -482,5 +482,58 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
     }
 }
 
+// Visitor of the forward draw: AddToNodeUsageList (:454-488) for the leaf
+// segments whose traversal index falls in this pixel's window (:663-671).
+struct UsageVisitor {
+    uint32_t usage[12];
+    int list_slot, nl_count, pushed, start_push, max_push;
+    int* status;
+    __device__ __forceinline__ bool segment_begin(const RayState&) { return true; }
+    __device__ __forceinline__ bool sample(int, const float4&, F3, float, int) { return true; }
+    __device__ __forceinline__ void segment_end(const RayState& s, bool, bool) {
+        if (nl_count >= start_push && nl_count < start_push + 12 && pushed < max_push) {
+            ++pushed;
+            const uint32_t bits = ((s.nptr_x + 1u) << 20) | ((s.nptr_y + 1u) << 10) | (s.nptr_z + 1u);
+#pragma unroll
+            for (int i = 0; i < 12; ++i)
+                if (i == list_slot) usage[i] = bits;
+            list_slot = list_slot == 11 ? 0 : list_slot + 1;
+        }
+        if (++nl_count >= 48) nl_count = 0;
+    }
+    __device__ __forceinline__ void fail(int code) { set_status(status, code); }
+};
+
+// One pixel of the forward draw: the fragment's ray walk, FragColor and the
+// three RGBA32UI usage-list layers (:490-751).
+template <int FMT, bool COUNT, int STEPS>
+__device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int py) {
+    const vv_uniforms& u = p.u;
+    const size_t pix = (size_t)py * u.width + px;
+    bool ok = true;
+    const WalkConsts k = walk_consts(p, fetch_node<COUNT>(p, 0, 0, 0, ok));
+    UsageVisitor vis;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) vis.usage[i] = 0u;
+    vis.list_slot = 0;
+    vis.nl_count = 0;
+    vis.pushed = 0;
+    vis.start_push = (px % 2) * 12 + (py % 2) * 24;
+    vis.max_push = u.max_nodes_to_push;
+    vis.status = p.status;
+    RayState s;
+    s.dst = make_float4(0.f, 0.f, 0.f, 0.f);
+    F3 pos;
+    if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s))
+        walk<FMT, COUNT, UsageVisitor, STEPS>(p, k, s, vis);
+    if (p.color) p.color[pix] = s.dst;
+    if (p.usage) {
+        uint4* o = p.usage + pix * 3;
+        o[0] = make_uint4(vis.usage[0], vis.usage[1], vis.usage[2], vis.usage[3]);
+        o[1] = make_uint4(vis.usage[4], vis.usage[5], vis.usage[6], vis.usage[7]);
+        o[2] = make_uint4(vis.usage[8], vis.usage[9], vis.usage[10], vis.usage[11]);
+    }
+}
+
 }  // namespace rc
 }  // namespace vv

@@ -137,11 +137,13 @@ def camera_path(seed: int, heights: np.ndarray, frames: int, width: int, height:
     return cams
 
 
-def converge_views(renderer, cams, max_passes: int = 64) -> int:
+def converge_views(renderer, cams, max_passes: int = 64, strict: bool = True):
     """Draw every view and service its page requests until one whole pass
     over the views uploads no brick (the paging fixed point of
     GigaVoxelsRenderer::postDraw + BrickPool::update for that view set).
-    Returns the number of passes; raises if the pool cannot hold the set."""
+    Returns the number of passes.  When the pool cannot hold the set, raises
+    (strict) or returns (max_passes, bricks uploaded in the last pass)."""
+    uploaded = 0
     for p in range(1, max_passes + 1):
         uploaded = 0
         for cam in cams:
@@ -149,5 +151,7 @@ def converge_views(renderer, cams, max_passes: int = 64) -> int:
             renderer.update()
             uploaded += renderer.stats()["bricks_uploaded"]
         if uploaded == 0:
-            return p
-    raise RuntimeError(f"paging did not converge in {max_passes} passes over {len(cams)} views")
+            return p if strict else (p, 0)
+    if strict:
+        raise RuntimeError(f"paging did not converge in {max_passes} passes over {len(cams)} views")
+    return max_passes, uploaded
