@@ -764,21 +764,53 @@ def run_batched(args):
 
     ms_frame_eager = timed(frame)
     counts_eager = [int(cnt.item()) for _, _, cnt in req]
+    # paging in the graph: each terrain's renderer defers its uploads; the
+    # host services every view's requests and stages the uploads, the graph
+    # applies them (brick production + node patches) before the ray cast
+    for t in trees:
+        t["r"].set_deferred(True)
+        t["r"].stage_uploads()
+
+    def frame_with_uploads():
+        for t in trees:
+            t["r"].enqueue_uploads()
+        frame()
+
+    def service_all():
+        for (t, _), (_, _, u, _, _), (_, rq, cnt) in zip(views, items, req):
+            t["r"].service(rq.data_ptr(), cnt.data_ptr(), u.width * u.height)
+        for t in trees:
+            t["r"].stage_uploads()
+
     graph = torch.cuda.CUDAGraph()
     side = torch.cuda.Stream()
     side.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(side):
         for t in trees:
             t["ctx"].set_stream(side.cuda_stream)
-        frame()  # sizes every scratch buffer on the capture stream
+        frame_with_uploads()  # sizes every scratch buffer on the capture stream
         side.synchronize()
         with torch.cuda.graph(graph, stream=side):
-            frame()
-    for t in trees:
-        t["ctx"].set_stream(0)
+            frame_with_uploads()
     torch.cuda.synchronize()
     ms_frame_graph = timed(graph.replay)
     counts_graph = [int(cnt.item()) for _, _, cnt in req]
+    # whole frames: graph replay, then the host service of all 64 views
+    uploads = []
+    t0 = time.perf_counter()
+    paged_frames = 4
+    total_before = sum(t["r"].stats()["bricks_uploaded_total"] for t in trees)
+    for _ in range(paged_frames):
+        graph.replay()
+        torch.cuda.synchronize()
+        service_all()
+        total_now = sum(t["r"].stats()["bricks_uploaded_total"] for t in trees)
+        uploads.append(int(total_now - total_before))
+        total_before = total_now
+    torch.cuda.synchronize()
+    ms_frame_paged = (time.perf_counter() - t0) / paged_frames * 1e3
+    for t in trees:
+        t["ctx"].set_stream(0)
     launches_frame = 1 + sum(2 + 2 * (int(np.ceil(np.log2(max(u.width, u.height)))) + 1) for _, _, u, _, _ in items)
     status = max(t["ctx"].device_status() for t in trees)
     out = {
@@ -787,7 +819,9 @@ def run_batched(args):
         "per_view_mrays_s": round(rays / (ms_per_view / 1e3) / 1e6, 1),
         "ms": {"per_view_launches": round(ms_per_view, 3), "batched_autotuned": round(ms_batch, 3),
                "batched_16x16_s1": default_ms, "frame_eager": round(ms_frame_eager, 3),
-               "frame_graph": round(ms_frame_graph, 3)},
+               "frame_graph_with_staged_uploads": round(ms_frame_graph, 3),
+               "frame_graph_plus_host_service": round(ms_frame_paged, 3)},
+        "uploads_per_paged_frame": uploads,
         "autotune": tune, "bitexact_vs_per_view": exact,
         "graph_requests_equal_eager": counts_graph == counts_eager,
         "kernel_launches_per_frame": launches_frame, "status": status,

@@ -446,6 +446,23 @@ int vv_renderer_draw(vv_renderer* r, const vv_camera* cam);
  * NodeUsageListProcessor / BrickPool::update policy (deterministic LRU),
  * produce and upload bricks and patch node words. */
 int vv_renderer_update(vv_renderer* r);
+/* The same page-request service for a compacted list drawn outside the
+ * renderer (for example by vv_render_batch followed by vv_render with
+ * VV_PASS_SELECT | VV_PASS_COMPACT): `requests` (device, 4 words per
+ * entry), `count` (device, one word), at most `cap` entries read.  Needs
+ * device_paging.  May be called for several views per frame. */
+int vv_renderer_service(vv_renderer* r, const uint32_t* requests, const uint32_t* count, int32_t cap);
+/* Deferred uploads (no counterpart in the reference, whose BrickPool::update
+ * uploads at once): with `on`, update/service only choose bricks and node
+ * words; vv_renderer_stage_uploads writes the frame's production jobs and
+ * node patches to pinned mapped host memory and vv_renderer_enqueue_uploads
+ * enqueues the device side on the context's stream.  The enqueued work reads
+ * the staged counts on the device, so it can be captured once into a CUDA
+ * graph and replayed every frame after staging.  The host must not stage
+ * again until the previous enqueue (or replay) has completed. */
+int vv_renderer_set_deferred(vv_renderer* r, int32_t on);
+int vv_renderer_stage_uploads(vv_renderer* r);
+int vv_renderer_enqueue_uploads(vv_renderer* r);
 int vv_renderer_get_stats(const vv_renderer* r, vv_renderer_stats* out);
 /* Device pointers of the last frame's buffers (valid until next draw). */
 int vv_renderer_frame_buffers(vv_renderer* r, float** color, uint32_t** usage,

@@ -415,6 +415,19 @@ class Renderer:
     def update(self) -> None:
         self._ck(lib().vv_renderer_update(self._h), "update")
 
+    def service(self, requests: int, count: int, cap: int) -> None:
+        """Page-request service for a compacted list drawn elsewhere (device pointers)."""
+        self._ck(lib().vv_renderer_service(self._h, C.c_void_p(requests), C.c_void_p(count), cap), "service")
+
+    def set_deferred(self, on: bool = True) -> None:
+        self._ck(lib().vv_renderer_set_deferred(self._h, 1 if on else 0), "set deferred")
+
+    def stage_uploads(self) -> None:
+        self._ck(lib().vv_renderer_stage_uploads(self._h), "stage uploads")
+
+    def enqueue_uploads(self) -> None:
+        self._ck(lib().vv_renderer_enqueue_uploads(self._h), "enqueue uploads")
+
     def stats(self) -> dict:
         s = N.RendererStats()
         self._ck(lib().vv_renderer_get_stats(self._h, C.byref(s)), "stats")

@@ -224,6 +224,10 @@ SIGNATURES = {
     "vv_renderer_destroy": (None, [P]),
     "vv_renderer_draw": (C.c_int, [P, C.POINTER(Camera)]),
     "vv_renderer_update": (C.c_int, [P]),
+    "vv_renderer_service": (C.c_int, [P, P, P, C.c_int32]),
+    "vv_renderer_set_deferred": (C.c_int, [P, C.c_int32]),
+    "vv_renderer_stage_uploads": (C.c_int, [P]),
+    "vv_renderer_enqueue_uploads": (C.c_int, [P]),
     "vv_renderer_get_stats": (C.c_int, [P, C.POINTER(RendererStats)]),
     "vv_renderer_frame_buffers": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "vv_renderer_read_color": (C.c_int, [P, P]),

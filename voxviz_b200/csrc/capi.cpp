@@ -177,6 +177,26 @@ int vv_renderer_update(vv_renderer* r) {
     return r->impl->update();
 }
 
+int vv_renderer_service(vv_renderer* r, const uint32_t* requests, const uint32_t* count, int32_t cap) {
+    if (!r) return VV_ERR_ARG;
+    return r->impl->service(requests, count, cap);
+}
+
+int vv_renderer_set_deferred(vv_renderer* r, int32_t on) {
+    if (!r) return VV_ERR_ARG;
+    return r->impl->set_deferred(on != 0);
+}
+
+int vv_renderer_stage_uploads(vv_renderer* r) {
+    if (!r) return VV_ERR_ARG;
+    return r->impl->stage_uploads();
+}
+
+int vv_renderer_enqueue_uploads(vv_renderer* r) {
+    if (!r) return VV_ERR_ARG;
+    return r->impl->enqueue_uploads();
+}
+
 int vv_renderer_get_stats(const vv_renderer* r, vv_renderer_stats* out) {
     if (!r || !out) return VV_ERR_ARG;
     r->impl->stats(*out);

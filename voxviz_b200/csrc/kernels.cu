@@ -16,6 +16,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "raycast_common.cuh"
 
 namespace vv {
@@ -278,6 +280,32 @@ __global__ void node_patch_kernel(const vv_node_patch* __restrict__ patches, int
         return;
     }
     nodes[block_linear(q.x, q.y, q.z, dx, dy)] = make_uint2(q.word0, q.word1);
+}
+
+__global__ void node_patch_staged_kernel(const vv_node_patch* patches, const volatile uint32_t* count,
+                                         uint32_t max_patches, uint2* __restrict__ nodes, int dx, int dy, int dz,
+                                         int* status) {
+    __shared__ uint32_t s_n;  // one read of host memory per CTA
+    if (threadIdx.x == 0) s_n = min(*count, max_patches);
+    __syncthreads();
+    const uint32_t n = s_n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const vv_node_patch q = patches[i];
+        if (q.x >= (uint32_t)dx || q.y >= (uint32_t)dy || q.z >= (uint32_t)dz) {
+            set_status(status, VV_ERR_BOUNDS);
+            continue;
+        }
+        nodes[block_linear(q.x, q.y, q.z, dx, dy)] = make_uint2(q.word0, q.word1);
+    }
+}
+
+cudaError_t launch_node_patch_staged(const vv_node_patch* patches, const uint32_t* count, uint32_t max_patches,
+                                     uint2* nodes, const int dim[3], int* status, cudaStream_t s) {
+    if (max_patches == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)std::min<uint32_t>((max_patches + 255) / 256, 1184u);
+    node_patch_staged_kernel<<<grid, 256, 0, s>>>(patches, count, max_patches, nodes, dim[0], dim[1], dim[2],
+                                                  status);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_node_upload(const uint32_t* grid_words, uint2* nodes, const int dim[3], cudaStream_t s) {

@@ -2,6 +2,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "../../include/voxviz_b200.h"
@@ -80,9 +81,8 @@ __device__ __forceinline__ void store_texel(void* pool, size_t i, uint32_t v) {
 // One CTA per brick.  Texel (bx,by,bz) of node (d; i,j,k) is the mip-level
 // (L-d) voxel (8i-1+bx, 8j-1+by, 8k-1+bz), transparent black outside the level.
 template <int FMT>
-__global__ void produce_kernel(const __grid_constant__ DeviceTerrainView t, const uint4* __restrict__ jobs,
-                               void* __restrict__ pool, long long total_slots, int* status) {
-    const uint4 job = jobs[blockIdx.x];
+__device__ __forceinline__ void produce_one(const DeviceTerrainView& t, const uint4 job, void* __restrict__ pool,
+                                            long long total_slots, int* status) {
     if ((long long)job.x >= total_slots || (int)job.y > t.depth) {
         if (threadIdx.x == 0 && status) atomicCAS(status, 0, VV_ERR_BOUNDS);
         return;
@@ -106,6 +106,32 @@ __global__ void produce_kernel(const __grid_constant__ DeviceTerrainView t, cons
             }
         }
         store_texel<FMT>(pool, base + (size_t)q, v);
+    }
+}
+
+template <int FMT>
+__global__ void produce_kernel(const __grid_constant__ DeviceTerrainView t, const uint4* __restrict__ jobs,
+                               void* __restrict__ pool, long long total_slots, int* status) {
+    produce_one<FMT>(t, jobs[blockIdx.x], pool, total_slots, status);
+}
+
+// Staged form: jobs and their count live in pinned host memory mapped into
+// the device address space and are read here, so the launch itself does not
+// depend on the count (it can sit in a CUDA graph replayed every frame).
+template <int FMT>
+__global__ void produce_staged_kernel(const __grid_constant__ DeviceTerrainView t, const uint4* jobs,
+                                      const volatile uint32_t* count, uint32_t max_jobs, void* __restrict__ pool,
+                                      long long total_slots, int* status) {
+    __shared__ uint32_t s_n;  // one read of host memory per CTA
+    if (threadIdx.x == 0) s_n = min(*count, max_jobs);
+    __syncthreads();
+    const uint32_t n = s_n;
+    __shared__ uint4 s_job;  // and one per job
+    for (uint32_t j = blockIdx.x; j < n; j += gridDim.x) {
+        if (threadIdx.x == 0) s_job = jobs[j];
+        __syncthreads();
+        produce_one<FMT>(t, s_job, pool, total_slots, status);
+        __syncthreads();
     }
 }
 
@@ -202,6 +228,32 @@ cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs,
         case VV_FMT_FP16: produce_kernel<VV_FMT_FP16><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
         case VV_FMT_BF16: produce_kernel<VV_FMT_BF16><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
         case VV_FMT_FP32: produce_kernel<VV_FMT_FP32><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs, const uint32_t* count,
+                                  uint32_t max_jobs, void* pool, int fmt, long long total_slots, int* status,
+                                  cudaStream_t s) {
+    if (max_jobs == 0) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned grid = (unsigned)std::min<long long>((long long)max_jobs, (long long)std::max(sms, 1) * 8);
+    switch (fmt) {
+        case VV_FMT_RGBA8:
+            produce_staged_kernel<VV_FMT_RGBA8><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            break;
+        case VV_FMT_FP16:
+            produce_staged_kernel<VV_FMT_FP16><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            break;
+        case VV_FMT_BF16:
+            produce_staged_kernel<VV_FMT_BF16><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            break;
+        case VV_FMT_FP32:
+            produce_staged_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

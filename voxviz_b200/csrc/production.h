@@ -52,6 +52,12 @@ private:
 cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs, int n, void* pool, int fmt,
                                   long long total_slots, int* status, cudaStream_t s);
 
+// The same with jobs and their count read on the device from pinned, mapped
+// host memory (at most max_jobs): a count-independent launch for CUDA graphs.
+cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs, const uint32_t* count,
+                                  uint32_t max_jobs, void* pool, int fmt, long long total_slots, int* status,
+                                  cudaStream_t s);
+
 struct DedupeBuffers {
     uint32_t* first = nullptr;       // per node-pool grid cell, all 0xFFFFFFFF between calls
     size_t first_cells = 0;

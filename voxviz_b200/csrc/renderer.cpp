@@ -2,6 +2,7 @@
 #include "renderer.h"
 
 #include "ctx.h"
+#include "kernels.cuh"
 
 #include <cuda_runtime.h>
 
@@ -165,6 +166,9 @@ GigaVoxelsRenderer::~GigaVoxelsRenderer() {
     void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, dd_.count, d_jobs_};
     for (void* b : dbufs)
         if (b) cudaFree(b);
+    void* hbufs[] = {h_def_jobs_, h_def_patches_, h_def_counts_};
+    for (void* b : hbufs)
+        if (b) cudaFreeHost(b);
 }
 
 int GigaVoxelsRenderer::init() {
@@ -421,7 +425,7 @@ int GigaVoxelsRenderer::update_host(uint32_t n, std::vector<uint32_t>& upload) {
     return VV_OK;
 }
 
-int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload) {
+int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload, const uint32_t* requests) {
     requests_on_host_ = false;
     if (!n) return VV_OK;
     const size_t ids = (size_t)n * 4, blocks = (ids + 1023) / 1024;
@@ -438,7 +442,7 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload)
         if (cudaMalloc((void**)&dd_.unique, dd_.unique_cap * 4) != cudaSuccess) return VV_ERR_OOM;
     }
     const int* pd = tree_->pool_dim();
-    if (launch_dedupe(d_requests, (int)n, pd, dd_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if (launch_dedupe(requests, (int)n, pd, dd_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     // read-backs land in pinned memory (pageable copies are staged and slow)
     if (cudaMemcpyAsync(h_small_ + 1, dd_.count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
@@ -482,17 +486,24 @@ int GigaVoxelsRenderer::update() {
     const uint32_t n = std::min<uint32_t>(count, (uint32_t)cap_);
     req_count_ = n;
     std::vector<uint32_t> upload;
-    int rc = device_paging_ ? update_device(n, upload) : update_host(n, upload);
+    int rc = device_paging_ ? update_device(n, upload, d_requests) : update_host(n, upload);
     if (rc) return rc;
     const auto t1 = std::chrono::steady_clock::now();
     ms_readback_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    rc = apply_policy(upload);
+    if (rc) return rc;
+    ms_policy_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    return deferred_ ? VV_OK : flush_uploads();
+}
+
+int GigaVoxelsRenderer::apply_policy(std::vector<uint32_t>& upload) {
     // GigaVoxelsOctTree::update touches the root every frame (:1821-1850).
     if (node_slot_[0] >= 0) lru_.touch((uint32_t)node_slot_[0]);
     // BrickPool::update (GigaVoxelsBrickPool.cpp:561-682), including the
     // upload of a non-resident non-constant parent (:629-673).
     for (uint32_t nidx : upload) {
         if (node_slot_[nidx] >= 0) continue;
-        rc = upload_nodes(nidx);
+        int rc = upload_nodes(nidx);
         if (rc) return rc;
         const uint32_t par = tree_->parent(nidx);
         if (par != kNoParent && !tree_->is_constant(par) && node_slot_[par] < 0) {
@@ -500,8 +511,120 @@ int GigaVoxelsRenderer::update() {
             if (rc) return rc;
         }
     }
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::service(const uint32_t* requests, const uint32_t* count, int cap) {
+    if (!device_paging_) return VV_ERR_STATE;
+    if (!requests || !count || cap < 0) return VV_ERR_ARG;
+    uploaded_ = 0;
+    if (!h_small_ && cudaMallocHost((void**)&h_small_, 16) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMemcpyAsync(h_small_, count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    const auto t0 = std::chrono::steady_clock::now();
+    active_ = h_small_[0];
+    const uint32_t n = std::min<uint32_t>(h_small_[0], (uint32_t)cap);
+    req_count_ = n;
+    std::vector<uint32_t> upload;
+    int rc = update_device(n, upload, requests);
+    if (rc) return rc;
+    const auto t1 = std::chrono::steady_clock::now();
+    ms_readback_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    rc = apply_policy(upload);
+    if (rc) return rc;
     ms_policy_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
-    return flush_uploads();
+    return deferred_ ? VV_OK : flush_uploads();
+}
+
+int GigaVoxelsRenderer::set_deferred(bool on) {
+    if (on == deferred_) return VV_OK;
+    if (!on) {
+        deferred_ = false;
+        return flush_uploads();  // whatever was pending goes out now
+    }
+    if (!device_paging_) return VV_ERR_STATE;
+    if (!h_def_jobs_) {
+        // a slot holds at most one job per staging (later jobs replace
+        // earlier ones); a node is patched at most once
+        def_job_cap_ = total_slots_;
+        def_patch_cap_ = (uint32_t)std::min<size_t>(w0_.size(), 2 * (size_t)total_slots_ + 4096);
+        if (cudaHostAlloc((void**)&h_def_jobs_, (size_t)def_job_cap_ * sizeof(uint4), cudaHostAllocMapped) !=
+                cudaSuccess ||
+            cudaHostAlloc((void**)&h_def_patches_, (size_t)def_patch_cap_ * sizeof(vv_node_patch),
+                          cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostAlloc((void**)&h_def_counts_, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess)
+            return VV_ERR_OOM;
+        h_def_counts_[0] = h_def_counts_[1] = 0;
+        slot_job_.assign(total_slots_, -1);
+    }
+    deferred_ = true;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::stage_uploads() {
+    if (!deferred_) return VV_ERR_STATE;
+    // the latest job per slot: an earlier job for the same slot belongs to a
+    // node that was evicted again before this staging
+    std::vector<uint32_t> keep;
+    keep.reserve(pending_nodes_.size());
+    for (size_t i = pending_nodes_.size(); i-- > 0;) {
+        const uint32_t s = pending_slots_[i];
+        if (slot_job_[s] >= 0) continue;
+        slot_job_[s] = (int32_t)i;
+        keep.push_back((uint32_t)i);
+    }
+    for (uint32_t i : keep) slot_job_[pending_slots_[i]] = -1;
+    if (keep.size() > def_job_cap_ || touched_.size() > def_patch_cap_) {
+        // does not fit the staging: apply at once on the stream instead
+        h_def_counts_[0] = h_def_counts_[1] = 0;
+        return flush_uploads();
+    }
+    uint32_t nj = 0;
+    for (size_t k = keep.size(); k-- > 0;) {  // back to first-seen order
+        const uint32_t i = keep[k];
+        const uint32_t node = pending_nodes_[i];
+        int ci, cj, ck;
+        tree_->origin(node, ci, cj, ck);
+        h_def_jobs_[nj++] = make_uint4(pending_slots_[i], (uint32_t)tree_->level(node),
+                                       ((uint32_t)ci << 20) | ((uint32_t)cj << 10) | (uint32_t)ck, 0u);
+    }
+    uint32_t np = 0;
+    for (uint32_t t : touched_) {
+        vv_node_patch& q = h_def_patches_[np++];
+        tree_->grid_of(t, q.x, q.y, q.z);
+        q.word0 = w0_[t];
+        q.word1 = w1_[t];
+        touched_mark_[t] = 0;
+    }
+    touched_.clear();
+    pending_nodes_.clear();
+    pending_slots_.clear();
+    h_def_counts_[0] = nj;
+    h_def_counts_[1] = np;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::enqueue_uploads() {
+    if (!deferred_) return VV_ERR_STATE;
+    uint4* jobs = nullptr;
+    vv_node_patch* patches = nullptr;
+    uint32_t* counts = nullptr;
+    if (cudaHostGetDevicePointer((void**)&jobs, h_def_jobs_, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&patches, h_def_patches_, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&counts, h_def_counts_, 0) != cudaSuccess)
+        return VV_ERR_CUDA;
+    void* pool = nullptr;
+    size_t pool_bytes = 0;
+    vv_brickpool_device_ptr(ctx_, &pool, &pool_bytes);
+    if (launch_produce_staged(dterrain_->view(), jobs, counts, def_job_cap_, pool, d_.fmt, (long long)total_slots_,
+                              ctx_->d_status, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    const DeviceTree& t = ctx_->trees[0];
+    if (launch_node_patch_staged(patches, counts + 1, def_patch_cap_, t.nodes, t.dim, ctx_->d_status,
+                                 ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    return VV_OK;
 }
 
 int GigaVoxelsRenderer::last_requests(std::vector<uint32_t>& out) {

@@ -46,6 +46,15 @@ public:
     int init();                          // Renderer::init
     int draw(const vv_camera& cam);      // Renderer::draw
     int update();                        // Renderer::postDraw + Renderer::update
+    // The page-request service for a compacted list drawn elsewhere (device
+    // pointers); uploads are applied at once, or staged when deferred.
+    int service(const uint32_t* requests, const uint32_t* count, int cap);
+    // Deferred uploads: service() only stages; stage_uploads() writes this
+    // frame's jobs and node patches to pinned mapped memory and
+    // enqueue_uploads() launches the count-independent device side.
+    int set_deferred(bool on);
+    int stage_uploads();
+    int enqueue_uploads();
     void stats(vv_renderer_stats& s) const;
 
     vv_ctx* ctx() { return ctx_; }
@@ -68,7 +77,8 @@ private:
     int upload_nodes(uint32_t node);     // upload the brick of node, evicting the LRU slot
     int flush_uploads();
     int update_host(uint32_t n, std::vector<uint32_t>& upload);
-    int update_device(uint32_t n, std::vector<uint32_t>& upload);
+    int update_device(uint32_t n, std::vector<uint32_t>& upload, const uint32_t* requests);
+    int apply_policy(std::vector<uint32_t>& upload);
     void visit(uint32_t nidx, std::vector<uint32_t>& upload);
 
     vv_ctx* ctx_;
@@ -106,6 +116,13 @@ private:
     bool requests_on_host_ = false;
     void* h_stage_ = nullptr;            // pinned brick staging
     size_t h_stage_cap_ = 0;
+    // deferred uploads (pinned, mapped): jobs, node patches, their counts
+    bool deferred_ = false;
+    uint4* h_def_jobs_ = nullptr;
+    vv_node_patch* h_def_patches_ = nullptr;
+    uint32_t* h_def_counts_ = nullptr;   // [0] jobs, [1] patches
+    uint32_t def_job_cap_ = 0, def_patch_cap_ = 0;
+    std::vector<int32_t> slot_job_;      // staging: latest job index per slot
 };
 
 }  // namespace vv
