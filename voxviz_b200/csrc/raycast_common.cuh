@@ -13,6 +13,7 @@
 #include <cuda_fp16.h>
 
 #include "kernels.cuh"
+#include "lod_bound.h"
 
 namespace vv {
 namespace rc {
@@ -258,6 +259,7 @@ struct WalkConsts {
     float RS, astop, lod, pixel_size, rvh;
     int L, max_iter;
     uint2 root;
+    lodb::Consts lodk;  // certificate constants of the LOD test (lod_bound.h)
 };
 
 struct RayState {
@@ -288,6 +290,10 @@ __device__ __forceinline__ WalkConsts walk_consts(const RaycastParams& p, uint2 
     k.L = u.oct_tree_depth_minus_one;
     k.max_iter = p.max_iter;
     k.root = root;
+    k.lodk = lodb::make_consts(lodb::V3{k.C.x, k.C.y, k.C.z}, lodb::V3{k.up.x, k.up.y, k.up.z},
+                               lodb::V3{k.left.x, k.left.y, k.left.z}, k.rvh, k.lod, k.pixel_size, k.L,
+                               k.vmin.x == 0.0f && k.vmin.y == 0.0f && k.vmin.z == 0.0f && k.vmax.x == 1.0f &&
+                                   k.vmax.y == 1.0f && k.vmax.z == 1.0f);
     return k;
 }
 
@@ -354,6 +360,8 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
     bool ok = true;
     for (;;) {
         if (!vis.segment_begin(s)) return;
+        int skip_lo, skip_hi;
+        lodb::clear_range(k.lodk, lodb::V3{s.pos.x, s.pos.y, s.pos.z}, skip_lo, skip_hi);
         uint2 node = k.root;
         F3 ext_min = k.vmin, ext_max = k.vmax;
         float node_size = 1.0f, vhalf = k.rvh;
@@ -377,8 +385,9 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             const uint32_t cx = (node.x >> 20) & 0x3FFu, cy = (node.x >> 10) & 0x3FFu, cz = node.x & 0x3FFu;
             if ((!is_const && !loaded) || (cx == 0u && cy == 0u && cz == 0u)) break;
             // ComputeVoxelSize (:429-441) * LodScalar, only when the other two
-            // stop conditions do not decide (it has no side effects)
-            {
+            // stop conditions do not decide (it has no side effects), and not
+            // at the levels lodb::clear_range has shown to continue
+            if (depth < skip_lo || depth > skip_hi) {
                 const F3 uh = muls(k.up, vhalf), lh = muls(k.left, vhalf);
                 const F3 ll = normalize3(sub(add(sub(s.pos, uh), lh), k.C));
                 const F3 ur = normalize3(sub(sub(add(s.pos, uh), lh), k.C));
