@@ -260,6 +260,7 @@ struct WalkConsts {
     int L, max_iter;
     uint2 root;
     lodb::Consts lodk;  // certificate constants of the LOD test (lod_bound.h)
+    bool unit_box;      // volume extent [0,1]^3 (as compute_uniforms derives it)
 };
 
 struct RayState {
@@ -290,10 +291,11 @@ __device__ __forceinline__ WalkConsts walk_consts(const RaycastParams& p, uint2 
     k.L = u.oct_tree_depth_minus_one;
     k.max_iter = p.max_iter;
     k.root = root;
+    k.unit_box = k.vmin.x == 0.0f && k.vmin.y == 0.0f && k.vmin.z == 0.0f && k.vmax.x == 1.0f &&
+                 k.vmax.y == 1.0f && k.vmax.z == 1.0f;
     k.lodk = lodb::make_consts(lodb::V3{k.C.x, k.C.y, k.C.z}, lodb::V3{k.up.x, k.up.y, k.up.z},
                                lodb::V3{k.left.x, k.left.y, k.left.z}, k.rvh, k.lod, k.pixel_size, k.L,
-                               k.vmin.x == 0.0f && k.vmin.y == 0.0f && k.vmin.z == 0.0f && k.vmax.x == 1.0f &&
-                                   k.vmax.y == 1.0f && k.vmax.z == 1.0f);
+                               k.unit_box);
     return k;
 }
 
@@ -365,6 +367,10 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
         uint2 node = k.root;
         F3 ext_min = k.vmin, ext_max = k.vmax;
         float node_size = 1.0f, vhalf = k.rvh;
+        // In the unit box the node's extent is its integer cell times 2^-depth
+        // exactly (the sums below add distinct powers of two), so the cell is
+        // tracked instead and the extent formed once after the descent.
+        uint32_t ccx = 0u, ccy = 0u, ccz = 0u;
         F3 rbp = s.pos, cur_brp = s.pos;
         uint32_t cur_bw = k.root.y;
         int depth = 0, brick_depth = 0;
@@ -403,15 +409,26 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             s.nptr_y = cy + oy;
             s.nptr_z = cz + oz;
             ++depth;
-            node_size = node_size * 0.5f;
-            ext_min = add(ext_min, muls(f3((float)ox, (float)oy, (float)oz), node_size));
-            ext_max = sub(ext_max, muls(f3(1.0f - (float)ox, 1.0f - (float)oy, 1.0f - (float)oz), node_size));
+            if (k.unit_box) {
+                ccx = 2u * ccx + ox;
+                ccy = 2u * ccy + oy;
+                ccz = 2u * ccz + oz;
+            } else {
+                node_size = node_size * 0.5f;
+                ext_min = add(ext_min, muls(f3((float)ox, (float)oy, (float)oz), node_size));
+                ext_max = sub(ext_max, muls(f3(1.0f - (float)ox, 1.0f - (float)oy, 1.0f - (float)oz), node_size));
+            }
             vhalf = vhalf * 0.5f;
             node = fetch_node<COUNT>(p, s.nptr_x, s.nptr_y, s.nptr_z, ok);
             if (!ok) {
                 vis.fail(VV_ERR_BOUNDS);
                 return;
             }
+        }
+        if (k.unit_box) {
+            const float sc = ldexpf(1.0f, -depth);
+            ext_min = f3((float)ccx * sc, (float)ccy * sc, (float)ccz * sc);
+            ext_max = f3((float)(ccx + 1u) * sc, (float)(ccy + 1u) * sc, (float)(ccz + 1u) * sc);
         }
         // ---- the leaf segment
         if (is_const) {
