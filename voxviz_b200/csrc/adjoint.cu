@@ -105,7 +105,7 @@ __device__ __forceinline__ void pixel_of(int& px, int& py) {
 }  // namespace
 
 template <int FMT>
-__global__ void __launch_bounds__(128) forward_ckpt_kernel(const __grid_constant__ RaycastParams p, int2* hdr,
+__global__ void __launch_bounds__(128, 5) forward_ckpt_kernel(const __grid_constant__ RaycastParams p, int2* hdr,
                                                            Ckpt* ckpt, int per_ray) {
     int px, py;
     pixel_of(px, py);
@@ -124,13 +124,17 @@ __global__ void __launch_bounds__(128) forward_ckpt_kernel(const __grid_constant
     s.dst = make_float4(0.f, 0.f, 0.f, 0.f);
     s.nsamples = 0;
     F3 pos;
-    if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s)) walk<FMT, false>(p, k, s, vis);
+    __shared__ uint2 path_w[kPathLevels][128];
+    __shared__ uint32_t path_p[kPathLevels][128];
+    if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s))
+        walk<FMT, false, CkptVisitor, 1, true>(p, k, s, vis,
+                                               PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
     if (p.color) p.color[pix] = s.dst;
     hdr[pix] = make_int2(vis.count, s.nsamples);
 }
 
 template <int FMT>
-__global__ void __launch_bounds__(128) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
+__global__ void __launch_bounds__(128, 5) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
                                                        const Ckpt* ckpt, int per_ray, const float4* dl_dcolor,
                                                        float4* grad) {
     int px, py;
@@ -150,6 +154,8 @@ __global__ void __launch_bounds__(128) backward_kernel(const __grid_constant__ R
     if (!ray_origin(u, k, px, py, pos)) return;
     ray_start(p, k, px, py, pos, s0);  // direction and brick step of this ray
     const Ckpt* ck = ckpt + pix * (size_t)per_ray;
+    __shared__ uint2 path_w[kPathLevels][128];
+    __shared__ uint32_t path_p[kPathLevels][128];
     ReplayVisitor rv;
     for (int c = C - 1; c >= 0; --c) {
         const Ckpt cc = ck[c];
@@ -166,7 +172,8 @@ __global__ void __launch_bounds__(128) backward_kernel(const __grid_constant__ R
             rv.first = a + m * kPiece;
             rv.last = min(b, rv.first + kPiece);
             rv.n = 0;
-            walk<FMT, false>(p, k, s, rv);
+            walk<FMT, false, ReplayVisitor, 1, true>(p, k, s, rv,
+                                                     PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
             for (int j = rv.n - 1; j >= 0; --j) {
                 const float t = rv.T[j];
                 const float4 sv = rv.src[j];

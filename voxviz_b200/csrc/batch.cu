@@ -32,11 +32,15 @@ struct BatchView {
 namespace {
 
 template <int FMT, int TW, int TH, int STEPS>
-__global__ void __launch_bounds__(TW * TH) batch_raycast_kernel(const BatchView* __restrict__ views, int nviews,
+// at least 16 warps per SM: at most 128 registers per thread
+__global__ void __launch_bounds__(TW * TH, 512 / (TW * TH)) batch_raycast_kernel(const BatchView* __restrict__ views,
+                                                                                 int nviews,
                                                                  unsigned* __restrict__ counter, int total_tiles) {
     static_assert(TW % 8 == 0 && TH % 4 == 0, "a tile is made of 8x4 warp tiles");
     __shared__ RaycastParams sp;
     __shared__ int s_tile, s_view, s_tx, s_ty;
+    __shared__ uint2 path_w[kPathLevels][TW * TH];
+    __shared__ uint32_t path_p[kPathLevels][TW * TH];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // each warp covers an 8x4 block of the tile (coherent descents)
     const int wx = (warp % (TW / 8)) * 8 + (lane & 7);
@@ -70,7 +74,9 @@ __global__ void __launch_bounds__(TW * TH) batch_raycast_kernel(const BatchView*
         }
         __syncthreads();
         const int px = s_tx * TW + wx, py = s_ty * TH + wy;
-        if (px < sp.u.width && py < sp.u.height) render_pixel<FMT, false, STEPS>(sp, px, py);
+        if (px < sp.u.width && py < sp.u.height)
+            render_pixel<FMT, false, STEPS, true>(sp, px, py,
+                                                  PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], TW * TH});
         // every thread is done with s_* and sp before thread 0 takes the next tile
         __syncthreads();
     }

@@ -25,12 +25,15 @@ namespace vv {
 using namespace rc;
 
 template <int FMT, bool COUNT>
-__global__ void __launch_bounds__(128) raycast_kernel(const __grid_constant__ RaycastParams p) {
+// 5 resident CTAs (20 warps) per SM: at most 102 registers per thread
+__global__ void __launch_bounds__(128, 5) raycast_kernel(const __grid_constant__ RaycastParams p) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int px = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
     const int py = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
     if (px >= p.u.width || py >= p.u.height) return;
-    render_pixel<FMT, COUNT, 1>(p, px, py);
+    __shared__ uint2 path_w[kPathLevels][128];
+    __shared__ uint32_t path_p[kPathLevels][128];
+    render_pixel<FMT, COUNT, 1, !COUNT>(p, px, py, PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
 }
 
 cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s) {

@@ -357,9 +357,26 @@ __device__ __forceinline__ bool ray_start(const RaycastParams& p, const WalkCons
     return inside_box(s.pos, k.vmin, k.vmax);
 }
 
-template <int FMT, bool COUNT, class V, int STEPS = 1>
-__device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis) {
+// The path of the ray's last descent, per thread in shared memory: node word
+// and packed grid position (x<<20 | y<<10 | z) of each level, `stride`
+// elements apart per level.  A later descent whose position lies in the same
+// level-r node, and whose LOD test lodb::clear_range shows to continue at
+// every level above r, starts at that node instead of the root: the levels
+// it skips would take exactly the recorded path (same nodes, same words,
+// every stop condition false), so the walk is unchanged.
+constexpr int kPathLevels = 11;  // levels 0..10
+struct PathSlots {
+    uint2* w;
+    uint32_t* p;
+    int stride;
+};
+
+template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false>
+__device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis,
+                                     PathSlots path = PathSlots{nullptr, nullptr, 0}) {
     bool ok = true;
+    int prev_depth = -1;       // where the last descent stopped (RESUME)
+    uint32_t prev_cell = 0u;   // its node's cell there, packed 10:10:10
     for (;;) {
         if (!vis.segment_begin(s)) return;
         int skip_lo, skip_hi;
@@ -375,11 +392,55 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
         uint32_t cur_bw = k.root.y;
         int depth = 0, brick_depth = 0;
         bool is_const, loaded;
+        if (RESUME && !COUNT && k.unit_box && prev_depth > 0 && prev_depth < kPathLevels && skip_lo == 0) {
+            // the deepest level whose node holds both this and the last position
+            const float sc = ldexpf(1.0f, prev_depth);
+            const uint32_t nx = (uint32_t)(s.pos.x * sc), ny = (uint32_t)(s.pos.y * sc),
+                           nz = (uint32_t)(s.pos.z * sc);
+            const uint32_t diff = (nx ^ (prev_cell >> 20)) | (ny ^ ((prev_cell >> 10) & 0x3FFu)) |
+                                  (nz ^ (prev_cell & 0x3FFu));
+            int r = prev_depth - (diff ? 32 - __clz(diff) : 0);
+            r = min(r, skip_hi + 1);
+            if (r >= 1 && s.iter + r <= k.max_iter) {
+                node = path.w[r * path.stride];
+                const uint32_t pp = path.p[r * path.stride];
+                s.nptr_x = pp >> 20;
+                s.nptr_y = (pp >> 10) & 0x3FFu;
+                s.nptr_z = pp & 0x3FFu;
+                depth = r;
+                vhalf = ldexpf(k.rvh, -r);
+                // cell and position in the cell at level r: exact (power-of-two scaling)
+                const float sr = ldexpf(1.0f, r);
+                const F3 pr = f3(s.pos.x * sr, s.pos.y * sr, s.pos.z * sr);
+                ccx = (uint32_t)pr.x;
+                ccy = (uint32_t)pr.y;
+                ccz = (uint32_t)pr.z;
+                rbp = f3(pr.x - (float)ccx, pr.y - (float)ccy, pr.z - (float)ccz);
+                // the deepest resident node above r holds the brick state
+#pragma unroll 1
+                for (int l = r - 1; l >= 0; --l) {
+                    const uint2 wl = path.w[l * path.stride];
+                    if (wl.x & kResident) {
+                        cur_bw = wl.y;
+                        brick_depth = l;
+                        const float sl = ldexpf(1.0f, l);
+                        const F3 pl = f3(s.pos.x * sl, s.pos.y * sl, s.pos.z * sl);
+                        cur_brp = f3(pl.x - floorf(pl.x), pl.y - floorf(pl.y), pl.z - floorf(pl.z));
+                        break;
+                    }
+                }
+                s.iter += r;
+            }
+        }
         // ---- descent to the node that stops it
         for (;;) {
             if (++s.iter > k.max_iter) {
                 vis.fail(VV_ERR_TIMEOUT);
                 return;
+            }
+            if (RESUME && depth < kPathLevels) {
+                path.w[depth * path.stride] = node;
+                path.p[depth * path.stride] = (s.nptr_x << 20) | (s.nptr_y << 10) | s.nptr_z;
             }
             is_const = (node.x & kConstant) != 0u;
             loaded = (node.x & kResident) != 0u;
@@ -429,6 +490,10 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             const float sc = ldexpf(1.0f, -depth);
             ext_min = f3((float)ccx * sc, (float)ccy * sc, (float)ccz * sc);
             ext_max = f3((float)(ccx + 1u) * sc, (float)(ccy + 1u) * sc, (float)(ccz + 1u) * sc);
+            if (RESUME) {
+                prev_depth = depth;
+                prev_cell = (ccx << 20) | (ccy << 10) | ccz;
+            }
         }
         // ---- the leaf segment
         if (is_const) {
@@ -532,8 +597,9 @@ struct UsageVisitor {
 
 // One pixel of the forward draw: the fragment's ray walk, FragColor and the
 // three RGBA32UI usage-list layers (:490-751).
-template <int FMT, bool COUNT, int STEPS>
-__device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int py) {
+template <int FMT, bool COUNT, int STEPS, bool RESUME = false>
+__device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int py,
+                                             PathSlots path = PathSlots{nullptr, nullptr, 0}) {
     const vv_uniforms& u = p.u;
     const size_t pix = (size_t)py * u.width + px;
     bool ok = true;
@@ -551,7 +617,7 @@ __device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int
     s.dst = make_float4(0.f, 0.f, 0.f, 0.f);
     F3 pos;
     if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s))
-        walk<FMT, COUNT, UsageVisitor, STEPS>(p, k, s, vis);
+        walk<FMT, COUNT, UsageVisitor, STEPS, RESUME>(p, k, s, vis, path);
     if (p.color) p.color[pix] = s.dst;
     if (p.usage) {
         uint4* o = p.usage + pix * 3;
