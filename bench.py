@@ -286,7 +286,8 @@ def run_ours(args):
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ray_ms, cmp_ms, uploads, requests = [], [], 0, 0
-    host_ms = {"ms_readback": 0.0, "ms_policy": 0.0, "ms_produce": 0.0, "ms_upload": 0.0}
+    host_ms = {"ms_readback": 0.0, "ms_visit": 0.0, "ms_policy": 0.0, "ms_produce": 0.0, "ms_upload": 0.0}
+    unique_nodes = 0
     timed_u = []
     ev0.record()
     for _ in range(args.steps):
@@ -298,6 +299,7 @@ def run_ours(args):
         st = r.stats()
         uploads += st["bricks_uploaded"]
         requests += st["requests"]
+        unique_nodes += st["unique_nodes"]
         for k in host_ms:
             host_ms[k] += st[k]
         timed_u.append(r.last_uniforms())
@@ -376,6 +378,7 @@ def run_ours(args):
                     "select_compact_ms_mean": round(float(np.mean(cmp_ms)), 3)},
         "paging": {"bricks_uploaded_per_frame": round(uploads / args.steps, 1),
                    "requests_per_frame": round(requests / args.steps, 1), "converge_draws": converge,
+                   "distinct_nodes_per_frame": round(unique_nodes / args.steps, 1),
                    "host_ms_per_frame": {k[3:]: round(v / args.steps, 3) for k, v in host_ms.items()},
                    "resident": r.stats()["resident_bricks"], "pool_slots": r.stats()["pool_slots"]},
         "fwd_bwd": fb,

@@ -433,6 +433,9 @@ typedef struct vv_renderer_stats {
     float ms_policy;           /* decode, dedupe, LRU                        */
     float ms_produce;          /* brick production on the host cores         */
     float ms_upload;           /* brick upload + node patches                */
+    float ms_visit;            /* host pass over the distinct requested nodes
+                                  (part of ms_readback with device paging)  */
+    int32_t unique_nodes;      /* distinct requested nodes, last service     */
 } vv_renderer_stats;
 
 /* vox::Renderer lifecycle of the "gv" renderer (VoxVizCore/Renderer.h:20-110,

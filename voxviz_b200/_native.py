@@ -151,6 +151,8 @@ class RendererStats(C.Structure):
         ("ms_policy", C.c_float),
         ("ms_produce", C.c_float),
         ("ms_upload", C.c_float),
+        ("ms_visit", C.c_float),
+        ("unique_nodes", C.c_int32),
     ]
 
 

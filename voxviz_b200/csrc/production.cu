@@ -218,7 +218,42 @@ __global__ void __launch_bounds__(1024) dedupe_scatter_kernel(const uint32_t* __
     }
 }
 
+// Per distinct requested node (grid cell g, first-seen order), its state in
+// the device node pool: the brick-pool slot if resident, 0x80000000 | g if
+// neither resident nor constant (an upload candidate), 0xFFFFFFFF otherwise.
+__global__ void classify_kernel(const uint32_t* __restrict__ unique, const uint32_t* __restrict__ count,
+                                uint32_t max_n, const uint2* __restrict__ nodes, int dx, int dy, int dz, int sx,
+                                int sy, uint32_t* __restrict__ codes) {
+    const uint32_t n = min(*count, max_n);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t g = unique[k];
+        const uint32_t x = g % (uint32_t)dx, y = (g / (uint32_t)dx) % (uint32_t)dy, z = g / ((uint32_t)dx * dy);
+        const uint32_t blk = ((z >> 1) * ((uint32_t)dy >> 1) + (y >> 1)) * ((uint32_t)dx >> 1) + (x >> 1);
+        const uint2 w = nodes[(size_t)blk * 8u + ((x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2))];
+        uint32_t c;
+        if (w.x & 0x80000000u) {
+            // brick pointer = slot origin + border (1,1,1), 10 texels per slot
+            const uint32_t px = ((w.y >> 20) & 0x3FFu) - 1u, py = ((w.y >> 10) & 0x3FFu) - 1u, pz = (w.y & 0x3FFu) - 1u;
+            c = ((pz / 10u) * (uint32_t)sy + py / 10u) * (uint32_t)sx + px / 10u;
+        } else if (w.x & 0x40000000u) {
+            c = 0xFFFFFFFFu;
+        } else {
+            c = 0x80000000u | g;
+        }
+        codes[k] = c;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_classify(const uint32_t* unique, const uint32_t* count, uint32_t max_n, const uint2* nodes,
+                            const int dim[3], const int slots[3], uint32_t* codes, cudaStream_t s) {
+    if (max_n == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)std::min<uint32_t>((max_n + 255u) / 256u, 4736u);
+    classify_kernel<<<grid, 256, 0, s>>>(unique, count, max_n, nodes, dim[0], dim[1], dim[2], slots[0], slots[1],
+                                         codes);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs, int n, void* pool, int fmt,
                                   long long total_slots, int* status, cudaStream_t s) {

@@ -68,6 +68,13 @@ struct DedupeBuffers {
     uint32_t* count = nullptr;       // number of distinct nodes
 };
 
+// State of each distinct node in the device node pool (block-linear, grid
+// dims `dim`): its brick slot when resident, 0x80000000 | cell when neither
+// resident nor constant, 0xFFFFFFFF when constant.  `count` is read on the
+// device; at most max_n entries.
+cudaError_t launch_classify(const uint32_t* unique, const uint32_t* count, uint32_t max_n, const uint2* nodes,
+                            const int dim[3], const int slots[3], uint32_t* codes, cudaStream_t s);
+
 // De-duplicate the node ids of `n_entries` compacted entries (4 ids each).
 cudaError_t launch_dedupe(const uint32_t* requests, int n_entries, const int grid_dim[3], const DedupeBuffers& b,
                           cudaStream_t s);

@@ -443,6 +443,16 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
     }
     const int* pd = tree_->pool_dim();
     if (launch_dedupe(requests, (int)n, pd, dd_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    // When the device node words hold this renderer's state (no node-word
+    // change is pending on the host), the distinct nodes are classified on
+    // the device (in place) and the host only replays the LRU touches.
+    const bool classified = !deferred_ && touched_.empty();
+    if (classified) {
+        const DeviceTree& t = ctx_->trees[0];
+        if (launch_classify(dd_.unique, dd_.count, (uint32_t)ids, t.nodes, t.dim, slots_, dd_.unique,
+                            ctx_->stream) != cudaSuccess)
+            return VV_ERR_CUDA;
+    }
     // read-backs land in pinned memory (pageable copies are staged and slow)
     if (cudaMemcpyAsync(h_small_ + 1, dd_.count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
@@ -463,13 +473,24 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
             return VV_ERR_CUDA;
         if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     }
+    const auto tv = std::chrono::steady_clock::now();
     const uint32_t dx = (uint32_t)pd[0], dy = (uint32_t)pd[1];
     for (uint32_t k = 0; k < u; ++k) {
-        const uint32_t g = h_unique_[k];
+        uint32_t g = h_unique_[k];
+        if (classified) {
+            if (g == 0xFFFFFFFFu) continue;           // constant, not resident
+            if (!(g & 0x80000000u)) {                 // resident: its slot
+                lru_.touch(g);
+                continue;
+            }
+            g &= 0x7FFFFFFFu;                         // upload candidate: checked below
+        }
         const uint32_t nidx = tree_->index_of(g % dx, (g / dx) % dy, g / (dx * dy));
         if (nidx == kNoParent || tree_->level(nidx) < 0) continue;
         visit(nidx, upload);
     }
+    ms_visit_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tv).count();
+    unique_ = (int32_t)u;
     return VV_OK;
 }
 
@@ -655,6 +676,8 @@ void GigaVoxelsRenderer::stats(vv_renderer_stats& s) const {
     s.ms_policy = ms_policy_;
     s.ms_produce = ms_produce_;
     s.ms_upload = ms_upload_;
+    s.ms_visit = ms_visit_;
+    s.unique_nodes = unique_;
 }
 
 void GigaVoxelsRenderer::residency(std::vector<uint32_t>& xyz, std::vector<uint32_t>& slot) const {

@@ -102,7 +102,8 @@ private:
     int64_t frame_ = -1;
     int32_t frame_for_compress_ = 0;
     int64_t req_count_ = 0, active_ = 0, uploaded_ = 0, uploaded_total_ = 0, evictions_ = 0, resident_ = 0;
-    float ms_readback_ = 0.f, ms_policy_ = 0.f, ms_produce_ = 0.f, ms_upload_ = 0.f;
+    float ms_readback_ = 0.f, ms_policy_ = 0.f, ms_produce_ = 0.f, ms_upload_ = 0.f, ms_visit_ = 0.f;
+    int32_t unique_ = 0;
     // device-side service
     bool device_paging_ = false;
     std::unique_ptr<DeviceTerrain> dterrain_;
