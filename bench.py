@@ -56,7 +56,9 @@ def parse():
 
 
 def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    from voxviz_b200 import dist as vdist
+
+    return vdist.env()
 
 
 def workload_config(extra=None):
@@ -123,7 +125,7 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-RAYCAST_VERSION = "v3"  # bumped whenever the ray-cast kernel changes; the ncu capture must match
+RAYCAST_VERSION = "v4"  # bumped whenever the ray-cast kernel changes; the ncu capture must match
 
 
 def ncu_traffic():
@@ -239,18 +241,16 @@ def run_ours(args):
     import voxviz_b200 as vv
     from voxviz_b200 import scene
 
-    rank, local_rank, world = dist_env()
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
+    from voxviz_b200 import dist as vdist
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
+    vdist.init(timeout_s=600)
     t_setup = time.perf_counter()
     octree = vv.Octree.terrain(seed=TERRAIN_SEED, depth=DEPTH)
     heights = octree.heights()
     cams = scene.camera_path(PATH_SEED, heights, PATH_FRAMES, WIDTH, HEIGHT)
-    offset = rank * PATH_FRAMES // world
+    offset, _ = vdist.path_segment(rank, world, PATH_FRAMES)
 
     def start_renderer():
         """A renderer in the state the timed frames start from: paging
@@ -278,9 +278,7 @@ def run_ours(args):
     ctx_e, r_e, _, frame_e = start_renderer()
     setup_s = time.perf_counter() - t_setup
     ctx.set_profiling(True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    vdist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -306,21 +304,16 @@ def run_ours(args):
         frame += 1
     ev1.record()
     torch.cuda.synchronize()
+    vdist.barrier()
     clk = clocks.stop()
-    elapsed = ev0.elapsed_time(ev1)
-    t = torch.tensor([elapsed], device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = vdist.max_over_ranks(ev0.elapsed_time(ev1), "cuda")
     rays = world * args.steps * WIDTH * HEIGHT
     value = rays / (max_ms / 1e3) / 1e6
     # end to end: same frames through the plugin API with the colour image
     # read back into pinned host memory each step
     host = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.float32, pin_memory=True)
     host_np = host.numpy()
-    if world > 1:
-        dist.barrier()
+    vdist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2e_uploads = 0
@@ -333,10 +326,8 @@ def run_ours(args):
         frame_e += 1
     e1.record()
     torch.cuda.synchronize()
-    te = torch.tensor([e0.elapsed_time(e1)], device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = rays / (float(te.item()) / 1e3) / 1e6
+    vdist.barrier()
+    e2e_value = rays / (vdist.max_over_ranks(e0.elapsed_time(e1), "cuda") / 1e3) / 1e6
     # check frame: the next frame of the path drawn on the current pools (no
     # update after it), so the downloaded pools are exactly what it read
     r.draw(cams[frame % PATH_FRAMES])
@@ -398,8 +389,7 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
     r.close()
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    vdist.shutdown()
 
 
 FIT_DEPTH, FIT_VIEWS, FIT_SIZE, FIT_SIGMA, FIT_LR = 8, 16, 512, 0.05, 5e-3
