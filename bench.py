@@ -895,6 +895,42 @@ def run_precision(args):
                                                           "rms": float(np.sqrt((e_fix ** 2).mean()))},
                      "status": status, "brick_bytes": 1000 * vv.TEXEL_BYTES[f]}
         ctx.close()
+    # the lighting path (GigaVoxels.frag with ComputeLighting): RGBA8 bricks,
+    # FP32 gradient bricks, against the FP64 oracle's lit shader
+    words, pool, slots, xyz = scene.resident_scene(octree, vv.VV_FMT_RGBA8)
+    grads = np.zeros((pool.shape[0], 16000), dtype=np.uint8)
+    grads[:xyz.shape[0]] = octree.produce_gradients(xyz, "fp32")
+    ctx = vv.Context(0)
+    ctx.upload_nodes(words)
+    ctx.create_brickpool(slots, "rgba8")
+    ctx.upload_bricks(np.arange(xyz.shape[0], dtype=np.uint32), pool[:xyz.shape[0]])
+    ctx.create_gradpool("fp32")
+    ctx.upload_gradients(np.arange(xyz.shape[0], dtype=np.uint32), grads[:xyz.shape[0]])
+    ctx.set_jitter(jit)
+    ctx.set_profiling(True)
+    color = torch.empty((512, 512, 4), dtype=torch.float32, device="cuda")
+    us = [vv.compute_uniforms(octree.info, c, slots, 1.0, ALPHA_STOP) for c in cams]
+    for u in us:
+        u.compute_lighting = 1
+    ms, imgs = [], []
+    for u in us[:3]:
+        ctx.render(u, color=color.data_ptr(), passes=vv.VV_PASS_RAYCAST)
+    for u in us:
+        ctx.render(u, color=color.data_ptr(), passes=vv.VV_PASS_RAYCAST)
+        ctx.synchronize()
+        ms.append(ctx.last_times()[0])
+        imgs.append(color.cpu().numpy().copy())
+    sc = go.Scene(words, pool, slots, vv.VV_FMT_RGBA8, jit, grads=grads, grad_fmt=vv.VV_FMT_FP32)
+    e64 = np.concatenate([np.abs(i.astype(np.float64) - go.raycast(u, sc, 64, threads=threads, want_usage=False)[0])
+                          .ravel() for i, u in zip(imgs, us)])
+    e32 = max(float(np.abs(i - go.raycast(u, sc, 32, threads=threads, want_usage=False)[0]).max())
+              for i, u in zip(imgs[:8], us[:8]))
+    rows["rgba8_lit"] = {"mrays_s": round(512 * 512 / (float(np.mean(ms)) / 1e3) / 1e6, 1),
+                         "raycast_ms": round(float(np.mean(ms)), 4), "gradients": "fp32",
+                         "err_vs_fp32_oracle_max": e32,
+                         "err_vs_fp64": {"max": float(e64.max()), "rms": float(np.sqrt((e64 ** 2).mean()))},
+                         "status": ctx.device_status(clear=True)}
+    ctx.close()
     out = {"workload": "precision", "metric": "Mrays/s, HBM GB/s and error vs FP64 per brick format",
            "config": {"workload": "fBm terrain 256^3 (depth 5), 64 seeded 512x512 views, FP32 compositing",
                       "peak_gbs": peak, "peak_source": peak_kind, "data": "synthetic"},

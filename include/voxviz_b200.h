@@ -105,6 +105,14 @@ typedef struct vv_uniforms {
     float near_origin[3];
     float near_dx[3];
     float near_dy[3];
+    /* Lighting: GigaVoxels.frag with ComputeLighting (:16, :27-28, shading
+     * :293-312, LookupGradient :314-325, TraverseBrick :337, :370-384).
+     * Off (0) in every benchmark configuration, which then follows
+     * GigaVoxelsNoLighting.frag.  On needs a gradient pool
+     * (vv_gradpool_create) and is supported by vv_render. */
+    float light_position[3];       /* LightPosition, normalized volume space */
+    int32_t compute_lighting;      /* ComputeLighting                        */
+    int32_t gradients_unsigned;    /* GradientsAreUnsigned: texel*2 - 1      */
 } vv_uniforms;
 
 /* One node-word update (OctTreeNodePool::update3DTexture,
@@ -190,6 +198,14 @@ int vv_upload_bricks(vv_ctx* ctx, const uint32_t* slots, int32_t n,
 /* Same with device-resident brick data (`texels_dev`, `slots_dev` device ptrs). */
 int vv_upload_bricks_device(vv_ctx* ctx, const uint32_t* slots_dev, int32_t n,
                             const void* texels_dev);
+/* The gradient texture of the brick pool (BrickPool::getGradientTextureID,
+ * GigaVoxelsBrickPool.cpp:820): the same slots, one gradient per texel, as
+ * VV_FMT_FP32 (x, y, z, unused: the reference's Vec3f gradients) or
+ * VV_FMT_RGBA8 (components stored as unsigned bytes; sampled /255 and, with
+ * gradients_unsigned, mapped back by *2-1).  Create after the brick pool. */
+int vv_gradpool_create(vv_ctx* ctx, int32_t fmt);
+int vv_upload_gradients(vv_ctx* ctx, const uint32_t* slots, int32_t n, const void* texels);
+int vv_gradpool_download(vv_ctx* ctx, void* texels);
 /* Read the whole pool back (slot-major, brick-linear) into host memory. */
 int vv_brickpool_download(vv_ctx* ctx, void* texels);
 /* Slots per axis and format of the brick pool (0 slots if none exists). */
@@ -370,6 +386,16 @@ int vv_octree_node_info(const vv_octree* tree, uint32_t x, uint32_t y,
  * pyramid of GenerateMipMaps (:1030-1194). */
 int vv_octree_produce_bricks(const vv_octree* tree, const uint32_t* xyz,
                              int32_t n, int32_t fmt, void* out);
+/* The gradient bricks of the same nodes (the pGradientData half of
+ * copyMipMapToBrick): leaf gradients are normalised central differences of
+ * alpha with 0 outside the volume (VolumeDataSet::convert,
+ * VolumeDataSet.cpp:144-209), coarser levels the box-filtered, renormalised
+ * average of the level below (GenerateMipMap / GetBoxFilterAverage,
+ * GigaVoxelsOctTree.cpp:809-960).  fmt VV_FMT_FP32 (float x, y, z, 0) or
+ * VV_FMT_RGBA8 (round((g + 1) / 2 * 255) per component, for
+ * gradients_unsigned).  Kept densely: trees of depth <= 6. */
+int vv_octree_produce_gradients(const vv_octree* tree, const uint32_t* xyz,
+                                int32_t n, int32_t fmt, void* out);
 /* Dense mip level (RGBA8, x fastest) for checking on small volumes. */
 int vv_octree_mip_level(const vv_octree* tree, int32_t level, uint32_t* out,
                         size_t out_words);

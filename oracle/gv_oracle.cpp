@@ -195,10 +195,13 @@ struct Shader {
     T RootVoxelHalfSize, PixelSize, LodScalar, AlphaStop;
     int OctTreeDepthMinusOne, MaxNodesToPushThisFrame, JitterTexSize;
     bool RootNodeIsConstant;
+    bool ComputeLighting = false, GradientsAreUnsigned = false;
+    vec3<T> LightPosition;
     // samplers
     const uint32_t* nodes;  // texture order, 2 words per texel
     int ndim[3];
     BrickTexture<T> brick;
+    BrickTexture<T> grads;  // BrickGradientsSampler (lighting); data NULL when absent
     const uint8_t* jitter;
     int max_iter;
     int* status;
@@ -223,6 +226,9 @@ struct Shader {
         MaxNodesToPushThisFrame = u->max_nodes_to_push;
         JitterTexSize = u->jitter_tex_size;
         RootNodeIsConstant = u->root_node_is_constant != 0;
+        ComputeLighting = u->compute_lighting != 0;
+        GradientsAreUnsigned = u->gradients_unsigned != 0;
+        LightPosition = from<T>(u->light_position);
     }
 
     bool texelFetchNode(int x, int y, int z, uint32_t& r, uint32_t& g) const {
@@ -234,7 +240,8 @@ struct Shader {
     }
 
     // texture(BrickSampler, p): GL_LINEAR, CLAMP_TO_EDGE.
-    vec4<T> texture(const vec3<T>& p) const {
+    vec4<T> texture(const vec3<T>& p) const { return texture_of(brick, p); }
+    vec4<T> texture_of(const BrickTexture<T>& brick, const vec3<T>& p) const {
         const T uv[3] = {p.x, p.y, p.z};
         const T N[3] = {BrickPoolDimension.x, BrickPoolDimension.y, BrickPoolDimension.z};
         const int n[3] = {brick.sx * 10, brick.sy * 10, brick.sz * 10};
@@ -354,6 +361,8 @@ struct Shader {
     void TraverseBrick(vec3<T>& pos, const vec3<T>& dir, const vec3<T>& worldRayStep, vec3<T> curBrickRayPos,
                        const vec3<T>& brickRayStep, T sampleRatio, const vec3<T>& mn, const vec3<T>& mx,
                        vec4<T>& dst) const {
+        // GigaVoxels.frag :337: lightDir at entry (lighting only)
+        const vec3<T> lightDir = ComputeLighting ? normalize(LightPosition - pos) : vec3<T>{0, 0, 0};
         T timeToExit = ComputeMinRayBoxIntersection(pos, dir, mn, mx);
         T rayStepSize = RayStepSize * sampleRatio;
         int numSteps = (int)(timeToExit / rayStepSize) + 1;
@@ -366,11 +375,49 @@ struct Shader {
             }
             vec4<T> src = texture(curBrickRayPos);
             src.a = (T)1 - pow_pow2((T)1 - src.a, 0);
+            if (ComputeLighting) Light(curBrickRayPos, dir, lightDir, src);
             record(true, src, dst, curBrickRayPos);
             composite(dst, src);
             curBrickRayPos += brickRayStep;
         }
     }
+    // GigaVoxels.frag shading (:293-312): k_Ambient 0.05, k_Diffuse =
+    // k_Specular = 1, k_Shininess 100 with pow(x, 100) restated as
+    // x^64 * x^32 * x^4 by squarings.
+    static T pow100(T x) {
+        const T x2 = x * x, x4 = x2 * x2, x8 = x4 * x4, x16 = x8 * x8, x32 = x16 * x16, x64 = x32 * x32;
+        return (x64 * x32) * x4;
+    }
+    vec3<T> shading(const vec3<T>& rgb, const vec3<T>& normal, const vec3<T>& toCamera,
+                    const vec3<T>& toLight) const {
+        const vec3<T> halfway = normalize(toLight + toCamera);
+        const T diffuseLight = std::fmax(dot(toLight, normal), (T)0);
+        vec3<T> diffuse{0, 0, 0}, specular{0, 0, 0};
+        if (diffuseLight > (T)0) {
+            diffuse = rgb * diffuseLight;
+            specular = rgb * pow100(std::fmax(dot(halfway, normal), (T)0));
+        }
+        const T ka = sizeof(T) == 4 ? (T)0.05f : (T)0.05;
+        const vec3<T> ambient = rgb * ka;
+        return (ambient + diffuse) + specular;
+    }
+    // LookupGradient (:314-325) and the lighting of TraverseBrick (:370-384).
+    void Light(const vec3<T>& curBrickRayPos, const vec3<T>& rayDir, const vec3<T>& lightDir, vec4<T>& src) const {
+        const vec4<T> g = texture_of(grads, curBrickRayPos);
+        vec3<T> normal{g.r, g.g, g.b};
+        if (GradientsAreUnsigned) {
+            normal = normal * (T)2;
+            normal = normal - vec3<T>{(T)1, (T)1, (T)1};
+        }
+        normal = normalize(normal);
+        if (std::isnan(normal.x) || std::isnan(normal.y) || std::isnan(normal.z)) return;
+        const vec3<T> rgb{src.r, src.g, src.b};
+        const vec3<T> sh = shading(rgb, normal, rayDir * (T)-1, lightDir);
+        src.r = src.r + sh.x;
+        src.g = src.g + sh.y;
+        src.b = src.b + sh.z;
+    }
+
     // :429-441
     T ComputeVoxelSize(const vec3<T>& p, T h) const {
         vec3<T> camToLL = normalize(((p - (CameraUp * h)) + (CameraLeft * h)) - CameraPosition);
@@ -589,6 +636,12 @@ int run_raycast(const vv_uniforms* u, const oracle_scene* s, int row0, int row1,
     sh.brick.sy = s->slots[1];
     sh.brick.sz = s->slots[2];
     sh.jitter = s->jitter;
+    sh.grads.data = s->grads;
+    sh.grads.fmt = s->grad_fmt;
+    sh.grads.sx = s->slots[0];
+    sh.grads.sy = s->slots[1];
+    sh.grads.sz = s->slots[2];
+    if (sh.ComputeLighting && !s->grads) return VV_ERR_STATE;  // lighting needs the gradient pool
     sh.max_iter = max_iterations(u);
     int st = 0;
     sh.status = &st;
@@ -723,6 +776,7 @@ int oracle_fixed_path(const vv_uniforms* u, const oracle_scene* traj, const orac
     base.brick.sy = traj->slots[1];
     base.brick.sz = traj->slots[2];
     base.jitter = traj->jitter;
+    if (base.ComputeLighting) return VV_ERR_ARG;  // unlit sample sequences only
     base.max_iter = max_iterations(u);
     int st = 0;
     base.status = &st;
@@ -786,6 +840,7 @@ int oracle_backward(const vv_uniforms* u, const oracle_scene* s, const float* dl
     sh.brick.sy = s->slots[1];
     sh.brick.sz = s->slots[2];
     sh.jitter = s->jitter;
+    if (sh.ComputeLighting) return VV_ERR_ARG;  // the adjoint covers the unlit ray cast
     sh.max_iter = max_iterations(u);
     int st = 0;
     sh.status = &st;

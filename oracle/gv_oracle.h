@@ -15,6 +15,8 @@ typedef struct oracle_scene {
     int32_t fmt;            /* vv_fmt */
     int32_t slots[3];
     const uint8_t* jitter;  /* jitter_tex_size^2 values */
+    const void* grads;      /* gradient pool, same slots (lighting), or NULL */
+    int32_t grad_fmt;       /* VV_FMT_FP32 or VV_FMT_RGBA8 */
 } oracle_scene;
 
 /* Rows [row0,row1) of the ray cast.  precision 32: float colour (4 floats per

@@ -24,6 +24,8 @@ class OracleScene(C.Structure):
         ("fmt", C.c_int32),
         ("slots", C.c_int32 * 3),
         ("jitter", C.c_void_p),
+        ("grads", C.c_void_p),
+        ("grad_fmt", C.c_int32),
     ]
 
 
@@ -74,10 +76,12 @@ def _p(a: np.ndarray) -> int:
 class Scene:
     """Node words (dz,dy,dx,2), brick pool (slots, bytes), format and jitter."""
 
-    def __init__(self, words: np.ndarray, pool: np.ndarray, slots, fmt: int, jitter: np.ndarray):
+    def __init__(self, words: np.ndarray, pool: np.ndarray, slots, fmt: int, jitter: np.ndarray,
+                 grads: np.ndarray | None = None, grad_fmt: int = 3):
         self.words = np.ascontiguousarray(words, dtype=np.uint32)
         self.pool = np.ascontiguousarray(pool)
         self.jitter = np.ascontiguousarray(jitter, dtype=np.uint8)
+        self.grads = None if grads is None else np.ascontiguousarray(grads)
         self.s = OracleScene()
         self.s.nodes = _p(self.words)
         dz, dy, dx = self.words.shape[:3]
@@ -86,6 +90,8 @@ class Scene:
         self.s.fmt = int(fmt)
         self.s.slots[:] = [int(v) for v in slots]
         self.s.jitter = _p(self.jitter)
+        self.s.grads = _p(self.grads) if self.grads is not None else None
+        self.s.grad_fmt = int(grad_fmt)
 
 
 def raycast(u, scene: Scene, precision: int = 32, rows=None, threads: int = 0, want_usage: bool = True):

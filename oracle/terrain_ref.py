@@ -242,3 +242,81 @@ def build_tree(mips, collapse=True, brick_dim=8):
         words[gz, gy, gx] = (w0, w1)
         real[(gx, gy, gz)] = (level, i, j, k)
     return {"node_count": num, "pool_dim": (dx, dy, dz), "words": words, "nodes": real}
+
+
+# ---- gradients (the lighting path) -----------------------------------------
+
+def leaf_gradients(alpha):
+    """VolumeDataSet::convert (VoxViz/VoxVizCore/VolumeDataSet.cpp:144-209):
+    per voxel (a(x-1) - a(x+1), a(y-1) - a(y+1), a(z-1) - a(z+1)) with a the
+    binary32 alpha/255 and 0 outside, normalised in double when its length
+    is positive (QVector3D::length, operator/=), stored as binary32.
+    alpha: (z, y, x) float32.  Returns (z, y, x, 3) float32."""
+    a = alpha.astype(F32)
+    z = np.zeros_like(a)
+
+    def shifted(axis, d):
+        out = z.copy()
+        src = [slice(None)] * 3
+        dst = [slice(None)] * 3
+        if d < 0:  # a(x-1) at x
+            src[axis] = slice(0, -1)
+            dst[axis] = slice(1, None)
+        else:      # a(x+1) at x
+            src[axis] = slice(1, None)
+            dst[axis] = slice(0, -1)
+        out[tuple(dst)] = a[tuple(src)]
+        return out
+
+    g = np.stack([(shifted(2, -1) - shifted(2, +1)).astype(F32),
+                  (shifted(1, -1) - shifted(1, +1)).astype(F32),
+                  (shifted(0, -1) - shifted(0, +1)).astype(F32)], axis=-1).astype(np.float64)
+    length = np.sqrt(g[..., 0] * g[..., 0] + g[..., 1] * g[..., 1] + g[..., 2] * g[..., 2])
+    safe = np.where(length > 0, length, 1.0)
+    g = np.where((length > 0)[..., None], g / safe[..., None], 0.0)
+    return g.astype(F32)
+
+
+def qt_normalize(v):
+    """QVector3D::normalize (Qt 4.8) on binary32 vectors, in double: left as is
+    when |len^2 - 1| <= 1e-12 or len^2 <= 1e-12."""
+    d = v.astype(np.float64)
+    len2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+    keep = (np.abs(len2 - 1.0) <= 1e-12) | (np.abs(len2) <= 1e-12)
+    length = np.sqrt(np.where(keep, 1.0, len2))
+    out = np.where(keep[..., None], d, d / length[..., None])
+    return out.astype(F32)
+
+
+def gradient_pyramid(leaf):
+    """GenerateMipMap / GetBoxFilterAverage for gradients
+    (GigaVoxelsOctTree.cpp:809-960): each coarser voxel sums its 2x2x2 block
+    in binary32 (z, y, x order, starting from 0), scales by 1/8 and applies
+    QVector3D::normalize."""
+    levels = [leaf]
+    cur = leaf
+    while cur.shape[0] > 1:
+        a = np.zeros((cur.shape[0] // 2, cur.shape[1] // 2, cur.shape[2] // 2, 3), dtype=F32)
+        for dz in (0, 1):
+            for dy in (0, 1):
+                for dx in (0, 1):
+                    a = (a + cur[dz::2, dy::2, dx::2]).astype(F32)
+        a = (a * F32(0.125)).astype(F32)
+        cur = qt_normalize(a)
+        levels.append(cur)
+    return levels
+
+
+def gradient_brick(level_grads, origin, brick_dim=8):
+    """copyMipMapToBrick for gradients: texel b = mip voxel origin - 1 + b,
+    zero outside (the brick is cleared first).  Returns (10, 10, 10, 3)."""
+    n = level_grads.shape[0]
+    out = np.zeros((brick_dim + 2,) * 3 + (3,), dtype=F32)
+    ox, oy, oz = (int(v) - 1 for v in origin)
+    for bz in range(brick_dim + 2):
+        for by in range(brick_dim + 2):
+            for bx in range(brick_dim + 2):
+                x, y, zz = ox + bx, oy + by, oz + bz
+                if 0 <= x < n and 0 <= y < n and 0 <= zz < n:
+                    out[bz, by, bx] = level_grads[zz, y, x]
+    return out

@@ -160,6 +160,15 @@ class Octree:
         _check(lib().vv_octree_produce_bricks(self._h, _ptr(xyz), n, f, _ptr(out)), what="produce bricks")
         return out
 
+    def produce_gradients(self, xyz: np.ndarray, fmt="fp32") -> np.ndarray:
+        """Gradient bricks of the nodes at grid positions xyz (trees of depth <= 6)."""
+        f = fmt_code(fmt)
+        xyz = np.ascontiguousarray(xyz, dtype=np.uint32).reshape(-1, 3)
+        n = xyz.shape[0]
+        out = np.zeros((n, 1000 * TEXEL_BYTES[f]), dtype=np.uint8)
+        _check(lib().vv_octree_produce_gradients(self._h, _ptr(xyz), n, f, _ptr(out)), what="produce gradients")
+        return out
+
     def mip_level(self, level: int) -> np.ndarray:
         d = (8 << self.info.depth) >> level
         out = np.zeros((d, d, d), dtype=np.uint32)
@@ -268,6 +277,15 @@ class Context:
         out = np.zeros((n, 1000 * TEXEL_BYTES[self.fmt]), dtype=np.uint8)
         self._ck(lib().vv_brickpool_download(self._h, _ptr(out)), "brick download")
         return out
+
+    def create_gradpool(self, fmt="fp32") -> None:
+        """Gradient pool with the brick pool's slots (lighting)."""
+        self._ck(lib().vv_gradpool_create(self._h, fmt_code(fmt)), "gradient pool")
+
+    def upload_gradients(self, slot_ids: np.ndarray, texels: np.ndarray) -> None:
+        s = np.ascontiguousarray(slot_ids, dtype=np.uint32)
+        t = np.ascontiguousarray(texels)
+        self._ck(lib().vv_upload_gradients(self._h, _ptr(s), s.size, _ptr(t)), "gradient upload")
 
     def set_jitter(self, table: np.ndarray) -> None:
         t = np.ascontiguousarray(table, dtype=np.uint8)

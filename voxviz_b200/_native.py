@@ -47,6 +47,9 @@ class Uniforms(C.Structure):
         ("near_origin", f3),
         ("near_dx", f3),
         ("near_dy", f3),
+        ("light_position", f3),
+        ("compute_lighting", C.c_int32),
+        ("gradients_unsigned", C.c_int32),
     ]
 
 
@@ -191,6 +194,10 @@ SIGNATURES = {
     "vv_brickpool_create": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "vv_upload_bricks": (C.c_int, [P, P, C.c_int32, P]),
     "vv_upload_bricks_device": (C.c_int, [P, P, C.c_int32, P]),
+    "vv_gradpool_create": (C.c_int, [P, C.c_int32]),
+    "vv_upload_gradients": (C.c_int, [P, P, C.c_int32, P]),
+    "vv_gradpool_download": (C.c_int, [P, P]),
+    "vv_octree_produce_gradients": (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
     "vv_brickpool_download": (C.c_int, [P, P]),
     "vv_brickpool_info": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "vv_nodepool_info": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int32)]),

@@ -169,6 +169,7 @@ static int batch_launch(vv_ctx* c, const vv_batch_view* views, int32_t n, const 
         if (u->jitter_tex_size != bv.ctx->jitter_size)
             return batch_fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
         if (!(u->ray_step_size > 0.0f)) return batch_fail(c, VV_ERR_ARG, "ray_step_size must be > 0");
+        if (u->compute_lighting) return batch_fail(c, VV_ERR_ARG, "the batched launch covers the unlit ray cast");
         for (int a = 0; a < 3; ++a)
             if (u->brick_pool_dimension[a] != (float)(bv.ctx->slots[a] * 10))
                 return batch_fail(c, VV_ERR_ARG, "brick_pool_dimension does not match the brick pool");

@@ -114,6 +114,28 @@ int vv_octree_produce_bricks(const vv_octree* t, const uint32_t* xyz, int32_t n,
     return VV_OK;
 }
 
+int vv_octree_produce_gradients(const vv_octree* t, const uint32_t* xyz, int32_t n, int32_t fmt, void* out) {
+    if (!t || n < 0 || (n > 0 && (!xyz || !out))) return VV_ERR_ARG;
+    if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return VV_ERR_ARG;
+    if (t->tree->depth() > 6) return VV_ERR_ARG;
+    const size_t tb = vv::texel_bytes(fmt);
+    for (int32_t i = 0; i < n; ++i) {
+        const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        if (idx == vv::kNoParent || t->tree->level(idx) < 0) return VV_ERR_ARG;
+    }
+    if (n > 0) {  // build the pyramid once, outside the parallel loop
+        const uint32_t idx = t->tree->index_of(xyz[0], xyz[1], xyz[2]);
+        if (!t->tree->produce_gradient_brick(idx, fmt, out)) return VV_ERR_ARG;
+    }
+    unsigned char* o = (unsigned char*)out;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int32_t i = 1; i < n; ++i) {
+        const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        t->tree->produce_gradient_brick(idx, fmt, o + (size_t)i * VV_BRICK_TEXELS * tb);
+    }
+    return VV_OK;
+}
+
 int vv_octree_mip_level(const vv_octree* t, int32_t level, uint32_t* out, size_t out_words) {
     if (!t || !out || level < 0 || level > t->tree->depth()) return VV_ERR_ARG;
     const vv::TerrainVolume& v = t->tree->volume();

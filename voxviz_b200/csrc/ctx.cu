@@ -145,7 +145,7 @@ int vv_ctx_destroy(vv_ctx* c) {
         if (t.nodes) cudaFree(t.nodes);
     if (c->bricks && !c->bricks_external) cudaFree(c->bricks);
     void* bufs[] = {c->d_status, c->d_jitter, c->d_usage, c->d_mask, c->d_counts, c->d_offsets,
-                    c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words, c->d_batch};
+                    c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words, c->d_batch, c->grads};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -257,6 +257,10 @@ int vv_brickpool_create(vv_ctx* c, int32_t sx, int32_t sy, int32_t sz, int32_t f
         if (!c->bricks_external) cudaFree(c->bricks);
         c->bricks = nullptr;
     }
+    if (c->grads) {  // its slots were those of the old pool
+        cudaFree(c->grads);
+        c->grads = nullptr;
+    }
     c->bricks_external = false;
     const long long total = (long long)sx * sy * sz;
     const size_t bytes = (size_t)total * VV_BRICK_TEXELS * tb;
@@ -300,6 +304,57 @@ int vv_upload_bricks(vv_ctx* c, const uint32_t* slots, int32_t n, const void* te
     VV_CUDA(c, launch_brick_scatter(c->d_up_slots, n, c->d_up_bricks, c->bricks, c->brick_bytes, c->total_slots,
                                     c->d_status, c->stream));
     // The caller's host buffers may be pageable and reused right after return.
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_gradpool_create(vv_ctx* c, int32_t fmt) {
+    if (!c) return VV_ERR_ARG;
+    if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return fail(c, VV_ERR_ARG, "gradient pool format: FP32 or RGBA8");
+    if (!c->bricks) return fail(c, VV_ERR_STATE, "create the brick pool first");
+    cudaSetDevice(c->device);
+    if (c->grads) {
+        VV_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->grads);
+        c->grads = nullptr;
+    }
+    const size_t tb = fmt_texel_bytes(fmt);
+    const size_t bytes = (size_t)c->total_slots * VV_BRICK_TEXELS * tb;
+    cudaError_t e = cudaMalloc(&c->grads, bytes);
+    if (e != cudaSuccess) {
+        c->grads = nullptr;
+        return fail(c, VV_ERR_OOM, "cudaMalloc gradient pool");
+    }
+    VV_CUDA(c, cudaMemsetAsync(c->grads, 0, bytes, c->stream));
+    c->grad_fmt = fmt;
+    c->grad_brick_bytes = VV_BRICK_TEXELS * tb;
+    c->grad_pool_bytes = bytes;
+    return VV_OK;
+}
+
+int vv_upload_gradients(vv_ctx* c, const uint32_t* slots, int32_t n, const void* texels) {
+    if (!c || n < 0 || (n > 0 && (!slots || !texels))) return fail(c, VV_ERR_ARG, "bad upload arguments");
+    if (!c->grads) return fail(c, VV_ERR_STATE, "gradient pool not created");
+    if (n == 0) return VV_OK;
+    cudaSetDevice(c->device);
+    const size_t bb = (size_t)n * c->grad_brick_bytes, sb = (size_t)n * sizeof(uint32_t);
+    int rc = ensure(c, &c->d_up_bricks, &c->up_bricks_cap, bb, "gradient staging");
+    if (rc) return rc;
+    rc = ensure(c, (void**)&c->d_up_slots, &c->up_slots_cap, sb, "slot staging");
+    if (rc) return rc;
+    VV_CUDA(c, cudaMemcpyAsync(c->d_up_bricks, texels, bb, cudaMemcpyHostToDevice, c->stream));
+    VV_CUDA(c, cudaMemcpyAsync(c->d_up_slots, slots, sb, cudaMemcpyHostToDevice, c->stream));
+    VV_CUDA(c, launch_brick_scatter(c->d_up_slots, n, c->d_up_bricks, c->grads, c->grad_brick_bytes, c->total_slots,
+                                    c->d_status, c->stream));
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VV_OK;
+}
+
+int vv_gradpool_download(vv_ctx* c, void* texels) {
+    if (!c || !texels) return VV_ERR_ARG;
+    if (!c->grads) return fail(c, VV_ERR_STATE, "gradient pool not created");
+    cudaSetDevice(c->device);
+    VV_CUDA(c, cudaMemcpyAsync(texels, c->grads, c->grad_pool_bytes, cudaMemcpyDeviceToHost, c->stream));
     VV_CUDA(c, cudaStreamSynchronize(c->stream));
     return VV_OK;
 }
@@ -354,6 +409,7 @@ static int diff_params(vv_ctx* c, int32_t tree, const vv_uniforms* u, RaycastPar
     for (int a = 0; a < 3; ++a)
         if (u->brick_pool_dimension[a] != (float)(c->slots[a] * 10))
             return fail(c, VV_ERR_ARG, "brick_pool_dimension does not match the brick pool");
+    if (u->compute_lighting) return fail(c, VV_ERR_ARG, "the adjoint covers the unlit ray cast only");
     std::memset(&p, 0, sizeof(p));
     p.u = *u;
     p.nodes = t.nodes;
@@ -466,6 +522,11 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         p.usage = usage;
         p.status = c->d_status;
         p.max_iter = vv_max_iterations(u);
+        if (u->compute_lighting) {
+            if (!c->grads) return fail(c, VV_ERR_STATE, "lighting needs a gradient pool (vv_gradpool_create)");
+            p.grads = c->grads;
+            p.grad_fmt = c->grad_fmt;
+        }
         VV_CUDA(c, launch_raycast_any(c, p));
     }
     if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
@@ -568,6 +629,7 @@ int vv_measure_footprint(vv_ctx* c, int32_t tree, const vv_uniforms* u, int64_t*
     p.jitter = c->d_jitter;
     p.status = c->d_status;
     p.max_iter = vv_max_iterations(u);
+    p.u.compute_lighting = 0;  // lighting reads the same slots of the gradient pool
     p.node_touch = bits;
     p.brick_touch = bits + nwords;
     cudaError_t e = launch_raycast_any(c, p);

@@ -39,6 +39,11 @@ struct vv_ctx {
     int fmt = VV_FMT_RGBA8;
     size_t brick_bytes = 0;
     size_t pool_bytes = 0;
+    // gradient pool (lighting): same slots as the brick pool
+    void* grads = nullptr;
+    int grad_fmt = VV_FMT_FP32;
+    size_t grad_brick_bytes = 0;
+    size_t grad_pool_bytes = 0;
     // jitter
     uint8_t* d_jitter = nullptr;
     int jitter_size = 0;

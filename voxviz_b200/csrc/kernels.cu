@@ -24,8 +24,9 @@ namespace vv {
 
 using namespace rc;
 
-template <int FMT, bool COUNT>
+// LIT: GigaVoxels.frag with ComputeLighting (gradient pool in p.grads).
 // 5 resident CTAs (20 warps) per SM: at most 102 registers per thread
+template <int FMT, bool COUNT, bool LIT>
 __global__ void __launch_bounds__(128, 5) raycast_kernel(const __grid_constant__ RaycastParams p) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int px = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
@@ -33,16 +34,19 @@ __global__ void __launch_bounds__(128, 5) raycast_kernel(const __grid_constant__
     if (px >= p.u.width || py >= p.u.height) return;
     __shared__ uint2 path_w[kPathLevels][128];
     __shared__ uint32_t path_p[kPathLevels][128];
-    render_pixel<FMT, COUNT, 1, !COUNT>(p, px, py, PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
+    render_pixel<FMT, COUNT, 1, !COUNT, LIT>(p, px, py,
+                                             PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
 }
 
 cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s) {
     dim3 block(128);
     dim3 grid((unsigned)((p.u.width + 15) / 16), (unsigned)((p.u.height + 7) / 8));
     const bool count = p.node_touch && p.brick_touch;
+    const bool lit = p.u.compute_lighting && p.grads && !count;
 #define VV_LAUNCH(F)                                                           \
-    if (count) raycast_kernel<F, true><<<grid, block, 0, s>>>(p);              \
-    else raycast_kernel<F, false><<<grid, block, 0, s>>>(p);
+    if (count) raycast_kernel<F, true, false><<<grid, block, 0, s>>>(p);       \
+    else if (lit) raycast_kernel<F, false, true><<<grid, block, 0, s>>>(p);    \
+    else raycast_kernel<F, false, false><<<grid, block, 0, s>>>(p);
     switch (fmt) {
         case VV_FMT_RGBA8: VV_LAUNCH(VV_FMT_RGBA8) break;
         case VV_FMT_FP16: VV_LAUNCH(VV_FMT_FP16) break;

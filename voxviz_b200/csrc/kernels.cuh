@@ -19,6 +19,8 @@ struct RaycastParams {
     float4* color;           // [H*W] or nullptr
     uint4* usage;            // [H*W*3] (12 uint32 per pixel)
     int* status;             // sticky device status word
+    const void* grads;       // gradient pool (lighting), same slots as bricks, or nullptr
+    int grad_fmt;            // VV_FMT_FP32 or VV_FMT_RGBA8
     int max_iter;            // bound on outer-loop iterations per ray
     uint32_t* node_touch;    // footprint mode: bit per node (block-linear index)
     uint32_t* brick_touch;   // footprint mode: bit per brick-pool slot

@@ -318,4 +318,42 @@ void GigaVoxelsOctTree::produce_brick(uint32_t n, int fmt, void* out) const {
     for (int t = 0; t < VV_BRICK_TEXELS; ++t) convert_texel(tmp[t], fmt, o + (size_t)t * tb);
 }
 
+bool GigaVoxelsOctTree::produce_gradient_brick(uint32_t n, int fmt, void* out) const {
+    if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return false;
+    {
+        std::lock_guard<std::mutex> lock(grads_mu_);
+        if (!grads_) {
+            if (depth_ > 6) return false;
+            grads_ = std::make_unique<GradientPyramid>(*vol_);
+        }
+    }
+    const int d = level_[n], m = depth_ - d;
+    const int i = ci_[n], j = cj_[n], k = ck_[n];
+    // copyMipMapToBrick: texel (bx,by,bz) is mip voxel (8i-1+bx, 8j-1+by,
+    // 8k-1+bz), zero outside the level (the brick is cleared first)
+    for (int bz = 0; bz < 10; ++bz)
+        for (int by = 0; by < 10; ++by)
+            for (int bx = 0; bx < 10; ++bx) {
+                float g[3];
+                grads_->at(m, 8 * i - 1 + bx, 8 * j - 1 + by, 8 * k - 1 + bz, g);
+                const size_t t = (size_t)(bz * 100 + by * 10 + bx);
+                if (fmt == VV_FMT_FP32) {
+                    float* o = (float*)out + 4 * t;
+                    o[0] = g[0];
+                    o[1] = g[1];
+                    o[2] = g[2];
+                    o[3] = 0.0f;
+                } else {
+                    uint32_t w = 0;
+                    for (int c = 0; c < 3; ++c) {
+                        const float u = std::floor(((g[c] + 1.0f) * 0.5f) * 255.0f + 0.5f);
+                        const uint32_t b = u < 0.0f ? 0u : (u > 255.0f ? 255u : (uint32_t)u);
+                        w |= b << (8 * c);
+                    }
+                    ((uint32_t*)out)[t] = w;
+                }
+            }
+    return true;
+}
+
 }  // namespace vv

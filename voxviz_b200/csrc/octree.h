@@ -11,8 +11,10 @@
 
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <vector>
 
+#include "gradients.h"
 #include "terrain.h"
 
 namespace vv {
@@ -63,8 +65,14 @@ public:
     void produce_brick_rgba8(uint32_t n, uint32_t* out) const;
     // Same, converted to fmt (vv_fmt) texels.
     void produce_brick(uint32_t n, int fmt, void* out) const;
+    // The gradient brick of node n (gradients.h), fmt VV_FMT_FP32 (x, y, z,
+    // 0) or VV_FMT_RGBA8 (unsigned mapping).  Builds the dense gradient
+    // pyramid on first use; false when the tree is too deep for it.
+    bool produce_gradient_brick(uint32_t n, int fmt, void* out) const;
 
 private:
+    mutable std::unique_ptr<GradientPyramid> grads_;
+    mutable std::mutex grads_mu_;
     std::shared_ptr<const TerrainVolume> vol_;
     int depth_ = 0;
     int pool_dim_[3] = {0, 0, 0};

@@ -371,7 +371,71 @@ struct PathSlots {
     int stride;
 };
 
-template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false>
+// ---- lighting (GigaVoxels.frag with ComputeLighting) ----------------------
+
+// texture(BrickGradientsSampler, p).rgb (:316): the trilinear filter of
+// sample_brick over the gradient pool (FP32 gradients, or RGBA8 / 255).
+template <int GFMT>
+__device__ __forceinline__ F3 sample_gradient(const RaycastParams& p, F3 uvw) {
+    const float* N = p.u.brick_pool_dimension;
+    const Axis ax = axis_taps(uvw.x, N[0], p.slots[0] * 10);
+    const Axis ay = axis_taps(uvw.y, N[1], p.slots[1] * 10);
+    const Axis az = axis_taps(uvw.z, N[2], p.slots[2] * 10);
+    const uint32_t SX = (uint32_t)p.slots[0], SY = (uint32_t)p.slots[1];
+    auto idx = [&](int sx, int lx, int sy, int ly, int sz, int lz) -> uint32_t {
+        const uint32_t slot = ((uint32_t)sz * SY + (uint32_t)sy) * SX + (uint32_t)sx;
+        return slot * 1000u + (uint32_t)((lz * 10 + ly) * 10 + lx);
+    };
+    const void* g = p.grads;
+    const float4 v000 = Texel<GFMT>::load(g, idx(ax.s0, ax.l0, ay.s0, ay.l0, az.s0, az.l0));
+    const float4 v100 = Texel<GFMT>::load(g, idx(ax.s1, ax.l1, ay.s0, ay.l0, az.s0, az.l0));
+    const float4 v010 = Texel<GFMT>::load(g, idx(ax.s0, ax.l0, ay.s1, ay.l1, az.s0, az.l0));
+    const float4 v110 = Texel<GFMT>::load(g, idx(ax.s1, ax.l1, ay.s1, ay.l1, az.s0, az.l0));
+    const float4 v001 = Texel<GFMT>::load(g, idx(ax.s0, ax.l0, ay.s0, ay.l0, az.s1, az.l1));
+    const float4 v101 = Texel<GFMT>::load(g, idx(ax.s1, ax.l1, ay.s0, ay.l0, az.s1, az.l1));
+    const float4 v011 = Texel<GFMT>::load(g, idx(ax.s0, ax.l0, ay.s1, ay.l1, az.s1, az.l1));
+    const float4 v111 = Texel<GFMT>::load(g, idx(ax.s1, ax.l1, ay.s1, ay.l1, az.s1, az.l1));
+    const float4 c0 = lerp4(lerp4(v000, v100, ax.f), lerp4(v010, v110, ax.f), ay.f);
+    const float4 c1 = lerp4(lerp4(v001, v101, ax.f), lerp4(v011, v111, ax.f), ay.f);
+    float4 c = lerp4(c0, c1, az.f);
+    if (Texel<GFMT>::kScale != 1.0f) {
+        const float kk = Texel<GFMT>::kScale;
+        c = make_float4(c.x * kk, c.y * kk, c.z * kk, c.w * kk);
+    }
+    return f3(c.x, c.y, c.z);
+}
+
+// pow(x, 100) as x^64 * x^32 * x^4 by squarings (the shininess power).
+__device__ __forceinline__ float pow100(float x) {
+    const float x2 = x * x, x4 = x2 * x2, x8 = x4 * x4, x16 = x8 * x8, x32 = x16 * x16, x64 = x32 * x32;
+    return (x64 * x32) * x4;
+}
+
+// shading (:293-312) with k_Ambient 0.05, k_Diffuse = k_Specular = 1,
+// k_Shininess 100, added to src.rgb when the gradient normalizes (:370-384).
+__device__ __forceinline__ void light_sample(const RaycastParams& p, F3 bpos, F3 dir, F3 light_dir, float4& src) {
+    F3 n = p.grad_fmt == VV_FMT_RGBA8 ? sample_gradient<VV_FMT_RGBA8>(p, bpos)
+                                      : sample_gradient<VV_FMT_FP32>(p, bpos);
+    if (p.u.gradients_unsigned) n = sub(muls(n, 2.0f), f3(1.0f, 1.0f, 1.0f));  // LookupGradient :318-322
+    n = normalize3(n);
+    if (isnan(n.x) || isnan(n.y) || isnan(n.z)) return;  // homogeneous region: no lighting
+    const F3 rgb = f3(src.x, src.y, src.z);
+    const F3 to_camera = muls(dir, -1.0f);
+    const F3 halfway = normalize3(add(light_dir, to_camera));
+    const float diffuse_light = fmaxf(dot3(light_dir, n), 0.0f);
+    F3 diffuse = f3(0.0f, 0.0f, 0.0f), specular = f3(0.0f, 0.0f, 0.0f);
+    if (diffuse_light > 0.0f) {
+        diffuse = muls(rgb, diffuse_light);
+        specular = muls(rgb, pow100(fmaxf(dot3(halfway, n), 0.0f)));
+    }
+    const F3 ambient = muls(rgb, 0.05f);
+    const F3 sh = add(add(ambient, diffuse), specular);
+    src.x = src.x + sh.x;
+    src.y = src.y + sh.y;
+    src.z = src.z + sh.z;
+}
+
+template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false, bool LIT = false>
 __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis,
                                      PathSlots path = PathSlots{nullptr, nullptr, 0}) {
     bool ok = true;
@@ -527,6 +591,8 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                 }
             }
         } else {
+            // lightDir = normalize(LightPosition - rayWorldPosition) at entry (:337)
+            const F3 light_dir = LIT ? normalize3(sub(ld3(p.u.light_position), s.pos)) : f3(0.0f, 0.0f, 0.0f);
             const F3 bptr = f3((float)((cur_bw >> 20) & 0x3FFu) / k.pdim.x, (float)((cur_bw >> 10) & 0x3FFu) / k.pdim.y,
                                (float)(cur_bw & 0x3FFu) / k.pdim.z);
             F3 bpos = add(bptr, divv(mul(cur_brp, k.bdim), k.pdim));
@@ -558,6 +624,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                 float4 src;
                 if (COUNT || !sample_in_slot<FMT>(p, bpos, base, slot_texel0, src)) src = sample_brick<FMT, COUNT>(p, bpos);
                 src.w = 1.0f - (1.0f - src.w);
+                if (LIT) light_sample(p, bpos, s.dir, light_dir, src);
                 const float T = 1.0f - s.dst.w;
                 const bool go = vis.sample(kSampleBrick, src, bpos, T, s.nsamples);
                 s.dst = make_float4(T * src.x + s.dst.x, T * src.y + s.dst.y, T * src.z + s.dst.z, T * src.w + s.dst.w);
@@ -597,7 +664,7 @@ struct UsageVisitor {
 
 // One pixel of the forward draw: the fragment's ray walk, FragColor and the
 // three RGBA32UI usage-list layers (:490-751).
-template <int FMT, bool COUNT, int STEPS, bool RESUME = false>
+template <int FMT, bool COUNT, int STEPS, bool RESUME = false, bool LIT = false>
 __device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int py,
                                              PathSlots path = PathSlots{nullptr, nullptr, 0}) {
     const vv_uniforms& u = p.u;
@@ -617,7 +684,7 @@ __device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int
     s.dst = make_float4(0.f, 0.f, 0.f, 0.f);
     F3 pos;
     if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s))
-        walk<FMT, COUNT, UsageVisitor, STEPS, RESUME>(p, k, s, vis, path);
+        walk<FMT, COUNT, UsageVisitor, STEPS, RESUME, LIT>(p, k, s, vis, path);
     if (p.color) p.color[pix] = s.dst;
     if (p.usage) {
         uint4* o = p.usage + pix * 3;

@@ -100,6 +100,11 @@ void compute_uniforms(int depth, bool root_is_constant, const vv_camera& cam, co
         u.brick_pool_dimension[a] = pool_dim;
     }
     u.root_voxel_half_size = (1.0f / 8.0f) * 0.5f;  // (:1780-1787)
+    // LightPosition: world (0, 100, 0) / volScale + 0.5 (:1695-1699); lighting off
+    const float light[3] = {0.0f, 100.0f, 0.0f};
+    for (int a = 0; a < 3; ++a) u.light_position[a] = (light[a] / scale) + 0.5f;
+    u.compute_lighting = 0;
+    u.gradients_unsigned = 0;
     u.pixel_size = camera_pixel_size(cam);
     u.lod_scalar = lod_scalar;
     u.alpha_stop = alpha_stop;
