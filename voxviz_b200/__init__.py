@@ -464,6 +464,15 @@ class Renderer:
         self._ck(lib().vv_renderer_read_color(self._h, _ptr(out)), "read color")
         return out
 
+    def read_color_async(self, out: np.ndarray) -> None:
+        """Queue the last frame's colour read-back into `out` (pinned, (H,W,4)
+        float32); it completes at wait_readback()."""
+        assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"]
+        self._ck(lib().vv_renderer_read_color_async(self._h, _ptr(out)), "read color async")
+
+    def wait_readback(self) -> None:
+        self._ck(lib().vv_renderer_wait_readback(self._h), "wait readback")
+
     def read_lists(self):
         """(usage (H,W,12), mask (H,W)) of the last frame, uint32."""
         u = self.last_uniforms()

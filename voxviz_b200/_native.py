@@ -240,6 +240,8 @@ SIGNATURES = {
     "vv_renderer_get_stats": (C.c_int, [P, C.POINTER(RendererStats)]),
     "vv_renderer_frame_buffers": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "vv_renderer_read_color": (C.c_int, [P, P]),
+    "vv_renderer_read_color_async": (C.c_int, [P, P]),
+    "vv_renderer_wait_readback": (C.c_int, [P]),
     "vv_renderer_read_lists": (C.c_int, [P, P, P]),
     "vv_renderer_last_requests": (C.c_int, [P, P, C.c_int32, i32p]),
     "vv_renderer_residency": (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),

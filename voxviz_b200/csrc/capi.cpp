@@ -245,6 +245,16 @@ int vv_renderer_read_color(vv_renderer* r, float* host_rgba) {
     return VV_OK;
 }
 
+int vv_renderer_read_color_async(vv_renderer* r, float* host_rgba) {
+    if (!r || !host_rgba) return VV_ERR_ARG;
+    return r->impl->read_color_async(host_rgba);
+}
+
+int vv_renderer_wait_readback(vv_renderer* r) {
+    if (!r) return VV_ERR_ARG;
+    return r->impl->wait_readback();
+}
+
 int vv_renderer_read_lists(vv_renderer* r, uint32_t* host_usage, uint32_t* host_mask) {
     if (!r || !r->impl->d_usage) return VV_ERR_ARG;
     const size_t np = (size_t)r->impl->width * r->impl->height;

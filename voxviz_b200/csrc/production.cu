@@ -161,9 +161,9 @@ __global__ void __launch_bounds__(1024) dedupe_count_kernel(const uint32_t* __re
     if (threadIdx.x == 0) block_sums[blockIdx.x] = (uint32_t)c;
 }
 
-// Exclusive scan of the block sums in place, total to *count (one CTA).
-__global__ void __launch_bounds__(1024) scan_sums_kernel(uint32_t* __restrict__ sums, int nb,
-                                                         uint32_t* __restrict__ count) {
+// Exclusive scan of the block sums in place, total to *count (one CTA of
+// 1024 threads).
+__device__ void scan_sums(uint32_t* __restrict__ sums, int nb, uint32_t* __restrict__ count) {
     __shared__ uint32_t warp_tot[32];
     __shared__ uint32_t carry;
     if (threadIdx.x == 0) carry = 0u;
@@ -197,6 +197,19 @@ __global__ void __launch_bounds__(1024) scan_sums_kernel(uint32_t* __restrict__ 
     if (threadIdx.x == 0) *count = carry;
 }
 
+__global__ void __launch_bounds__(1024) scan_sums_kernel(uint32_t* __restrict__ sums, int nb,
+                                                         uint32_t* __restrict__ count) {
+    scan_sums(sums, nb, count);
+}
+
+// Two independent scans, one per CTA.
+__global__ void __launch_bounds__(1024) scan_sums2_kernel(uint32_t* __restrict__ sums_a, uint32_t* __restrict__ sums_b,
+                                                          int nb, uint32_t* __restrict__ count_a,
+                                                          uint32_t* __restrict__ count_b) {
+    if (blockIdx.x == 0) scan_sums(sums_a, nb, count_a);
+    else scan_sums(sums_b, nb, count_b);
+}
+
 __global__ void __launch_bounds__(1024) dedupe_scatter_kernel(const uint32_t* __restrict__ ids, int n, int dx,
                                                               int dy, int dz, uint32_t* __restrict__ first,
                                                               const uint32_t* __restrict__ block_off,
@@ -218,41 +231,257 @@ __global__ void __launch_bounds__(1024) dedupe_scatter_kernel(const uint32_t* __
     }
 }
 
-// Per distinct requested node (grid cell g, first-seen order), its state in
-// the device node pool: the brick-pool slot if resident, 0x80000000 | g if
-// neither resident nor constant (an upload candidate), 0xFFFFFFFF otherwise.
-__global__ void classify_kernel(const uint32_t* __restrict__ unique, const uint32_t* __restrict__ count,
-                                uint32_t max_n, const uint2* __restrict__ nodes, int dx, int dy, int dz, int sx,
-                                int sy, uint32_t* __restrict__ codes) {
-    const uint32_t n = min(*count, max_n);
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t g = unique[k];
-        const uint32_t x = g % (uint32_t)dx, y = (g / (uint32_t)dx) % (uint32_t)dy, z = g / ((uint32_t)dx * dy);
-        const uint32_t blk = ((z >> 1) * ((uint32_t)dy >> 1) + (y >> 1)) * ((uint32_t)dx >> 1) + (x >> 1);
-        const uint2 w = nodes[(size_t)blk * 8u + ((x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2))];
-        uint32_t c;
-        if (w.x & 0x80000000u) {
-            // brick pointer = slot origin + border (1,1,1), 10 texels per slot
-            const uint32_t px = ((w.y >> 20) & 0x3FFu) - 1u, py = ((w.y >> 10) & 0x3FFu) - 1u, pz = (w.y & 0x3FFu) - 1u;
-            c = ((pz / 10u) * (uint32_t)sy + py / 10u) * (uint32_t)sx + px / 10u;
-        } else if (w.x & 0x40000000u) {
-            c = 0xFFFFFFFFu;
-        } else {
-            c = 0x80000000u | g;
-        }
-        codes[k] = c;
+// State of a distinct requested node (grid cell g) in the device node pool
+// (block-linear, 2x2x2 node blocks): the brick-pool slot if resident,
+// 0x80000000 | g if neither resident nor constant (an upload candidate),
+// 0xFFFFFFFF otherwise.
+__device__ __forceinline__ uint32_t node_state(uint32_t g, const uint2* __restrict__ nodes, int dx, int dy, int sx,
+                                               int sy) {
+    const uint32_t x = g % (uint32_t)dx, y = (g / (uint32_t)dx) % (uint32_t)dy, z = g / ((uint32_t)dx * dy);
+    const uint32_t blk = ((z >> 1) * ((uint32_t)dy >> 1) + (y >> 1)) * ((uint32_t)dx >> 1) + (x >> 1);
+    const uint2 w = nodes[(size_t)blk * 8u + ((x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2))];
+    if (w.x & 0x80000000u) {
+        // brick pointer = slot origin + border (1,1,1), 10 texels per slot
+        const uint32_t px = ((w.y >> 20) & 0x3FFu) - 1u, py = ((w.y >> 10) & 0x3FFu) - 1u, pz = (w.y & 0x3FFu) - 1u;
+        return ((pz / 10u) * (uint32_t)sy + py / 10u) * (uint32_t)sx + px / 10u;
     }
+    return (w.x & 0x40000000u) ? 0xFFFFFFFFu : (0x80000000u | g);
+}
+
+__device__ __forceinline__ bool is_touch(uint32_t st, uint32_t root_slot) {
+    return st < 0x80000000u && st != root_slot;
+}
+__device__ __forceinline__ bool is_candidate(uint32_t st) { return (st & 0x80000000u) && st != 0xFFFFFFFFu; }
+
+// Per 1024 distinct nodes: their states (in place) and the block counts of
+// resident nodes other than the root's slot and of upload candidates.
+__global__ void __launch_bounds__(1024) classify_count_kernel(uint32_t* __restrict__ unique,
+                                                              const uint32_t* __restrict__ count, uint32_t max_n,
+                                                              const uint2* __restrict__ nodes, int dx, int dy, int sx,
+                                                              int sy, uint32_t root_slot,
+                                                              uint32_t* __restrict__ sums_touch,
+                                                              uint32_t* __restrict__ sums_cand) {
+    const uint32_t n = min(*count, max_n);
+    const uint32_t k = blockIdx.x * 1024u + threadIdx.x;
+    bool t = false, c = false;
+    if (k < n) {
+        const uint32_t st = node_state(unique[k], nodes, dx, dy, sx, sy);
+        unique[k] = st;
+        t = is_touch(st, root_slot);
+        c = is_candidate(st);
+    }
+    const int nt = __syncthreads_count(t);
+    const int nc = __syncthreads_count(c);
+    if (threadIdx.x == 0) {
+        sums_touch[blockIdx.x] = (uint32_t)nt;
+        sums_cand[blockIdx.x] = (uint32_t)nc;
+    }
+}
+
+// Offset of this lane's flagged element inside its CTA, from per-warp counts.
+__device__ __forceinline__ uint32_t warp_offset(const uint32_t* warp_cnt, int warp, int lane, unsigned ballot) {
+    uint32_t off = 0;
+    for (int w = 0; w < warp; ++w) off += warp_cnt[w];
+    return off + (uint32_t)__popc(ballot & ((1u << lane) - 1u));
+}
+
+// Scatter of the touched slots (first-seen order, marked with `epoch`) and of
+// the upload candidates' cells, from the scanned block counts.
+__global__ void __launch_bounds__(1024) split_scatter_kernel(const uint32_t* __restrict__ states,
+                                                             const uint32_t* __restrict__ count, uint32_t max_n,
+                                                             uint32_t root_slot, const uint32_t* __restrict__ off_touch,
+                                                             const uint32_t* __restrict__ off_cand, uint32_t n_slots,
+                                                             uint32_t epoch, uint32_t* __restrict__ seq,
+                                                             uint32_t* __restrict__ mark, uint32_t* __restrict__ cand,
+                                                             int* status) {
+    __shared__ uint32_t wt[32], wc[32];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && root_slot < n_slots) mark[root_slot] = epoch;
+    const uint32_t n = min(*count, max_n);
+    if (blockIdx.x * 1024u >= n) return;  // whole CTA
+    const uint32_t k = blockIdx.x * 1024u + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t st = k < n ? states[k] : 0xFFFFFFFFu;
+    const bool t = is_touch(st, root_slot), c = is_candidate(st);
+    const unsigned bt = __ballot_sync(0xFFFFFFFFu, t), bc = __ballot_sync(0xFFFFFFFFu, c);
+    if (lane == 0) {
+        wt[warp] = (uint32_t)__popc(bt);
+        wc[warp] = (uint32_t)__popc(bc);
+    }
+    __syncthreads();
+    if (t) {
+        const uint32_t off = off_touch[blockIdx.x] + warp_offset(wt, warp, lane, bt);
+        if (st < n_slots && off < n_slots) {
+            seq[off] = st;
+            mark[st] = epoch;
+        } else {
+            atomicCAS(status, 0, VV_ERR_BOUNDS);
+        }
+    }
+    if (c) cand[off_cand[blockIdx.x] + warp_offset(wc, warp, lane, bc)] = st & 0x7FFFFFFFu;
+}
+
+__global__ void mark_touched_kernel(const uint32_t* __restrict__ seq, uint32_t m, uint32_t n_slots, uint32_t epoch,
+                                    uint32_t* __restrict__ mark, int* status) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t s = seq[i];
+        if (s < n_slots) mark[s] = epoch;
+        else atomicCAS(status, 0, VV_ERR_BOUNDS);
+    }
+}
+
+__device__ __forceinline__ uint32_t ring(uint32_t head, uint32_t j, uint32_t n) {
+    const uint32_t p = head + j;
+    return p >= n ? p - n : p;
+}
+
+__global__ void __launch_bounds__(1024) order_count_kernel(const uint32_t* __restrict__ order, uint32_t n,
+                                                           uint32_t head, const uint32_t* __restrict__ mark,
+                                                           uint32_t epoch, uint32_t* __restrict__ sums) {
+    const uint32_t j = blockIdx.x * 1024u + threadIdx.x;
+    const uint32_t slot = j < n ? order[ring(head, j, n)] : n;
+    const bool f = slot < n && mark[slot] != epoch;  // a slot out of range drops out: the counts then disagree
+    const int c = __syncthreads_count(f);
+    if (threadIdx.x == 0) sums[blockIdx.x] = (uint32_t)c;
+}
+
+// CTAs [0, nb_order): the untouched slots in their order; the CTAs after
+// them: the touched slots (seq's m entries, then root_slot when it is a
+// slot) after the untouched ones.
+__global__ void __launch_bounds__(1024) order_scatter_kernel(const uint32_t* __restrict__ order, uint32_t n,
+                                                             uint32_t head, const uint32_t* __restrict__ mark,
+                                                             uint32_t epoch, const uint32_t* __restrict__ off,
+                                                             uint32_t nb_order, const uint32_t* __restrict__ counters,
+                                                             bool seq_on_device, uint32_t m_host, uint32_t root_slot,
+                                                             const uint32_t* __restrict__ seq,
+                                                             uint32_t* __restrict__ out, int* status) {
+    __shared__ uint32_t wcnt[32];
+    if (blockIdx.x < nb_order) {
+        const uint32_t j = blockIdx.x * 1024u + threadIdx.x;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        uint32_t slot = 0;
+        bool f = false;
+        if (j < n) {
+            slot = order[ring(head, j, n)];
+            f = slot < n && mark[slot] != epoch;
+        }
+        const unsigned b = __ballot_sync(0xFFFFFFFFu, f);
+        if (lane == 0) wcnt[warp] = (uint32_t)__popc(b);
+        __syncthreads();
+        if (f) out[off[blockIdx.x] + warp_offset(wcnt, warp, lane, b)] = slot;
+        return;
+    }
+    const uint32_t m = seq_on_device ? counters[1] : m_host;
+    const uint32_t u = counters[3];
+    const uint32_t total = m + (root_slot < n ? 1u : 0u);
+    if (u > n || total != n - u) {
+        if (blockIdx.x == nb_order && threadIdx.x == 0) atomicCAS(status, 0, VV_ERR_BOUNDS);
+        return;
+    }
+    const uint32_t stride = (gridDim.x - nb_order) * 1024u;
+    for (uint32_t i = (blockIdx.x - nb_order) * 1024u + threadIdx.x; i < total; i += stride)
+        out[u + i] = i < m ? seq[i] : root_slot;
+}
+
+__global__ void service_readout_kernel(const uint32_t* __restrict__ counters, const uint32_t* __restrict__ cand,
+                                       const uint32_t* __restrict__ order, uint32_t n_slots,
+                                       uint32_t* __restrict__ h_counters, uint32_t* __restrict__ h_cand,
+                                       uint32_t cand_cap, uint32_t* __restrict__ h_win) {
+    const uint32_t c = min(counters[2], cand_cap);
+    const uint32_t len = (uint32_t)min((unsigned long long)n_slots, 2ull * c + 2ull);
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (t < 4) h_counters[t] = counters[t];
+    for (uint32_t i = t; i < c; i += stride) h_cand[i] = cand[i];
+    for (uint32_t i = t; i < len; i += stride) h_win[i] = order[i];
+}
+
+__global__ void read_word_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst) { *dst = *src; }
+
+__global__ void iota_kernel(uint32_t* __restrict__ o, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = i;
 }
 
 }  // namespace
 
-cudaError_t launch_classify(const uint32_t* unique, const uint32_t* count, uint32_t max_n, const uint2* nodes,
-                            const int dim[3], const int slots[3], uint32_t* codes, cudaStream_t s) {
-    if (max_n == 0) return cudaSuccess;
-    const unsigned grid = (unsigned)std::min<uint32_t>((max_n + 255u) / 256u, 4736u);
-    classify_kernel<<<grid, 256, 0, s>>>(unique, count, max_n, nodes, dim[0], dim[1], dim[2], slots[0], slots[1],
-                                         codes);
+cudaError_t slot_order_init(SlotOrderBuffers& b, uint32_t n, cudaStream_t s) {
+    slot_order_free(b);
+    if (n == 0) return cudaErrorInvalidValue;
+    const size_t nb = (n + 1023u) / 1024u;
+    cudaError_t e;
+    if ((e = cudaMalloc((void**)&b.order[0], (size_t)n * 4)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&b.order[1], (size_t)n * 4)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&b.mark, (size_t)n * 4)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&b.seq, (size_t)n * 4)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&b.block_sums, nb * 4)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&b.counters, 4 * 4)) != cudaSuccess)
+        return e;
+    b.n = n;
+    b.cur = 0;
+    if ((e = cudaMemsetAsync(b.mark, 0, (size_t)n * 4, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(b.counters, 0, 16, s)) != cudaSuccess) return e;
+    // both buffers start as valid slot lists, so no stale entry is ever out of range
+    const unsigned grid = (unsigned)std::min<size_t>((n + 255u) / 256u, 4096u);
+    iota_kernel<<<grid, 256, 0, s>>>(b.order[0], n);
+    iota_kernel<<<grid, 256, 0, s>>>(b.order[1], n);
     return cudaGetLastError();
+}
+
+void slot_order_free(SlotOrderBuffers& b) {
+    void* bufs[] = {b.order[0], b.order[1], b.mark, b.seq, b.block_sums, b.counters, b.cand, b.cand_sums};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    b = SlotOrderBuffers{};
+}
+
+cudaError_t launch_classify_split(const DedupeBuffers& dd, uint32_t max_n, const uint2* nodes, const int dim[3],
+                                  const int slots[3], uint32_t root_slot, uint32_t epoch, SlotOrderBuffers& b,
+                                  int* status, cudaStream_t s) {
+    if (max_n == 0) return cudaMemsetAsync(b.counters + 1, 0, 8, s);
+    const size_t nb = (max_n + 1023u) / 1024u;
+    if (nb > dd.block_cap || nb > b.cand_sums_cap || max_n > dd.unique_cap || max_n > b.cand_cap)
+        return cudaErrorInvalidValue;
+    classify_count_kernel<<<(unsigned)nb, 1024, 0, s>>>(dd.unique, dd.count, max_n, nodes, dim[0], dim[1], slots[0],
+                                                         slots[1], root_slot, dd.block_sums, b.cand_sums);
+    scan_sums2_kernel<<<2, 1024, 0, s>>>(dd.block_sums, b.cand_sums, (int)nb, b.counters + 1, b.counters + 2);
+    split_scatter_kernel<<<(unsigned)nb, 1024, 0, s>>>(dd.unique, dd.count, max_n, root_slot, dd.block_sums,
+                                                        b.cand_sums, b.n, epoch, b.seq, b.mark, b.cand, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_service_readout(const SlotOrderBuffers& b, uint32_t* h_counters, uint32_t* h_cand,
+                                   uint32_t cand_cap, uint32_t* h_win, cudaStream_t s) {
+    service_readout_kernel<<<64, 256, 0, s>>>(b.counters, b.cand, b.order[b.cur], b.n, h_counters, h_cand, cand_cap,
+                                              h_win);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_read_word(const uint32_t* src, uint32_t* h_dst, cudaStream_t s) {
+    read_word_kernel<<<1, 1, 0, s>>>(src, h_dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mark_touched(SlotOrderBuffers& b, uint32_t m, uint32_t epoch, int* status, cudaStream_t s) {
+    if (m == 0) return cudaSuccess;
+    if (m > b.n) return cudaErrorInvalidValue;
+    mark_touched_kernel<<<(unsigned)std::min<uint32_t>((m + 255u) / 256u, 2048u), 256, 0, s>>>(b.seq, m, b.n, epoch,
+                                                                                             b.mark, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_order_partition(SlotOrderBuffers& b, uint32_t head, uint32_t epoch, bool seq_on_device,
+                                   uint32_t m_host, uint32_t max_m, uint32_t root_slot, int* status,
+                                   cudaStream_t s) {
+    if (b.n == 0 || head >= b.n) return cudaErrorInvalidValue;
+    const uint32_t nb = (b.n + 1023u) / 1024u;
+    const uint32_t bound = std::min<uint32_t>((seq_on_device ? max_m : m_host) + 1u, b.n);
+    const uint32_t append_blocks = std::max<uint32_t>(1u, std::min<uint32_t>((bound + 1023u) / 1024u, 148u));
+    order_count_kernel<<<nb, 1024, 0, s>>>(b.order[b.cur], b.n, head, b.mark, epoch, b.block_sums);
+    scan_sums_kernel<<<1, 1024, 0, s>>>(b.block_sums, (int)nb, b.counters + 3);
+    order_scatter_kernel<<<nb + append_blocks, 1024, 0, s>>>(b.order[b.cur], b.n, head, b.mark, epoch, b.block_sums,
+                                                             nb, b.counters, seq_on_device, m_host, root_slot, b.seq,
+                                                             b.order[b.cur ^ 1], status);
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) b.cur ^= 1;
+    return e;
 }
 
 cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs, int n, void* pool, int fmt,

@@ -68,14 +68,70 @@ struct DedupeBuffers {
     uint32_t* count = nullptr;       // number of distinct nodes
 };
 
-// State of each distinct node in the device node pool (block-linear, grid
-// dims `dim`): its brick slot when resident, 0x80000000 | cell when neither
-// resident nor constant, 0xFFFFFFFF when constant.  `count` is read on the
-// device; at most max_n entries.
-cudaError_t launch_classify(const uint32_t* unique, const uint32_t* count, uint32_t max_n, const uint2* nodes,
-                            const int dim[3], const int slots[3], uint32_t* codes, cudaStream_t s);
+// The brick pool's LRU order on the device (BrickPool::m_loadedBricks,
+// GigaVoxelsBrickPool.cpp:330-424, made deterministic): order[cur] lists
+// every slot once, least recently used first, read circularly from a head
+// position the host keeps.  Evicting the front and re-using its slot moves it
+// to the back, which in a full circular list is advancing the head, so only
+// touches of other slots move data: a partition keeps the untouched slots in
+// their order and appends the touched ones in touch order.
+struct SlotOrderBuffers {
+    uint32_t* order[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint32_t n = 0;                  // slots
+    uint32_t* mark = nullptr;        // per slot: epoch of the partition that last touched it
+    uint32_t* block_sums = nullptr;  // partition scan, one per 1024 slots
+    uint32_t* seq = nullptr;         // touched slots in touch order (n entries)
+    uint32_t* cand = nullptr;        // upload candidates: grid cells, first-seen order
+    size_t cand_cap = 0;
+    uint32_t* cand_sums = nullptr;   // candidate scan, one per 1024 distinct nodes
+    size_t cand_sums_cap = 0;
+    // device counters: [0] distinct nodes, [1] touched, [2] candidates, [3] untouched
+    uint32_t* counters = nullptr;
+};
 
-// De-duplicate the node ids of `n_entries` compacted entries (4 ids each).
+// Identity order (slot-id order: the empty slots lead), marks cleared.
+cudaError_t slot_order_init(SlotOrderBuffers& b, uint32_t n, cudaStream_t s);
+void slot_order_free(SlotOrderBuffers& b);
+
+// For the distinct requested nodes (dd.unique, dd.count: grid cells in
+// first-seen order) against the device node pool: the resident nodes' slots
+// go to seq in first-seen order, except root_slot (0xFFFFFFFF when the root
+// is not resident), and are marked with `epoch`, together with root_slot;
+// the cells of the non-resident, non-constant nodes go to cand.  Counts land
+// in counters[1] and [2].  At most max_n distinct nodes; dd.unique is
+// overwritten with each node's state (slot, 0x80000000 | cell, 0xFFFFFFFF).
+cudaError_t launch_classify_split(const DedupeBuffers& dd, uint32_t max_n, const uint2* nodes, const int dim[3],
+                                  const int slots[3], uint32_t root_slot, uint32_t epoch, SlotOrderBuffers& b,
+                                  int* status, cudaStream_t s);
+
+// Mark the m touched slots already in b.seq (host-known m) with `epoch`.
+cudaError_t launch_mark_touched(SlotOrderBuffers& b, uint32_t m, uint32_t epoch, int* status, cudaStream_t s);
+
+// Partition the order read from `head`: the slots not marked with `epoch`
+// keep their order, then the touched ones follow: seq's first m entries (m
+// from counters[1] when seq_on_device, else m_host) and root_slot last when
+// it is a slot.  Writes order[cur ^ 1] from position 0 and flips cur;
+// counters[3] receives the untouched count.  A touched count that does not
+// complete the list (a repeated or invalid slot) sets VV_ERR_BOUNDS.
+cudaError_t launch_order_partition(SlotOrderBuffers& b, uint32_t head, uint32_t epoch, bool seq_on_device,
+                                   uint32_t m_host, uint32_t max_m, uint32_t root_slot, int* status,
+                                   cudaStream_t s);
+
+// Read-out of a classified service into mapped host memory, written by the
+// SMs so that it does not queue behind copies on the copy engines (such as a
+// frame's colour read-back): counters[0..3] to h_counters, the candidates to
+// h_cand (at most cand_cap) and the order's first min(n, 2 * candidates + 2)
+// entries from position 0 to h_win.  All three are device views of mapped
+// host allocations.
+cudaError_t launch_service_readout(const SlotOrderBuffers& b, uint32_t* h_counters, uint32_t* h_cand,
+                                   uint32_t cand_cap, uint32_t* h_win, cudaStream_t s);
+
+// One word from device memory to mapped host memory.
+cudaError_t launch_read_word(const uint32_t* src, uint32_t* h_dst, cudaStream_t s);
+
+// De-duplicate the node ids of `n_entries` compacted entries (4 ids each);
+// the distinct count goes to b.count.
 cudaError_t launch_dedupe(const uint32_t* requests, int n_entries, const int grid_dim[3], const DedupeBuffers& b,
                           cudaStream_t s);
 

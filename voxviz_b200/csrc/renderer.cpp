@@ -130,47 +130,32 @@ void compute_uniforms(int depth, bool root_is_constant, const vv_camera& cam, co
     }
 }
 
-void SlotLRU::init(uint32_t n) {
-    n_ = n;
-    prev_.resize(n);
-    next_.resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        prev_[i] = i == 0 ? UINT32_MAX : i - 1;
-        next_[i] = i + 1 == n ? UINT32_MAX : i + 1;
-    }
-    head_ = 0;
-    tail_ = n ? n - 1 : 0;
-}
-
-void SlotLRU::touch(uint32_t s) {
-    if (s == tail_) return;
-    // unlink
-    uint32_t p = prev_[s], q = next_[s];
-    if (p != UINT32_MAX) next_[p] = q;
-    else head_ = q;
-    if (q != UINT32_MAX) prev_[q] = p;
-    // append
-    prev_[s] = tail_;
-    next_[s] = UINT32_MAX;
-    next_[tail_] = s;
-    tail_ = s;
-}
-
 GigaVoxelsRenderer::GigaVoxelsRenderer(vv_ctx* ctx, vv_octree*, const GigaVoxelsOctTree* tree,
                                        const vv_renderer_desc& d)
     : ctx_(ctx), tree_(tree), d_(d) {}
 
 GigaVoxelsRenderer::~GigaVoxelsRenderer() {
     if (ctx_) vv_ctx_synchronize(ctx_);
-    void* bufs[] = {d_color, d_usage, d_mask, d_requests, d_count};
+    if (copy_stream_) {
+        cudaStreamSynchronize(copy_stream_);
+        cudaStreamDestroy(copy_stream_);
+        for (cudaEvent_t e : {ev_copied_[0], ev_copied_[1], ev_drawn_})
+            if (e) cudaEventDestroy(e);
+    }
+    void* bufs[] = {color_buf_[0], color_buf_[1], d_usage, d_mask, d_requests, d_count};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h_stage_) cudaFreeHost(h_stage_);
     if (h_small_) cudaFreeHost(h_small_);
+    if (h_cand_) cudaFreeHost(h_cand_);
     if (h_unique_) cudaFreeHost(h_unique_);
-    void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, dd_.count, d_jobs_};
+    if (h_win_) cudaFreeHost(h_win_);
+    if (h_seq_) cudaFreeHost(h_seq_);
+    if (ev_seq_) cudaEventDestroy(ev_seq_);
+    void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, d_jobs_};  // dd_.count is in order_.counters
     for (void* b : dbufs)
         if (b) cudaFree(b);
+    slot_order_free(order_);
     void* hbufs[] = {h_def_jobs_, h_def_patches_, h_def_counts_};
     for (void* b : hbufs)
         if (b) cudaFreeHost(b);
@@ -196,6 +181,21 @@ int GigaVoxelsRenderer::init() {
     total_slots_ = (uint32_t)(sx * sy * sz);
     int rc = vv_brickpool_create(ctx_, slots_[0], slots_[1], slots_[2], d_.fmt);
     if (rc) return rc;
+    // LRU order: slot-id order on the device, and the same in the host window
+    if (slot_order_init(order_, total_slots_, ctx_->stream) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaHostAlloc((void**)&h_win_, (size_t)total_slots_ * 4, cudaHostAllocMapped) != cudaSuccess ||
+        cudaMallocHost((void**)&h_seq_, (size_t)total_slots_ * 4) != cudaSuccess)
+        return VV_ERR_OOM;
+    if (cudaHostGetDevicePointer((void**)&dh_win_, h_win_, 0) != cudaSuccess) return VV_ERR_CUDA;
+    rc = ensure_small();
+    if (rc) return rc;
+    if (cudaEventCreateWithFlags(&ev_seq_, cudaEventDisableTiming) != cudaSuccess) return VV_ERR_CUDA;
+    for (uint32_t i = 0; i < total_slots_; ++i) h_win_[i] = i;
+    head_ = 0;
+    epoch_ = 1;
+    win_start_ = 0;
+    win_len_ = total_slots_;
+    touch_seen_.assign(total_slots_, 0u);
     if (d_.device_paging) {
         device_paging_ = true;
         dterrain_ = std::make_unique<DeviceTerrain>();
@@ -204,7 +204,7 @@ int GigaVoxelsRenderer::init() {
         dd_.first_cells = (size_t)g[0] * g[1] * g[2];
         if (cudaMalloc((void**)&dd_.first, dd_.first_cells * 4) != cudaSuccess) return VV_ERR_OOM;
         if (cudaMemset(dd_.first, 0xFF, dd_.first_cells * 4) != cudaSuccess) return VV_ERR_CUDA;
-        if (cudaMalloc((void**)&dd_.count, 4) != cudaSuccess) return VV_ERR_OOM;
+        dd_.count = order_.counters;  // counters[0]: the distinct count
     }
     const size_t nn = tree_->node_count();
     w0_.resize(nn);
@@ -222,7 +222,6 @@ int GigaVoxelsRenderer::init() {
     make_jitter(d_.jitter_seed, 32, jit.data());
     rc = vv_set_jitter(ctx_, jit.data(), 32);
     if (rc) return rc;
-    lru_.init(total_slots_);
     slot_node_.assign(total_slots_, -1);
     node_slot_.assign(nn, -1);
     touched_mark_.assign(nn, 0);
@@ -247,16 +246,23 @@ int GigaVoxelsRenderer::init() {
 
 int GigaVoxelsRenderer::alloc_frame(int w, int h) {
     if (w == width && h == height && d_color) return VV_OK;
-    void** bufs[] = {(void**)&d_color, (void**)&d_usage, (void**)&d_mask, (void**)&d_requests, (void**)&d_count};
+    void** bufs[] = {(void**)&color_buf_[0], (void**)&color_buf_[1], (void**)&d_usage, (void**)&d_mask,
+                     (void**)&d_requests, (void**)&d_count};
     vv_ctx_synchronize(ctx_);
+    if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+    copy_pending_[0] = copy_pending_[1] = false;
     for (void** b : bufs)
         if (*b) {
             cudaFree(*b);
             *b = nullptr;
         }
+    d_color = nullptr;
     const size_t np = (size_t)w * h;
     cap_ = d_.request_cap > 0 ? d_.request_cap : (int)np;
-    if (cudaMalloc((void**)&d_color, np * 16) != cudaSuccess) return VV_ERR_OOM;
+    // two colour buffers: a frame's read-back may run while the next is drawn
+    if (cudaMalloc((void**)&color_buf_[0], np * 16) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMalloc((void**)&color_buf_[1], np * 16) != cudaSuccess) return VV_ERR_OOM;
+    d_color = color_buf_[cur_color_];
     if (cudaMalloc((void**)&d_usage, np * 48) != cudaSuccess) return VV_ERR_OOM;
     if (cudaMalloc((void**)&d_mask, np * 4) != cudaSuccess) return VV_ERR_OOM;
     if (cudaMalloc((void**)&d_requests, (size_t)cap_ * 16) != cudaSuccess) return VV_ERR_OOM;
@@ -269,6 +275,13 @@ int GigaVoxelsRenderer::alloc_frame(int w, int h) {
 int GigaVoxelsRenderer::draw(const vv_camera& cam) {
     int rc = alloc_frame(cam.width, cam.height);
     if (rc) return rc;
+    // alternate colour buffers; wait for a pending read-back of the one reused
+    cur_color_ ^= 1;
+    if (copy_pending_[cur_color_]) {
+        if (cudaStreamWaitEvent(ctx_->stream, ev_copied_[cur_color_], 0) != cudaSuccess) return VV_ERR_CUDA;
+        copy_pending_[cur_color_] = false;
+    }
+    d_color = color_buf_[cur_color_];
     compute_uniforms(tree_->depth(), tree_->is_constant(0), cam, slots_, d_.lod_scalar, d_.alpha_stop, last_u_);
     vv_frame_out o;
     std::memset(&o, 0, sizeof(o));
@@ -284,10 +297,128 @@ int GigaVoxelsRenderer::draw(const vv_camera& cam) {
     return vv_render(ctx_, 0, &last_u_, &o);
 }
 
+int GigaVoxelsRenderer::read_color_async(void* host) {
+    if (!d_color || !host) return VV_ERR_ARG;
+    if (!copy_stream_) {
+        if (cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking) != cudaSuccess) return VV_ERR_CUDA;
+        for (int i = 0; i < 2; ++i)
+            if (cudaEventCreateWithFlags(&ev_copied_[i], cudaEventDisableTiming) != cudaSuccess) return VV_ERR_CUDA;
+        if (cudaEventCreateWithFlags(&ev_drawn_, cudaEventDisableTiming) != cudaSuccess) return VV_ERR_CUDA;
+    }
+    if (cudaEventRecord(ev_drawn_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaStreamWaitEvent(copy_stream_, ev_drawn_, 0) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaMemcpyAsync(host, d_color, (size_t)width * height * 16, cudaMemcpyDeviceToHost, copy_stream_) !=
+        cudaSuccess)
+        return VV_ERR_CUDA;
+    if (cudaEventRecord(ev_copied_[cur_color_], copy_stream_) != cudaSuccess) return VV_ERR_CUDA;
+    copy_pending_[cur_color_] = true;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::wait_readback() {
+    if (copy_stream_ && cudaStreamSynchronize(copy_stream_) != cudaSuccess) return VV_ERR_CUDA;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::ensure_small() {
+    if (h_small_) return VV_OK;
+    if (cudaHostAlloc((void**)&h_small_, 32, cudaHostAllocMapped) != cudaSuccess) return VV_ERR_OOM;
+    std::memset(h_small_, 0, 32);
+    if (cudaHostGetDevicePointer((void**)&dh_small_, h_small_, 0) != cudaSuccess) return VV_ERR_CUDA;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::read_count(const uint32_t* count, uint32_t& out) {
+    int rc = ensure_small();
+    if (rc) return rc;
+    if (launch_read_word(count, dh_small_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    out = h_small_[0];
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::next_epoch() {
+    if (++epoch_ == 0) {  // marks of every earlier epoch would collide: clear them
+        if (cudaMemsetAsync(order_.mark, 0, (size_t)total_slots_ * 4, ctx_->stream) != cudaSuccess)
+            return VV_ERR_CUDA;
+        epoch_ = 1;
+    }
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::flush_touches() {
+    if (pending_touch_.empty()) return VV_OK;
+    const uint32_t n = total_slots_;
+    if (++touch_stamp_ == 0) {
+        std::fill(touch_seen_.begin(), touch_seen_.end(), 0u);
+        touch_stamp_ = 1;
+    }
+    // the previous partition's copy out of h_seq_ must have been read
+    if (cudaEventSynchronize(ev_seq_) != cudaSuccess) return VV_ERR_CUDA;
+    // a slot touched more than once keeps its last touch
+    uint32_t m = 0;
+    for (size_t i = pending_touch_.size(); i-- > 0;) {
+        const uint32_t s = pending_touch_[i];
+        if (s >= n) return ctx_fail(ctx_, VV_ERR_BOUNDS, "touch of a slot outside the brick pool");
+        if (touch_seen_[s] == touch_stamp_) continue;
+        touch_seen_[s] = touch_stamp_;
+        h_seq_[m++] = s;
+    }
+    std::reverse(h_seq_, h_seq_ + m);
+    pending_touch_.clear();
+    if (cudaMemcpyAsync(order_.seq, h_seq_, (size_t)m * 4, cudaMemcpyHostToDevice, ctx_->stream) != cudaSuccess ||
+        cudaEventRecord(ev_seq_, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (launch_mark_touched(order_, m, epoch_, ctx_->d_status, ctx_->stream) != cudaSuccess ||
+        launch_order_partition(order_, head_, epoch_, false, m, m, 0xFFFFFFFFu, ctx_->d_status, ctx_->stream) !=
+            cudaSuccess)
+        return VV_ERR_CUDA;
+    head_ = 0;
+    win_len_ = 0;
+    return next_epoch();
+}
+
+int GigaVoxelsRenderer::fetch_order(uint32_t want) {
+    const uint32_t n = total_slots_;
+    const uint32_t len = std::min<uint32_t>(n, std::max<uint32_t>(want, 65536u));
+    const uint32_t first = std::min<uint32_t>(len, n - head_);
+    const uint32_t* d = order_.order[order_.cur];
+    if (cudaMemcpyAsync(h_win_, d + head_, (size_t)first * 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (len > first &&
+        cudaMemcpyAsync(h_win_ + first, d, (size_t)(len - first) * 4, cudaMemcpyDeviceToHost, ctx_->stream) !=
+            cudaSuccess)
+        return VV_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    win_start_ = head_;
+    win_len_ = len;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::evict_front(uint32_t& s) {
+    int rc = flush_touches();  // touches made so far come before this eviction
+    if (rc) return rc;
+    const uint32_t n = total_slots_;
+    uint32_t off = head_ >= win_start_ ? head_ - win_start_ : head_ + n - win_start_;
+    if (off >= win_len_) {
+        rc = fetch_order(evict_hint_);
+        if (rc) return rc;
+        off = 0;
+    }
+    s = h_win_[off];
+    if (s >= n) return ctx_fail(ctx_, VV_ERR_BOUNDS, "the LRU order holds a slot outside the brick pool");
+    // the front slot goes to the back: in the full circular order, the head advances
+    head_ = head_ + 1 == n ? 0 : head_ + 1;
+    if (evict_hint_) --evict_hint_;
+    return VV_OK;
+}
+
 int GigaVoxelsRenderer::upload_nodes(uint32_t n) {
     // BrickPool::update body (GigaVoxelsBrickPool.cpp:583-629): evict the
     // LRU front, upload into its slot, move it to the back.
-    const uint32_t s = lru_.front();
+    uint32_t s;
+    const int rc = evict_front(s);
+    if (rc) return rc;
     const int32_t old = slot_node_[s];
     if (old >= 0) {
         node_slot_[(size_t)old] = -1;
@@ -310,7 +441,6 @@ int GigaVoxelsRenderer::upload_nodes(uint32_t n) {
         touched_mark_[n] = 1;
         touched_.push_back(n);
     }
-    lru_.touch(s);
     pending_nodes_.push_back(n);
     pending_slots_.push_back(s);
     ++uploaded_;
@@ -400,7 +530,7 @@ int GigaVoxelsRenderer::flush_uploads() {
 // GigaVoxelsOctTree.cpp:509-523): touch its brick if resident, else queue a
 // non-constant node for upload.
 void GigaVoxelsRenderer::visit(uint32_t nidx, std::vector<uint32_t>& upload) {
-    if (node_slot_[nidx] >= 0) lru_.touch((uint32_t)node_slot_[nidx]);
+    if (node_slot_[nidx] >= 0) touch((uint32_t)node_slot_[nidx]);
     else if (!tree_->is_constant(nidx)) upload.push_back(nidx);
 }
 
@@ -432,6 +562,7 @@ int GigaVoxelsRenderer::update_host(uint32_t n, std::vector<uint32_t>& upload) {
 
 int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload, const uint32_t* requests) {
     requests_on_host_ = false;
+    root_on_device_ = false;
     if (!n) return VV_OK;
     const size_t ids = (size_t)n * 4, blocks = (ids + 1023) / 1024;
     if (dd_.block_cap < blocks) {
@@ -450,69 +581,119 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
     if (launch_dedupe(requests, (int)n, pd, dd_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     // When the device node words hold this renderer's state (no node-word
     // change is pending on the host), the distinct nodes are classified on
-    // the device (in place) and the host only replays the LRU touches.
+    // the device, whose LRU order takes their touches and the root's; the
+    // host reads back only the upload candidates and the order's front.
     const bool classified = !deferred_ && touched_.empty();
+    uint32_t root_slot = 0xFFFFFFFFu;
     if (classified) {
-        const DeviceTree& t = ctx_->trees[0];
-        if (launch_classify(dd_.unique, dd_.count, (uint32_t)ids, t.nodes, t.dim, slots_, dd_.unique,
-                            ctx_->stream) != cudaSuccess)
-            return VV_ERR_CUDA;
-    }
-    // read-backs land in pinned memory (pageable copies are staged and slow)
-    if (cudaMemcpyAsync(h_small_ + 1, dd_.count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
-        return VV_ERR_CUDA;
-    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
-    const uint32_t u = h_small_[1];
-    if (h_unique_cap_ < u) {
-        if (h_unique_) cudaFreeHost(h_unique_);
-        h_unique_ = nullptr;
-        h_unique_cap_ = std::max((size_t)u, 2 * h_unique_cap_);
-        if (cudaMallocHost((void**)&h_unique_, h_unique_cap_ * 4) != cudaSuccess) {
-            h_unique_cap_ = 0;
-            return VV_ERR_OOM;
+        int rc = flush_touches();  // earlier host touches come first
+        if (rc) return rc;
+        if (order_.cand_cap < ids) {
+            if (order_.cand) cudaFree(order_.cand);
+            order_.cand = nullptr;
+            order_.cand_cap = std::max(ids, 2 * order_.cand_cap);
+            if (cudaMalloc((void**)&order_.cand, order_.cand_cap * 4) != cudaSuccess) {
+                order_.cand_cap = 0;
+                return VV_ERR_OOM;
+            }
         }
+        if (order_.cand_sums_cap < blocks) {
+            if (order_.cand_sums) cudaFree(order_.cand_sums);
+            order_.cand_sums = nullptr;
+            order_.cand_sums_cap = dd_.block_cap;
+            if (cudaMalloc((void**)&order_.cand_sums, order_.cand_sums_cap * 4) != cudaSuccess) {
+                order_.cand_sums_cap = 0;
+                return VV_ERR_OOM;
+            }
+        }
+        if (node_slot_[0] >= 0) root_slot = (uint32_t)node_slot_[0];
+        const DeviceTree& t = ctx_->trees[0];
+        if (launch_classify_split(dd_, (uint32_t)ids, t.nodes, t.dim, slots_, root_slot, epoch_, order_,
+                                  ctx_->d_status, ctx_->stream) != cudaSuccess ||
+            launch_order_partition(order_, head_, epoch_, true, 0, (uint32_t)std::min<size_t>(ids, total_slots_),
+                                   root_slot, ctx_->d_status, ctx_->stream) != cudaSuccess)
+            return VV_ERR_CUDA;
+        head_ = 0;
+        win_len_ = 0;
+        rc = next_epoch();
+        if (rc) return rc;
     }
-    if (u) {
-        if (cudaMemcpyAsync(h_unique_, dd_.unique, (size_t)u * 4, cudaMemcpyDeviceToHost, ctx_->stream) !=
+    uint32_t u = 0, back = 0;
+    const uint32_t* list = nullptr;
+    if (classified) {
+        // one read-out: counters, candidates and the order's front, enough
+        // for every upload a candidate can cause (itself and its parent)
+        if (h_cand_cap_ < ids) {
+            if (h_cand_) cudaFreeHost(h_cand_);
+            h_cand_ = nullptr;
+            h_cand_cap_ = std::max(ids, 2 * h_cand_cap_);
+            if (cudaHostAlloc((void**)&h_cand_, h_cand_cap_ * 4, cudaHostAllocMapped) != cudaSuccess) {
+                h_cand_cap_ = 0;
+                return VV_ERR_OOM;
+            }
+            if (cudaHostGetDevicePointer((void**)&dh_cand_, h_cand_, 0) != cudaSuccess) return VV_ERR_CUDA;
+        }
+        if (launch_service_readout(order_, dh_small_ + 4, dh_cand_, (uint32_t)h_cand_cap_, dh_win_, ctx_->stream) !=
             cudaSuccess)
             return VV_ERR_CUDA;
         if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+        u = h_small_[4];
+        back = h_small_[6];
+        const uint32_t m = h_small_[5], untouched = h_small_[7];
+        if (m > u || back > u || back > h_cand_cap_ || untouched > total_slots_ ||
+            m + (root_slot < total_slots_ ? 1u : 0u) != total_slots_ - untouched)
+            return ctx_fail(ctx_, VV_ERR_BOUNDS, "LRU order partition: touched and untouched counts disagree");
+        win_start_ = 0;
+        win_len_ = (uint32_t)std::min<size_t>(total_slots_, 2 * (size_t)back + 2);
+        list = h_cand_;
+    } else {
+        // every distinct node comes back for the host's visit
+        int rc = read_count(order_.counters, u);
+        if (rc) return rc;
+        back = u;
+        if (h_unique_cap_ < back) {
+            if (h_unique_) cudaFreeHost(h_unique_);
+            h_unique_ = nullptr;
+            h_unique_cap_ = std::max((size_t)back, 2 * h_unique_cap_);
+            if (cudaMallocHost((void**)&h_unique_, h_unique_cap_ * 4) != cudaSuccess) {
+                h_unique_cap_ = 0;
+                return VV_ERR_OOM;
+            }
+        }
+        if (back) {
+            if (cudaMemcpyAsync(h_unique_, dd_.unique, (size_t)back * 4, cudaMemcpyDeviceToHost, ctx_->stream) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(ctx_->stream) != cudaSuccess)
+                return VV_ERR_CUDA;
+        }
+        list = h_unique_;
     }
     const auto tv = std::chrono::steady_clock::now();
     const uint32_t dx = (uint32_t)pd[0], dy = (uint32_t)pd[1];
-    for (uint32_t k = 0; k < u; ++k) {
-        uint32_t g = h_unique_[k];
-        if (classified) {
-            if (g == 0xFFFFFFFFu) continue;           // constant, not resident
-            if (!(g & 0x80000000u)) {                 // resident: its slot
-                lru_.touch(g);
-                continue;
-            }
-            g &= 0x7FFFFFFFu;                         // upload candidate: checked below
-        }
+    for (uint32_t k = 0; k < back; ++k) {
+        const uint32_t g = list[k];
         const uint32_t nidx = tree_->index_of(g % dx, (g / dx) % dy, g / (dx * dy));
         if (nidx == kNoParent || tree_->level(nidx) < 0) continue;
         visit(nidx, upload);
     }
     ms_visit_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tv).count();
     unique_ = (int32_t)u;
+    root_on_device_ = classified;
     return VV_OK;
 }
 
 int GigaVoxelsRenderer::update() {
     if (!d_count) return VV_ERR_STATE;
     uploaded_ = 0;
-    if (!h_small_ && cudaMallocHost((void**)&h_small_, 16) != cudaSuccess) return VV_ERR_OOM;
-    if (cudaMemcpyAsync(h_small_, d_count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
-        return VV_ERR_CUDA;
-    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
-    const uint32_t count = h_small_[0];
+    uint32_t count = 0;
+    int rc = read_count(d_count, count);
+    if (rc) return rc;
     const auto t0 = std::chrono::steady_clock::now();  // the draw has finished here
     active_ = count;
     const uint32_t n = std::min<uint32_t>(count, (uint32_t)cap_);
     req_count_ = n;
     std::vector<uint32_t> upload;
-    int rc = device_paging_ ? update_device(n, upload, d_requests) : update_host(n, upload);
+    rc = device_paging_ ? update_device(n, upload, d_requests) : update_host(n, upload);
     if (rc) return rc;
     const auto t1 = std::chrono::steady_clock::now();
     ms_readback_ = std::chrono::duration<float, std::milli>(t1 - t0).count();
@@ -523,8 +704,11 @@ int GigaVoxelsRenderer::update() {
 }
 
 int GigaVoxelsRenderer::apply_policy(std::vector<uint32_t>& upload) {
-    // GigaVoxelsOctTree::update touches the root every frame (:1821-1850).
-    if (node_slot_[0] >= 0) lru_.touch((uint32_t)node_slot_[0]);
+    // GigaVoxelsOctTree::update touches the root every frame (:1821-1850);
+    // after a device classification that touch is already in the order.
+    if (!root_on_device_ && node_slot_[0] >= 0) touch((uint32_t)node_slot_[0]);
+    root_on_device_ = false;
+    evict_hint_ = 2 * (uint32_t)upload.size() + 1;
     // BrickPool::update (GigaVoxelsBrickPool.cpp:561-682), including the
     // upload of a non-resident non-constant parent (:629-673).
     for (uint32_t nidx : upload) {
@@ -537,23 +721,23 @@ int GigaVoxelsRenderer::apply_policy(std::vector<uint32_t>& upload) {
             if (rc) return rc;
         }
     }
-    return VV_OK;
+    evict_hint_ = 0;
+    return flush_touches();  // touches that no eviction followed
 }
 
 int GigaVoxelsRenderer::service(const uint32_t* requests, const uint32_t* count, int cap) {
     if (!device_paging_) return VV_ERR_STATE;
     if (!requests || !count || cap < 0) return VV_ERR_ARG;
     uploaded_ = 0;
-    if (!h_small_ && cudaMallocHost((void**)&h_small_, 16) != cudaSuccess) return VV_ERR_OOM;
-    if (cudaMemcpyAsync(h_small_, count, 4, cudaMemcpyDeviceToHost, ctx_->stream) != cudaSuccess)
-        return VV_ERR_CUDA;
-    if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    uint32_t c = 0;
+    int rc = read_count(count, c);
+    if (rc) return rc;
     const auto t0 = std::chrono::steady_clock::now();
-    active_ = h_small_[0];
-    const uint32_t n = std::min<uint32_t>(h_small_[0], (uint32_t)cap);
+    active_ = c;
+    const uint32_t n = std::min<uint32_t>(c, (uint32_t)cap);
     req_count_ = n;
     std::vector<uint32_t> upload;
-    int rc = update_device(n, upload, requests);
+    rc = update_device(n, upload, requests);
     if (rc) return rc;
     const auto t1 = std::chrono::steady_clock::now();
     ms_readback_ = std::chrono::duration<float, std::milli>(t1 - t0).count();

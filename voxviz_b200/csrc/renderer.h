@@ -22,22 +22,6 @@ float camera_pixel_size(const vv_camera& cam);
 // instead of srand(time): values in [1,255].
 void make_jitter(uint32_t seed, int size, uint8_t* out);
 
-// The brick pool's slot bookkeeping: an LRU list over slot ids
-// (BrickPool::m_loadedBricks, GigaVoxelsBrickPool.cpp:330-424) made
-// deterministic: touching a slot moves it to the back, eviction takes the
-// front, and initially the empty slots lead in slot-id order.
-class SlotLRU {
-public:
-    void init(uint32_t slots);
-    uint32_t front() const { return head_; }
-    void touch(uint32_t s);  // move to back
-    uint32_t size() const { return n_; }
-
-private:
-    std::vector<uint32_t> prev_, next_;
-    uint32_t head_ = 0, tail_ = 0, n_ = 0;
-};
-
 class GigaVoxelsRenderer {
 public:
     GigaVoxelsRenderer(vv_ctx* ctx, vv_octree* tree_handle, const GigaVoxelsOctTree* tree,
@@ -55,6 +39,10 @@ public:
     int set_deferred(bool on);
     int stage_uploads();
     int enqueue_uploads();
+    // Read-back of the last frame's colour on a copy stream (overlapping the
+    // page-request service and the next draw); wait_readback completes it.
+    int read_color_async(void* host);
+    int wait_readback();
     void stats(vv_renderer_stats& s) const;
 
     vv_ctx* ctx() { return ctx_; }
@@ -80,6 +68,16 @@ private:
     int update_device(uint32_t n, std::vector<uint32_t>& upload, const uint32_t* requests);
     int apply_policy(std::vector<uint32_t>& upload);
     void visit(uint32_t nidx, std::vector<uint32_t>& upload);
+    // The brick pool's LRU order (BrickPool::m_loadedBricks,
+    // GigaVoxelsBrickPool.cpp:330-424, made deterministic: touching a slot
+    // moves it to the back, eviction takes the front, initially the empty
+    // slots lead in slot-id order) lives on the device; touches made on the
+    // host wait in pending_touch_ until the next partition.
+    void touch(uint32_t s) { pending_touch_.push_back(s); }
+    int flush_touches();
+    int evict_front(uint32_t& s);      // the LRU slot, moved to the back
+    int fetch_order(uint32_t want);    // order entries from head_ into h_win_
+    int next_epoch();
 
     vv_ctx* ctx_;
     const GigaVoxelsOctTree* tree_;
@@ -87,7 +85,18 @@ private:
     int slots_[3] = {0, 0, 0};
     uint32_t total_slots_ = 0;
     size_t texel_bytes_ = 4;
-    SlotLRU lru_;
+    SlotOrderBuffers order_;
+    uint32_t head_ = 0;                  // position of the LRU front in order_.order[order_.cur]
+    uint32_t epoch_ = 1;                 // mark of the next partition's touches
+    uint32_t* h_win_ = nullptr;          // pinned: order entries from win_start_ on (circular)
+    uint32_t win_start_ = 0, win_len_ = 0;
+    uint32_t evict_hint_ = 0;            // evictions still expected in this service
+    bool root_on_device_ = false;        // this service's root touch is in the device partition
+    std::vector<uint32_t> pending_touch_;
+    std::vector<uint32_t> touch_seen_;   // per slot: stamp of its last de-duplication
+    uint32_t touch_stamp_ = 0;
+    uint32_t* h_seq_ = nullptr;          // pinned: de-duplicated pending touches
+    cudaEvent_t ev_seq_ = nullptr;       // the last copy out of h_seq_ has been read
     std::vector<int32_t> slot_node_;     // node index held by slot, -1 empty
     std::vector<int32_t> node_slot_;     // slot of node index, -1 not resident
     std::vector<uint32_t> w0_, w1_;      // current node words
@@ -108,8 +117,20 @@ private:
     bool device_paging_ = false;
     std::unique_ptr<DeviceTerrain> dterrain_;
     DedupeBuffers dd_;
-    uint32_t* h_small_ = nullptr;   // pinned: request count, distinct count
-    uint32_t* h_unique_ = nullptr;  // pinned: distinct node cells of the last frame
+    // Read-backs of the service go to mapped pinned memory, written by
+    // kernels (dh_* are the device views), so that they do not wait behind
+    // a colour read-back on the copy engines.
+    // [0] request count, [1] distinct count, [4..7] order_.counters
+    uint32_t* h_small_ = nullptr;
+    uint32_t* dh_small_ = nullptr;
+    uint32_t* h_cand_ = nullptr;    // upload candidates of a classified service
+    uint32_t* dh_cand_ = nullptr;
+    size_t h_cand_cap_ = 0;
+    uint32_t* dh_win_ = nullptr;
+    int ensure_small();
+    int read_count(const uint32_t* count, uint32_t& out);
+    // pinned: distinct node cells of the last frame (unclassified service)
+    uint32_t* h_unique_ = nullptr;
     size_t h_unique_cap_ = 0;
     std::vector<uint4> jobs_;
     uint4* d_jobs_ = nullptr;
@@ -124,6 +145,13 @@ private:
     uint32_t* h_def_counts_ = nullptr;   // [0] jobs, [1] patches
     uint32_t def_job_cap_ = 0, def_patch_cap_ = 0;
     std::vector<int32_t> slot_job_;      // staging: latest job index per slot
+    // colour buffers (alternating per draw) and their read-back
+    float* color_buf_[2] = {nullptr, nullptr};
+    int cur_color_ = 0;
+    cudaStream_t copy_stream_ = nullptr;
+    cudaEvent_t ev_copied_[2] = {nullptr, nullptr};
+    cudaEvent_t ev_drawn_ = nullptr;
+    bool copy_pending_[2] = {false, false};
 };
 
 }  // namespace vv
