@@ -499,12 +499,14 @@ int vv_renderer_frame_buffers(vv_renderer* r, float** color, uint32_t** usage,
                               uint32_t** request_count);
 /* Copy the last frame's colour (H*W*4 floats) to host memory. */
 int vv_renderer_read_color(vv_renderer* r, float* host_rgba);
-/* The same copy queued on the renderer's copy stream after the last draw,
- * returning at once (no counterpart in the reference, which blits on the
- * GL thread): it overlaps vv_renderer_update and the next draw (frames
- * alternate between two colour buffers; a draw waits only for the copy of
- * the buffer it reuses).  `host_rgba` should be pinned and must stay valid
- * until vv_renderer_wait_readback returns. */
+/* The same copy on the renderer's copy stream, returning at once (no
+ * counterpart in the reference, which blits on the GL thread).  The copy
+ * starts when the page-request service (vv_renderer_update or _service)
+ * has finished its read-outs, or at the next draw or wait, whichever comes
+ * first, and overlaps the next draw (frames alternate between two colour
+ * buffers; a draw waits only for the copy of the buffer it reuses).
+ * `host_rgba` should be pinned and must stay valid until
+ * vv_renderer_wait_readback returns. */
 int vv_renderer_read_color_async(vv_renderer* r, float* host_rgba);
 int vv_renderer_wait_readback(vv_renderer* r);
 /* Copy the last frame's node-usage lists (H*W*12 words) and selection mask

@@ -396,6 +396,15 @@ __global__ void service_readout_kernel(const uint32_t* __restrict__ counters, co
 
 __global__ void read_word_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst) { *dst = *src; }
 
+__global__ void pull_kernel(const uint4* __restrict__ src_a, uint4* __restrict__ dst_a, size_t n_a,
+                            const uint4* __restrict__ src_b, uint4* __restrict__ dst_b, size_t n_b) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_a + n_b; i += stride) {
+        if (i < n_a) dst_a[i] = src_a[i];
+        else dst_b[i - n_a] = src_b[i - n_a];
+    }
+}
+
 __global__ void iota_kernel(uint32_t* __restrict__ o, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = i;
 }
@@ -451,6 +460,16 @@ cudaError_t launch_service_readout(const SlotOrderBuffers& b, uint32_t* h_counte
                                    uint32_t cand_cap, uint32_t* h_win, cudaStream_t s) {
     service_readout_kernel<<<64, 256, 0, s>>>(b.counters, b.cand, b.order[b.cur], b.n, h_counters, h_cand, cand_cap,
                                               h_win);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pull(const uint4* src_a, uint4* dst_a, size_t n_a, const uint4* src_b, uint4* dst_b, size_t n_b,
+                        cudaStream_t s) {
+    const size_t n = n_a + n_b;
+    if (n == 0) return cudaSuccess;
+    // every read in flight at once: one 16-byte word per thread up to 148 x 8 CTAs
+    const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, 1184);
+    pull_kernel<<<grid, 256, 0, s>>>(src_a, dst_a, n_a, src_b, dst_b, n_b);
     return cudaGetLastError();
 }
 

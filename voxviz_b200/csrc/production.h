@@ -127,6 +127,12 @@ cudaError_t launch_order_partition(SlotOrderBuffers& b, uint32_t head, uint32_t 
 cudaError_t launch_service_readout(const SlotOrderBuffers& b, uint32_t* h_counters, uint32_t* h_cand,
                                    uint32_t cand_cap, uint32_t* h_win, cudaStream_t s);
 
+// Copy two ranges of 16-byte words from mapped host memory into device
+// memory, coalesced (a service's production jobs and node patches): the SMs
+// read over the bus, so nothing queues on the copy engines.
+cudaError_t launch_pull(const uint4* src_a, uint4* dst_a, size_t n_a, const uint4* src_b, uint4* dst_b, size_t n_b,
+                        cudaStream_t s);
+
 // One word from device memory to mapped host memory.
 cudaError_t launch_read_word(const uint32_t* src, uint32_t* h_dst, cudaStream_t s);
 

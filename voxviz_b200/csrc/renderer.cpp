@@ -152,11 +152,12 @@ GigaVoxelsRenderer::~GigaVoxelsRenderer() {
     if (h_win_) cudaFreeHost(h_win_);
     if (h_seq_) cudaFreeHost(h_seq_);
     if (ev_seq_) cudaEventDestroy(ev_seq_);
-    void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, d_jobs_};  // dd_.count is in order_.counters
+    void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, d_fjobs_, d_fpatch_};  // dd_.count: order_.counters
     for (void* b : dbufs)
         if (b) cudaFree(b);
     slot_order_free(order_);
-    void* hbufs[] = {h_def_jobs_, h_def_patches_, h_def_counts_};
+    if (ev_flush_) cudaEventDestroy(ev_flush_);
+    void* hbufs[] = {h_def_jobs_, h_def_patches_, h_def_counts_, h_fjobs_, h_fpatch_};
     for (void* b : hbufs)
         if (b) cudaFreeHost(b);
 }
@@ -189,7 +190,9 @@ int GigaVoxelsRenderer::init() {
     if (cudaHostGetDevicePointer((void**)&dh_win_, h_win_, 0) != cudaSuccess) return VV_ERR_CUDA;
     rc = ensure_small();
     if (rc) return rc;
-    if (cudaEventCreateWithFlags(&ev_seq_, cudaEventDisableTiming) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&ev_seq_, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_flush_, cudaEventDisableTiming) != cudaSuccess)
+        return VV_ERR_CUDA;
     for (uint32_t i = 0; i < total_slots_; ++i) h_win_[i] = i;
     head_ = 0;
     epoch_ = 1;
@@ -273,7 +276,9 @@ int GigaVoxelsRenderer::alloc_frame(int w, int h) {
 }
 
 int GigaVoxelsRenderer::draw(const vv_camera& cam) {
-    int rc = alloc_frame(cam.width, cam.height);
+    int rc = start_readback();  // a read-back requested without a service since
+    if (rc) return rc;
+    rc = alloc_frame(cam.width, cam.height);
     if (rc) return rc;
     // alternate colour buffers; wait for a pending read-back of the one reused
     cur_color_ ^= 1;
@@ -305,17 +310,35 @@ int GigaVoxelsRenderer::read_color_async(void* host) {
             if (cudaEventCreateWithFlags(&ev_copied_[i], cudaEventDisableTiming) != cudaSuccess) return VV_ERR_CUDA;
         if (cudaEventCreateWithFlags(&ev_drawn_, cudaEventDisableTiming) != cudaSuccess) return VV_ERR_CUDA;
     }
+    int rc = start_readback();  // an earlier request goes out first
+    if (rc) return rc;
     if (cudaEventRecord(ev_drawn_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
-    if (cudaStreamWaitEvent(copy_stream_, ev_drawn_, 0) != cudaSuccess) return VV_ERR_CUDA;
-    if (cudaMemcpyAsync(host, d_color, (size_t)width * height * 16, cudaMemcpyDeviceToHost, copy_stream_) !=
-        cudaSuccess)
-        return VV_ERR_CUDA;
-    if (cudaEventRecord(ev_copied_[cur_color_], copy_stream_) != cudaSuccess) return VV_ERR_CUDA;
+    // The copy starts at the end of the page-request service (update or
+    // service), or at the next draw or wait: the bulk transfer would
+    // otherwise hold the device-to-host direction of the bus while the
+    // service waits for its small read-outs.  It then overlaps the next ray
+    // cast instead.
+    readback_host_ = host;
+    readback_buf_ = cur_color_;
     copy_pending_[cur_color_] = true;
     return VV_OK;
 }
 
+int GigaVoxelsRenderer::start_readback() {
+    if (!readback_host_) return VV_OK;
+    void* host = readback_host_;
+    readback_host_ = nullptr;
+    if (cudaStreamWaitEvent(copy_stream_, ev_drawn_, 0) != cudaSuccess) return VV_ERR_CUDA;
+    if (cudaMemcpyAsync(host, color_buf_[readback_buf_], (size_t)width * height * 16, cudaMemcpyDeviceToHost,
+                        copy_stream_) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (cudaEventRecord(ev_copied_[readback_buf_], copy_stream_) != cudaSuccess) return VV_ERR_CUDA;
+    return VV_OK;
+}
+
 int GigaVoxelsRenderer::wait_readback() {
+    int rc = start_readback();
+    if (rc) return rc;
     if (copy_stream_ && cudaStreamSynchronize(copy_stream_) != cudaSuccess) return VV_ERR_CUDA;
     return VV_OK;
 }
@@ -450,39 +473,28 @@ int GigaVoxelsRenderer::upload_nodes(uint32_t n) {
 }
 
 int GigaVoxelsRenderer::flush_uploads() {
-    const size_t n = pending_nodes_.size();
     int rc = VV_OK;
     ms_produce_ = 0.0f;
     const auto t0 = std::chrono::steady_clock::now();
-    if (n && device_paging_) {
-        // brick production on the GPU, straight into the slots
-        jobs_.resize(n);
-        for (size_t i = 0; i < n; ++i) {
-            const uint32_t node = pending_nodes_[i];
-            int ci, cj, ck;
-            tree_->origin(node, ci, cj, ck);
-            jobs_[i] = make_uint4(pending_slots_[i], (uint32_t)tree_->level(node),
-                                  ((uint32_t)ci << 20) | ((uint32_t)cj << 10) | (uint32_t)ck, 0u);
-        }
-        if (jobs_cap_ < n) {
-            if (d_jobs_) cudaFree(d_jobs_);
-            d_jobs_ = nullptr;
-            jobs_cap_ = std::max(n, 2 * jobs_cap_);
-            if (cudaMalloc((void**)&d_jobs_, jobs_cap_ * sizeof(uint4)) != cudaSuccess) {
-                jobs_cap_ = 0;
-                return VV_ERR_OOM;
-            }
-        }
-        if (cudaMemcpyAsync(d_jobs_, jobs_.data(), n * sizeof(uint4), cudaMemcpyHostToDevice, ctx_->stream) !=
-            cudaSuccess)
-            return VV_ERR_CUDA;
-        void* pool = nullptr;
-        size_t pool_bytes = 0;
-        vv_brickpool_device_ptr(ctx_, &pool, &pool_bytes);
-        if (launch_produce_bricks(dterrain_->view(), d_jobs_, (int)n, pool, d_.fmt, (long long)total_slots_,
-                                  ctx_->d_status, ctx_->stream) != cudaSuccess)
-            return VV_ERR_CUDA;
-    } else if (n) {
+    // One upload per slot, the latest: a slot re-used within a service holds
+    // its last node, and the bricks of one launch are written in no fixed
+    // order.  keep_ lists those pending uploads, latest first.
+    if (slot_job_.size() != total_slots_) slot_job_.assign(total_slots_, -1);
+    keep_.clear();
+    for (size_t i = pending_nodes_.size(); i-- > 0;) {
+        const uint32_t s = pending_slots_[i];
+        if (slot_job_[s] >= 0) continue;
+        slot_job_[s] = (int32_t)i;
+        keep_.push_back((uint32_t)i);
+    }
+    for (uint32_t i : keep_) slot_job_[pending_slots_[i]] = -1;
+    const size_t n = keep_.size();
+    if (device_paging_) {
+        rc = flush_device();
+        ms_upload_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
+    }
+    if (n) {
         const size_t bb = VV_BRICK_TEXELS * texel_bytes_;
         const size_t bytes = n * bb;
         if (h_stage_cap_ < bytes) {
@@ -496,13 +508,16 @@ int GigaVoxelsRenderer::flush_uploads() {
         }
         unsigned char* st = (unsigned char*)h_stage_;
         const int fmt = d_.fmt;
+        up_slots_.resize(n);
+        for (size_t k = 0; k < n; ++k) up_slots_[k] = pending_slots_[keep_[k]];
 #pragma omp parallel for schedule(dynamic, 16) num_threads(d_.producer_threads > 0 ? d_.producer_threads : omp_get_max_threads())
-        for (long i = 0; i < (long)n; ++i) tree_->produce_brick(pending_nodes_[(size_t)i], fmt, st + (size_t)i * bb);
+        for (long k = 0; k < (long)n; ++k)
+            tree_->produce_brick(pending_nodes_[keep_[(size_t)k]], fmt, st + (size_t)k * bb);
         ms_produce_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     const auto t2 = std::chrono::steady_clock::now();
-    if (n && !device_paging_) {
-        rc = vv_upload_bricks(ctx_, pending_slots_.data(), (int32_t)n, h_stage_);
+    if (n) {
+        rc = vv_upload_bricks(ctx_, up_slots_.data(), (int32_t)n, h_stage_);
         if (rc) return rc;
     }
     if (!touched_.empty()) {
@@ -524,6 +539,79 @@ int GigaVoxelsRenderer::flush_uploads() {
     pending_slots_.clear();
     ms_upload_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t2).count();
     return rc;
+}
+
+// Device paging: brick production on the GPU, straight into the slots, and
+// the node patches.  Jobs and patches are written to mapped pinned memory;
+// one coalesced kernel pulls them into device memory, so the service queues
+// no transfer on the copy engines (which a frame's colour read-back may
+// hold), and the production and patch kernels read device memory.
+int GigaVoxelsRenderer::flush_device() {
+    const size_t n = keep_.size(), np = touched_.size();
+    if (n == 0 && np == 0) {
+        pending_nodes_.clear();
+        pending_slots_.clear();
+        return VV_OK;
+    }
+    // the previous flush's pull has finished reading the mapped buffers
+    if (cudaEventSynchronize(ev_flush_) != cudaSuccess) return VV_ERR_CUDA;
+    if (fjobs_cap_ < n) {  // pinned allocations are slow: grow geometrically
+        if (h_fjobs_) cudaFreeHost(h_fjobs_);
+        if (d_fjobs_) cudaFree(d_fjobs_);
+        h_fjobs_ = d_fjobs_ = nullptr;
+        fjobs_cap_ = std::max<size_t>(std::max(n, 2 * fjobs_cap_), 16384);
+        if (cudaHostAlloc((void**)&h_fjobs_, fjobs_cap_ * sizeof(uint4), cudaHostAllocMapped) != cudaSuccess ||
+            cudaMalloc((void**)&d_fjobs_, fjobs_cap_ * sizeof(uint4)) != cudaSuccess) {
+            fjobs_cap_ = 0;
+            return VV_ERR_OOM;
+        }
+        if (cudaHostGetDevicePointer((void**)&dh_fjobs_, h_fjobs_, 0) != cudaSuccess) return VV_ERR_CUDA;
+    }
+    if (fpatch_cap_ < np) {
+        if (h_fpatch_) cudaFreeHost(h_fpatch_);
+        if (d_fpatch_) cudaFree(d_fpatch_);
+        h_fpatch_ = d_fpatch_ = nullptr;
+        fpatch_cap_ = std::max<size_t>(std::max(np, 2 * fpatch_cap_), 32768);
+        // whole 16-byte words: the pull reads the last partial one
+        const size_t bytes = (fpatch_cap_ * sizeof(vv_node_patch) + 15) / 16 * 16;
+        if (cudaHostAlloc((void**)&h_fpatch_, bytes, cudaHostAllocMapped) != cudaSuccess ||
+            cudaMalloc((void**)&d_fpatch_, bytes) != cudaSuccess) {
+            fpatch_cap_ = 0;
+            return VV_ERR_OOM;
+        }
+        if (cudaHostGetDevicePointer((void**)&dh_fpatch_, h_fpatch_, 0) != cudaSuccess) return VV_ERR_CUDA;
+    }
+    for (size_t k = 0; k < n; ++k) {
+        const uint32_t i = keep_[k], node = pending_nodes_[i];
+        int ci, cj, ck;
+        tree_->origin(node, ci, cj, ck);
+        h_fjobs_[k] = make_uint4(pending_slots_[i], (uint32_t)tree_->level(node),
+                                 ((uint32_t)ci << 20) | ((uint32_t)cj << 10) | (uint32_t)ck, 0u);
+    }
+    for (size_t k = 0; k < np; ++k) {
+        const uint32_t t = touched_[k];
+        vv_node_patch& q = h_fpatch_[k];
+        tree_->grid_of(t, q.x, q.y, q.z);
+        q.word0 = w0_[t];
+        q.word1 = w1_[t];
+        touched_mark_[t] = 0;
+    }
+    void* pool = nullptr;
+    size_t pool_bytes = 0;
+    vv_brickpool_device_ptr(ctx_, &pool, &pool_bytes);
+    const DeviceTree& t = ctx_->trees[0];
+    const size_t patch_words = (np * sizeof(vv_node_patch) + 15) / 16;
+    if (launch_pull(dh_fjobs_, d_fjobs_, n, (const uint4*)dh_fpatch_, (uint4*)d_fpatch_, patch_words,
+                    ctx_->stream) != cudaSuccess ||
+        cudaEventRecord(ev_flush_, ctx_->stream) != cudaSuccess ||
+        launch_produce_bricks(dterrain_->view(), d_fjobs_, (int)n, pool, d_.fmt, (long long)total_slots_,
+                              ctx_->d_status, ctx_->stream) != cudaSuccess ||
+        launch_node_patch(d_fpatch_, (int)np, t.nodes, t.dim, ctx_->d_status, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    touched_.clear();
+    pending_nodes_.clear();
+    pending_slots_.clear();
+    return VV_OK;
 }
 
 // One distinct requested node, in first-seen order (NodeUsageListProcessor::run,
@@ -700,7 +788,9 @@ int GigaVoxelsRenderer::update() {
     rc = apply_policy(upload);
     if (rc) return rc;
     ms_policy_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
-    return deferred_ ? VV_OK : flush_uploads();
+    rc = deferred_ ? VV_OK : flush_uploads();
+    if (rc) return rc;
+    return start_readback();  // the service's last read-out is done
 }
 
 int GigaVoxelsRenderer::apply_policy(std::vector<uint32_t>& upload) {
@@ -744,7 +834,9 @@ int GigaVoxelsRenderer::service(const uint32_t* requests, const uint32_t* count,
     rc = apply_policy(upload);
     if (rc) return rc;
     ms_policy_ = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
-    return deferred_ ? VV_OK : flush_uploads();
+    rc = deferred_ ? VV_OK : flush_uploads();
+    if (rc) return rc;
+    return start_readback();  // the service's last read-out is done
 }
 
 int GigaVoxelsRenderer::set_deferred(bool on) {

@@ -39,8 +39,9 @@ public:
     int set_deferred(bool on);
     int stage_uploads();
     int enqueue_uploads();
-    // Read-back of the last frame's colour on a copy stream (overlapping the
-    // page-request service and the next draw); wait_readback completes it.
+    // Read-back of the last frame's colour on a copy stream, started once
+    // the page-request service is done (overlapping the next draw);
+    // wait_readback completes it.
     int read_color_async(void* host);
     int wait_readback();
     void stats(vv_renderer_stats& s) const;
@@ -132,9 +133,19 @@ private:
     // pinned: distinct node cells of the last frame (unclassified service)
     uint32_t* h_unique_ = nullptr;
     size_t h_unique_cap_ = 0;
-    std::vector<uint4> jobs_;
-    uint4* d_jobs_ = nullptr;
-    size_t jobs_cap_ = 0;
+    // eager device uploads: production jobs and node patches in mapped
+    // pinned memory (h_*, device views dh_*) pulled into device copies
+    // (d_*); ev_flush_ marks the end of the pull
+    int flush_device();
+    uint4* h_fjobs_ = nullptr;
+    uint4* dh_fjobs_ = nullptr;
+    uint4* d_fjobs_ = nullptr;
+    size_t fjobs_cap_ = 0;
+    vv_node_patch* h_fpatch_ = nullptr;
+    vv_node_patch* dh_fpatch_ = nullptr;
+    vv_node_patch* d_fpatch_ = nullptr;
+    size_t fpatch_cap_ = 0;
+    cudaEvent_t ev_flush_ = nullptr;
     bool requests_on_host_ = false;
     void* h_stage_ = nullptr;            // pinned brick staging
     size_t h_stage_cap_ = 0;
@@ -144,7 +155,9 @@ private:
     vv_node_patch* h_def_patches_ = nullptr;
     uint32_t* h_def_counts_ = nullptr;   // [0] jobs, [1] patches
     uint32_t def_job_cap_ = 0, def_patch_cap_ = 0;
-    std::vector<int32_t> slot_job_;      // staging: latest job index per slot
+    std::vector<int32_t> slot_job_;      // latest pending upload per slot (-1 between uses)
+    std::vector<uint32_t> keep_;         // pending uploads kept by a flush
+    std::vector<uint32_t> up_slots_;     // their slots (host production)
     // colour buffers (alternating per draw) and their read-back
     float* color_buf_[2] = {nullptr, nullptr};
     int cur_color_ = 0;
@@ -152,6 +165,9 @@ private:
     cudaEvent_t ev_copied_[2] = {nullptr, nullptr};
     cudaEvent_t ev_drawn_ = nullptr;
     bool copy_pending_[2] = {false, false};
+    void* readback_host_ = nullptr;      // a requested read-back not started yet
+    int readback_buf_ = 0;
+    int start_readback();
 };
 
 }  // namespace vv
