@@ -292,7 +292,7 @@ __global__ void node_patch_kernel(const vv_node_patch* __restrict__ patches, int
 __global__ void node_patch_staged_kernel(const vv_node_patch* patches, const volatile uint32_t* count,
                                          uint32_t max_patches, uint2* __restrict__ nodes, int dx, int dy, int dz,
                                          int* status) {
-    __shared__ uint32_t s_n;  // one read of host memory per CTA
+    __shared__ uint32_t s_n;  // one read of the count per CTA
     if (threadIdx.x == 0) s_n = min(*count, max_patches);
     __syncthreads();
     const uint32_t n = s_n;

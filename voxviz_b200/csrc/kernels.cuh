@@ -60,8 +60,9 @@ cudaError_t launch_node_upload(const uint32_t* grid_words, uint2* nodes, const i
                                cudaStream_t s);
 cudaError_t launch_node_download(const uint2* nodes, uint32_t* grid_words, const int dim[3],
                                  cudaStream_t s);
-// Patches and their count read on the device from pinned, mapped host
-// memory (at most max_patches): a count-independent launch for CUDA graphs.
+// Patches and their count read on the device (at most max_patches): a
+// count-independent launch for CUDA graphs.  Device copies of both make it
+// fast (mapped host memory costs a bus round trip per CTA).
 cudaError_t launch_node_patch_staged(const vv_node_patch* patches, const uint32_t* count, uint32_t max_patches,
                                      uint2* nodes, const int dim[3], int* status, cudaStream_t s);
 cudaError_t launch_node_patch(const vv_node_patch* patches, int n, uint2* nodes, const int dim[3],

@@ -115,14 +115,15 @@ __global__ void produce_kernel(const __grid_constant__ DeviceTerrainView t, cons
     produce_one<FMT>(t, jobs[blockIdx.x], pool, total_slots, status);
 }
 
-// Staged form: jobs and their count live in pinned host memory mapped into
-// the device address space and are read here, so the launch itself does not
-// depend on the count (it can sit in a CUDA graph replayed every frame).
+// Staged form: the job count is read on the device, so the launch itself
+// does not depend on it (it can sit in a CUDA graph replayed every frame).
+// Jobs and count are device copies (see launch_pull_staged): a read of
+// mapped host memory from every CTA costs a bus round trip each.
 template <int FMT>
 __global__ void produce_staged_kernel(const __grid_constant__ DeviceTerrainView t, const uint4* jobs,
                                       const volatile uint32_t* count, uint32_t max_jobs, void* __restrict__ pool,
                                       long long total_slots, int* status) {
-    __shared__ uint32_t s_n;  // one read of host memory per CTA
+    __shared__ uint32_t s_n;  // one read of the count per CTA
     if (threadIdx.x == 0) s_n = min(*count, max_jobs);
     __syncthreads();
     const uint32_t n = s_n;
@@ -396,6 +397,23 @@ __global__ void service_readout_kernel(const uint32_t* __restrict__ counters, co
 
 __global__ void read_word_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst) { *dst = *src; }
 
+__global__ void pull_staged_kernel(const volatile uint32_t* h_counts, const uint4* __restrict__ h_jobs,
+                                   uint32_t max_jobs, const uint4* __restrict__ h_patch_words, uint32_t max_patches,
+                                   uint32_t* __restrict__ d_counts, uint4* __restrict__ d_jobs,
+                                   uint4* __restrict__ d_patch_words) {
+    __shared__ uint32_t s_n[2];
+    if (threadIdx.x < 2) s_n[threadIdx.x] = min(h_counts[threadIdx.x], threadIdx.x ? max_patches : max_jobs);
+    __syncthreads();
+    const uint32_t nj = s_n[0], np = s_n[1];
+    if (blockIdx.x == 0 && threadIdx.x < 2) d_counts[threadIdx.x] = s_n[threadIdx.x];
+    const size_t nw = ((size_t)np * 20u + 15u) / 16u;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nj + nw; i += stride) {
+        if (i < nj) d_jobs[i] = h_jobs[i];
+        else d_patch_words[i - nj] = h_patch_words[i - nj];
+    }
+}
+
 __global__ void pull_kernel(const uint4* __restrict__ src_a, uint4* __restrict__ dst_a, size_t n_a,
                             const uint4* __restrict__ src_b, uint4* __restrict__ dst_b, size_t n_b) {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -470,6 +488,14 @@ cudaError_t launch_pull(const uint4* src_a, uint4* dst_a, size_t n_a, const uint
     // every read in flight at once: one 16-byte word per thread up to 148 x 8 CTAs
     const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, 1184);
     pull_kernel<<<grid, 256, 0, s>>>(src_a, dst_a, n_a, src_b, dst_b, n_b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pull_staged(const uint32_t* h_counts, const uint4* h_jobs, uint32_t max_jobs,
+                               const void* h_patches, uint32_t max_patches, uint32_t* d_counts, uint4* d_jobs,
+                               void* d_patches, cudaStream_t s) {
+    pull_staged_kernel<<<64, 256, 0, s>>>(h_counts, h_jobs, max_jobs, (const uint4*)h_patches, max_patches, d_counts,
+                                          d_jobs, (uint4*)d_patches);
     return cudaGetLastError();
 }
 

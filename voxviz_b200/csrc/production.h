@@ -52,8 +52,9 @@ private:
 cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs, int n, void* pool, int fmt,
                                   long long total_slots, int* status, cudaStream_t s);
 
-// The same with jobs and their count read on the device from pinned, mapped
-// host memory (at most max_jobs): a count-independent launch for CUDA graphs.
+// The same with the job count read on the device (at most max_jobs): a
+// count-independent launch for CUDA graphs.  Jobs and count should be in
+// device memory (launch_pull_staged puts them there).
 cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs, const uint32_t* count,
                                   uint32_t max_jobs, void* pool, int fmt, long long total_slots, int* status,
                                   cudaStream_t s);
@@ -132,6 +133,16 @@ cudaError_t launch_service_readout(const SlotOrderBuffers& b, uint32_t* h_counte
 // read over the bus, so nothing queues on the copy engines.
 cudaError_t launch_pull(const uint4* src_a, uint4* dst_a, size_t n_a, const uint4* src_b, uint4* dst_b, size_t n_b,
                         cudaStream_t s);
+
+// The same for staged uploads, whose counts are read on the device (a
+// count-independent launch for CUDA graphs): h_counts[0] jobs (at most
+// max_jobs) and h_counts[1] node patches (at most max_patches, 20 bytes
+// each, the mapped allocation rounded up to whole 16-byte words) are pulled
+// into d_jobs / d_patches, the clamped counts into d_counts[0..1].  A few
+// CTAs, each reading the counts once.
+cudaError_t launch_pull_staged(const uint32_t* h_counts, const uint4* h_jobs, uint32_t max_jobs,
+                               const void* h_patches, uint32_t max_patches, uint32_t* d_counts, uint4* d_jobs,
+                               void* d_patches, cudaStream_t s);
 
 // One word from device memory to mapped host memory.
 cudaError_t launch_read_word(const uint32_t* src, uint32_t* h_dst, cudaStream_t s);

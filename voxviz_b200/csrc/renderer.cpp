@@ -152,7 +152,8 @@ GigaVoxelsRenderer::~GigaVoxelsRenderer() {
     if (h_win_) cudaFreeHost(h_win_);
     if (h_seq_) cudaFreeHost(h_seq_);
     if (ev_seq_) cudaEventDestroy(ev_seq_);
-    void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, d_fjobs_, d_fpatch_};  // dd_.count: order_.counters
+    void* dbufs[] = {dd_.first, dd_.block_sums, dd_.unique, d_fjobs_, d_fpatch_,  // dd_.count: order_.counters
+                     d_def_jobs_, d_def_patches_, d_def_counts_};
     for (void* b : dbufs)
         if (b) cudaFree(b);
     slot_order_free(order_);
@@ -851,11 +852,15 @@ int GigaVoxelsRenderer::set_deferred(bool on) {
         // earlier ones); a node is patched at most once
         def_job_cap_ = total_slots_;
         def_patch_cap_ = (uint32_t)std::min<size_t>(w0_.size(), 2 * (size_t)total_slots_ + 4096);
+        // patches in whole 16-byte words: the pull reads the last partial one
+        const size_t patch_bytes = ((size_t)def_patch_cap_ * sizeof(vv_node_patch) + 15) / 16 * 16;
         if (cudaHostAlloc((void**)&h_def_jobs_, (size_t)def_job_cap_ * sizeof(uint4), cudaHostAllocMapped) !=
                 cudaSuccess ||
-            cudaHostAlloc((void**)&h_def_patches_, (size_t)def_patch_cap_ * sizeof(vv_node_patch),
-                          cudaHostAllocMapped) != cudaSuccess ||
-            cudaHostAlloc((void**)&h_def_counts_, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess)
+            cudaHostAlloc((void**)&h_def_patches_, patch_bytes, cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostAlloc((void**)&h_def_counts_, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
+            cudaMalloc((void**)&d_def_jobs_, (size_t)def_job_cap_ * sizeof(uint4)) != cudaSuccess ||
+            cudaMalloc((void**)&d_def_patches_, patch_bytes) != cudaSuccess ||
+            cudaMalloc((void**)&d_def_counts_, 2 * sizeof(uint32_t)) != cudaSuccess)
             return VV_ERR_OOM;
         h_def_counts_[0] = h_def_counts_[1] = 0;
         slot_job_.assign(total_slots_, -1);
@@ -919,11 +924,16 @@ int GigaVoxelsRenderer::enqueue_uploads() {
     void* pool = nullptr;
     size_t pool_bytes = 0;
     vv_brickpool_device_ptr(ctx_, &pool, &pool_bytes);
-    if (launch_produce_staged(dterrain_->view(), jobs, counts, def_job_cap_, pool, d_.fmt, (long long)total_slots_,
-                              ctx_->d_status, ctx_->stream) != cudaSuccess)
+    // counts, jobs and patches into device memory, then production and
+    // patches from there
+    if (launch_pull_staged(counts, jobs, def_job_cap_, patches, def_patch_cap_, d_def_counts_, d_def_jobs_,
+                           d_def_patches_, ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    if (launch_produce_staged(dterrain_->view(), d_def_jobs_, d_def_counts_, def_job_cap_, pool, d_.fmt,
+                              (long long)total_slots_, ctx_->d_status, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
     const DeviceTree& t = ctx_->trees[0];
-    if (launch_node_patch_staged(patches, counts + 1, def_patch_cap_, t.nodes, t.dim, ctx_->d_status,
+    if (launch_node_patch_staged(d_def_patches_, d_def_counts_ + 1, def_patch_cap_, t.nodes, t.dim, ctx_->d_status,
                                  ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
     return VV_OK;

@@ -154,6 +154,10 @@ private:
     uint4* h_def_jobs_ = nullptr;
     vv_node_patch* h_def_patches_ = nullptr;
     uint32_t* h_def_counts_ = nullptr;   // [0] jobs, [1] patches
+    // their device copies, pulled at the start of each enqueue
+    uint4* d_def_jobs_ = nullptr;
+    vv_node_patch* d_def_patches_ = nullptr;
+    uint32_t* d_def_counts_ = nullptr;
     uint32_t def_job_cap_ = 0, def_patch_cap_ = 0;
     std::vector<int32_t> slot_job_;      // latest pending upload per slot (-1 between uses)
     std::vector<uint32_t> keep_;         // pending uploads kept by a flush
