@@ -340,7 +340,7 @@ def run_ours(args):
     # roofline of the ray cast: algorithmic bytes of the check frame (same
     # path, same pools) over the mean launch duration of the timed region
     nodes, bricks = ctx.footprint(u_last)
-    alg_bytes = 8 * nodes + 4000 * bricks + WIDTH * HEIGHT * (16 + 48)
+    alg_bytes = 8 * nodes + (4000 + 128) * bricks + WIDTH * HEIGHT * (16 + 48)  # + each slot's cell mask
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (float(np.mean(ray_ms)) / 1e3) / 1e9
     traffic = ncu_traffic()
@@ -363,7 +363,7 @@ def run_ours(args):
                      "kernel": "raycast_kernel<RGBA8>",
                      "algorithmic_bytes": {"per_launch": int(alg_bytes), "nodes_touched": int(nodes),
                                            "bricks_touched": int(bricks),
-                                           "formula": "8*nodes + 4000*bricks + W*H*(16 colour + 48 usage)",
+                                           "formula": "8*nodes + (4000 texels + 128 cell mask)*bricks + W*H*(16 colour + 48 usage)",
                                            "measured_on": "check frame after the timed region",
                                            "check_frame_raycast_ms": round(chk_ray_ms, 3)},
                      "traffic_source": (traffic or {}).get("source")},

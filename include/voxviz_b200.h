@@ -210,8 +210,23 @@ int vv_gradpool_download(vv_ctx* ctx, void* texels);
 int vv_brickpool_download(vv_ctx* ctx, void* texels);
 /* Slots per axis and format of the brick pool (0 slots if none exists). */
 int vv_brickpool_info(const vv_ctx* ctx, int32_t slots[3], int32_t* fmt);
-/* Device address of the pool texels (for callers that manage data on device). */
+/* Device address of the pool texels (for callers that manage data on device).
+ * After writing pool texels through it, call vv_brickpool_update_cell_masks. */
 int vv_brickpool_device_ptr(vv_ctx* ctx, void** ptr, size_t* bytes);
+/* Empty-cell masks (no counterpart in the reference: an acceleration of the
+ * ray cast that leaves every result unchanged).  Per slot, bit
+ * (z*9 + y)*9 + x of 32 uint32 words is set when the eight texels of the
+ * 2x2x2 cell whose first texel is (x,y,z), x,y,z in [0,8], are zero in every
+ * bit; a sample whose taps are such a cell is exactly zero, so the ray cast
+ * takes the zero without reading texels.  The library keeps the masks for
+ * pools it writes (creation, vv_upload_bricks*, the renderer's production);
+ * vv_brickpool_attach leaves them invalid (no skipping) until
+ * vv_brickpool_update_cell_masks rebuilds them from the pool's contents,
+ * which is also the call to make after writing texels through
+ * vv_brickpool_device_ptr or an attached buffer.  Download: slots*32 words,
+ * VV_ERR_STATE while the masks are invalid. */
+int vv_brickpool_update_cell_masks(vv_ctx* ctx);
+int vv_brickpool_download_cell_masks(vv_ctx* ctx, uint32_t* words);
 
 /* The 2D jitter texture (GLUtils::Create2DJitterTexture, GLUtils.cpp:455-497):
  * size*size uint8 values in [1,255], row-major. */

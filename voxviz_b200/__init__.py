@@ -278,6 +278,19 @@ class Context:
         self._ck(lib().vv_brickpool_download(self._h, _ptr(out)), "brick download")
         return out
 
+    def update_cell_masks(self) -> None:
+        """Rebuild the pool's empty-cell masks from its contents (after writing
+        texels through an attached buffer or the device pointer)."""
+        self._ck(lib().vv_brickpool_update_cell_masks(self._h), "cell masks")
+
+    def download_cell_masks(self) -> np.ndarray:
+        """(slots, 32) uint32: bit (z*9+y)*9+x set when the 2x2x2 texel cell at
+        (x,y,z) is zero in every bit."""
+        sx, sy, sz = self.slots
+        out = np.zeros((sx * sy * sz, 32), dtype=np.uint32)
+        self._ck(lib().vv_brickpool_download_cell_masks(self._h, _ptr(out)), "cell mask download")
+        return out
+
     def create_gradpool(self, fmt="fp32") -> None:
         """Gradient pool with the brick pool's slots (lighting)."""
         self._ck(lib().vv_gradpool_create(self._h, fmt_code(fmt)), "gradient pool")

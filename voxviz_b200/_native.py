@@ -199,6 +199,8 @@ SIGNATURES = {
     "vv_gradpool_download": (C.c_int, [P, P]),
     "vv_octree_produce_gradients": (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
     "vv_brickpool_download": (C.c_int, [P, P]),
+    "vv_brickpool_update_cell_masks": (C.c_int, [P]),
+    "vv_brickpool_download_cell_masks": (C.c_int, [P, P]),
     "vv_brickpool_info": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "vv_nodepool_info": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int32)]),
     "vv_brickpool_device_ptr": (C.c_int, [P, C.POINTER(P), C.POINTER(C.c_size_t)]),

@@ -184,6 +184,7 @@ static int batch_launch(vv_ctx* c, const vv_batch_view* views, int32_t n, const 
             v.p.slots[a] = bv.ctx->slots[a];
         }
         v.p.bricks = bv.ctx->bricks;
+        v.p.cell_mask = ctx_cell_mask(bv.ctx);
         v.p.jitter = bv.ctx->d_jitter;
         v.p.color = (float4*)bv.color;
         v.p.usage = (uint4*)bv.usage;

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "cellmask.cuh"
 #include "kernels.cuh"
 
 using namespace vv;
@@ -86,7 +87,42 @@ int ctx_ensure(vv_ctx* c, void** ptr, size_t* cap, size_t bytes, const char* wha
     return ensure(c, ptr, cap, bytes, what);
 }
 int ctx_ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes) { return ensure_host(c, ptr, cap, bytes); }
+const uint32_t* ctx_cell_mask(const vv_ctx* c) { return c->cell_mask_valid ? c->cell_mask : nullptr; }
+uint32_t* ctx_cell_mask_rw(vv_ctx* c) { return c->cell_mask_valid ? c->cell_mask : nullptr; }
 }  // namespace vv
+
+namespace {
+
+// Cell masks sized for the pool's current slots (contents not yet valid).
+int alloc_cell_masks(vv_ctx* c) {
+    c->cell_mask_valid = false;
+    if (c->cell_mask && c->cell_mask_slots == c->total_slots) return VV_OK;
+    if (c->cell_mask) {
+        VV_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->cell_mask);
+        c->cell_mask = nullptr;
+        c->cell_mask_slots = 0;
+    }
+    const size_t bytes = (size_t)c->total_slots * vv::kCellMaskWords * sizeof(uint32_t);
+    if (cudaMalloc((void**)&c->cell_mask, bytes) != cudaSuccess) {
+        c->cell_mask = nullptr;
+        return fail(c, VV_ERR_OOM, "cudaMalloc cell masks");
+    }
+    c->cell_mask_slots = c->total_slots;
+    return VV_OK;
+}
+
+// Every slot's mask from the pool's current contents.
+int rebuild_cell_masks(vv_ctx* c) {
+    int rc = alloc_cell_masks(c);
+    if (rc) return rc;
+    VV_CUDA(c, vv::launch_cell_masks(nullptr, c->total_slots, c->bricks, c->fmt, c->total_slots, c->cell_mask,
+                                     c->stream));
+    c->cell_mask_valid = true;
+    return VV_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -145,7 +181,8 @@ int vv_ctx_destroy(vv_ctx* c) {
         if (t.nodes) cudaFree(t.nodes);
     if (c->bricks && !c->bricks_external) cudaFree(c->bricks);
     void* bufs[] = {c->d_status, c->d_jitter, c->d_usage, c->d_mask, c->d_counts, c->d_offsets,
-                    c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words, c->d_batch, c->grads};
+                    c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words, c->d_batch, c->grads,
+                    c->cell_mask};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -277,6 +314,23 @@ int vv_brickpool_create(vv_ctx* c, int32_t sx, int32_t sy, int32_t sz, int32_t f
     c->fmt = fmt;
     c->brick_bytes = VV_BRICK_TEXELS * tb;
     c->pool_bytes = bytes;
+    return rebuild_cell_masks(c);  // of the zeroed pool
+}
+
+int vv_brickpool_update_cell_masks(vv_ctx* c) {
+    if (!c) return VV_ERR_ARG;
+    if (!c->bricks) return fail(c, VV_ERR_STATE, "brick pool not created");
+    cudaSetDevice(c->device);
+    return rebuild_cell_masks(c);
+}
+
+int vv_brickpool_download_cell_masks(vv_ctx* c, uint32_t* words) {
+    if (!c || !words) return VV_ERR_ARG;
+    if (!c->bricks || !c->cell_mask_valid) return fail(c, VV_ERR_STATE, "cell masks not valid");
+    cudaSetDevice(c->device);
+    VV_CUDA(c, cudaMemcpyAsync(words, c->cell_mask, (size_t)c->total_slots * kCellMaskWords * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, c->stream));
+    VV_CUDA(c, cudaStreamSynchronize(c->stream));
     return VV_OK;
 }
 
@@ -286,6 +340,8 @@ int vv_upload_bricks_device(vv_ctx* c, const uint32_t* slots_dev, int32_t n, con
     cudaSetDevice(c->device);
     VV_CUDA(c, launch_brick_scatter(slots_dev, n, texels_dev, c->bricks, c->brick_bytes, c->total_slots,
                                     c->d_status, c->stream));
+    if (c->cell_mask_valid)
+        VV_CUDA(c, launch_cell_masks(slots_dev, n, c->bricks, c->fmt, c->total_slots, c->cell_mask, c->stream));
     return VV_OK;
 }
 
@@ -303,6 +359,8 @@ int vv_upload_bricks(vv_ctx* c, const uint32_t* slots, int32_t n, const void* te
     VV_CUDA(c, cudaMemcpyAsync(c->d_up_slots, slots, sb, cudaMemcpyHostToDevice, c->stream));
     VV_CUDA(c, launch_brick_scatter(c->d_up_slots, n, c->d_up_bricks, c->bricks, c->brick_bytes, c->total_slots,
                                     c->d_status, c->stream));
+    if (c->cell_mask_valid)
+        VV_CUDA(c, launch_cell_masks(c->d_up_slots, n, c->bricks, c->fmt, c->total_slots, c->cell_mask, c->stream));
     // The caller's host buffers may be pageable and reused right after return.
     VV_CUDA(c, cudaStreamSynchronize(c->stream));
     return VV_OK;
@@ -391,7 +449,9 @@ int vv_brickpool_attach(vv_ctx* c, void* texels, int32_t sx, int32_t sy, int32_t
     c->fmt = fmt;
     c->brick_bytes = VV_BRICK_TEXELS * tb;
     c->pool_bytes = (size_t)c->total_slots * VV_BRICK_TEXELS * tb;
-    return VV_OK;
+    // the caller writes this memory: no empty-cell skipping until
+    // vv_brickpool_update_cell_masks
+    return alloc_cell_masks(c);
 }
 
 size_t vv_ckpt_bytes(int32_t width, int32_t height, int32_t per_ray) {
@@ -418,6 +478,7 @@ static int diff_params(vv_ctx* c, int32_t tree, const vv_uniforms* u, RaycastPar
         p.slots[a] = c->slots[a];
     }
     p.bricks = c->bricks;
+    p.cell_mask = ctx_cell_mask(c);
     p.jitter = c->d_jitter;
     p.status = c->d_status;
     p.max_iter = vv_max_iterations(u);
@@ -514,6 +575,7 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         p.node_dim[1] = t.dim[1];
         p.node_dim[2] = t.dim[2];
         p.bricks = c->bricks;
+        p.cell_mask = ctx_cell_mask(c);
         p.slots[0] = c->slots[0];
         p.slots[1] = c->slots[1];
         p.slots[2] = c->slots[2];

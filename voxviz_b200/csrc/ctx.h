@@ -22,6 +22,9 @@ int vv_max_iterations(const vv_uniforms* u);
 int ctx_fail(vv_ctx* c, int code, const std::string& msg);
 int ctx_ensure(vv_ctx* c, void** ptr, size_t* cap, size_t bytes, const char* what);
 int ctx_ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes);
+// The pool's empty-cell masks when valid, else nullptr (no skipping).
+const uint32_t* ctx_cell_mask(const vv_ctx* c);
+uint32_t* ctx_cell_mask_rw(vv_ctx* c);
 
 }  // namespace vv
 
@@ -39,6 +42,11 @@ struct vv_ctx {
     int fmt = VV_FMT_RGBA8;
     size_t brick_bytes = 0;
     size_t pool_bytes = 0;
+    // empty-cell masks of the brick pool (cellmask.cuh), 32 words per slot;
+    // valid while every write to the pool went through this library
+    uint32_t* cell_mask = nullptr;
+    long long cell_mask_slots = 0;
+    bool cell_mask_valid = false;
     // gradient pool (lighting): same slots as the brick pool
     void* grads = nullptr;
     int grad_fmt = VV_FMT_FP32;

@@ -353,6 +353,33 @@ __global__ void brick_scatter_kernel(const uint32_t* __restrict__ slots, const u
     for (int i = threadIdx.x; i < vec_per_brick; i += blockDim.x) d[i] = __ldg(s + i);
 }
 
+template <int FMT>
+__global__ void cell_mask_kernel(const uint32_t* __restrict__ slots, const void* __restrict__ pool,
+                                 long long total_slots, uint32_t* __restrict__ masks) {
+    __shared__ uint8_t zero[VV_BRICK_TEXELS];
+    const long long slot = slots ? (long long)slots[blockIdx.x] : (long long)blockIdx.x;
+    if (slot >= total_slots) return;  // whole CTA (a bad slot was reported by the upload)
+    for (int q = threadIdx.x; q < VV_BRICK_TEXELS; q += blockDim.x)
+        zero[q] = texel_is_zero<FMT>(pool, (size_t)slot * VV_BRICK_TEXELS + q) ? 1 : 0;
+    __syncthreads();
+    write_cell_mask(zero, masks + (size_t)slot * kCellMaskWords);
+}
+
+cudaError_t launch_cell_masks(const uint32_t* slots, long long n, const void* pool, int fmt, long long total_slots,
+                              uint32_t* masks, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    if (n > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
+    const unsigned grid = (unsigned)n;
+    switch (fmt) {
+        case VV_FMT_RGBA8: cell_mask_kernel<VV_FMT_RGBA8><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
+        case VV_FMT_FP16: cell_mask_kernel<VV_FMT_FP16><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
+        case VV_FMT_BF16: cell_mask_kernel<VV_FMT_BF16><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
+        case VV_FMT_FP32: cell_mask_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_brick_scatter(const uint32_t* slots, int n, const void* src, void* pool, size_t brick_bytes,
                                  long long total_slots, int* status, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;

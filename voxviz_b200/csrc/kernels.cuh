@@ -24,6 +24,7 @@ struct RaycastParams {
     int max_iter;            // bound on outer-loop iterations per ray
     uint32_t* node_touch;    // footprint mode: bit per node (block-linear index)
     uint32_t* brick_touch;   // footprint mode: bit per brick-pool slot
+    const uint32_t* cell_mask;  // empty-cell masks of the pool (cellmask.cuh), or nullptr
 };
 
 // Pyramid/compaction launch state.
@@ -70,5 +71,9 @@ cudaError_t launch_node_patch(const vv_node_patch* patches, int n, uint2* nodes,
 cudaError_t launch_brick_scatter(const uint32_t* slots, int n, const void* src, void* pool,
                                  size_t brick_bytes, long long total_slots, int* status,
                                  cudaStream_t s);
+// Empty-cell masks (cellmask.cuh) of n slots (slots[i], or slot i when slots
+// is null) from the pool's current contents: 32 words per slot.
+cudaError_t launch_cell_masks(const uint32_t* slots, long long n, const void* pool, int fmt, long long total_slots,
+                              uint32_t* masks, cudaStream_t s);
 
 }  // namespace vv

@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "../../include/voxviz_b200.h"
+#include "cellmask.cuh"
 #include "production.h"
 #include "terrain.h"
 
@@ -82,7 +83,8 @@ __device__ __forceinline__ void store_texel(void* pool, size_t i, uint32_t v) {
 // (L-d) voxel (8i-1+bx, 8j-1+by, 8k-1+bz), transparent black outside the level.
 template <int FMT>
 __device__ __forceinline__ void produce_one(const DeviceTerrainView& t, const uint4 job, void* __restrict__ pool,
-                                            long long total_slots, int* status) {
+                                            uint32_t* __restrict__ masks, long long total_slots, int* status) {
+    __shared__ uint8_t zero[VV_BRICK_TEXELS];  // texel all-zero flags for the slot's cell mask
     if ((long long)job.x >= total_slots || (int)job.y > t.depth) {
         if (threadIdx.x == 0 && status) atomicCAS(status, 0, VV_ERR_BOUNDS);
         return;
@@ -106,13 +108,20 @@ __device__ __forceinline__ void produce_one(const DeviceTerrainView& t, const ui
             }
         }
         store_texel<FMT>(pool, base + (size_t)q, v);
+        zero[q] = v == 0u ? 1 : 0;  // RGBA8 zero stores as zero in every format
+    }
+    if (masks) {  // the same for the whole CTA
+        __syncthreads();
+        write_cell_mask(zero, masks + (size_t)job.x * kCellMaskWords);
+        __syncthreads();  // zero[] serves the CTA's next job
     }
 }
 
 template <int FMT>
 __global__ void produce_kernel(const __grid_constant__ DeviceTerrainView t, const uint4* __restrict__ jobs,
-                               void* __restrict__ pool, long long total_slots, int* status) {
-    produce_one<FMT>(t, jobs[blockIdx.x], pool, total_slots, status);
+                               void* __restrict__ pool, uint32_t* __restrict__ masks, long long total_slots,
+                               int* status) {
+    produce_one<FMT>(t, jobs[blockIdx.x], pool, masks, total_slots, status);
 }
 
 // Staged form: the job count is read on the device, so the launch itself
@@ -122,7 +131,7 @@ __global__ void produce_kernel(const __grid_constant__ DeviceTerrainView t, cons
 template <int FMT>
 __global__ void produce_staged_kernel(const __grid_constant__ DeviceTerrainView t, const uint4* jobs,
                                       const volatile uint32_t* count, uint32_t max_jobs, void* __restrict__ pool,
-                                      long long total_slots, int* status) {
+                                      uint32_t* __restrict__ masks, long long total_slots, int* status) {
     __shared__ uint32_t s_n;  // one read of the count per CTA
     if (threadIdx.x == 0) s_n = min(*count, max_jobs);
     __syncthreads();
@@ -131,7 +140,7 @@ __global__ void produce_staged_kernel(const __grid_constant__ DeviceTerrainView 
     for (uint32_t j = blockIdx.x; j < n; j += gridDim.x) {
         if (threadIdx.x == 0) s_job = jobs[j];
         __syncthreads();
-        produce_one<FMT>(t, s_job, pool, total_slots, status);
+        produce_one<FMT>(t, s_job, pool, masks, total_slots, status);
         __syncthreads();
     }
 }
@@ -530,21 +539,21 @@ cudaError_t launch_order_partition(SlotOrderBuffers& b, uint32_t head, uint32_t 
 }
 
 cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs, int n, void* pool, int fmt,
-                                  long long total_slots, int* status, cudaStream_t s) {
+                                  uint32_t* masks, long long total_slots, int* status, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     switch (fmt) {
-        case VV_FMT_RGBA8: produce_kernel<VV_FMT_RGBA8><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
-        case VV_FMT_FP16: produce_kernel<VV_FMT_FP16><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
-        case VV_FMT_BF16: produce_kernel<VV_FMT_BF16><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
-        case VV_FMT_FP32: produce_kernel<VV_FMT_FP32><<<n, 256, 0, s>>>(t, jobs, pool, total_slots, status); break;
+        case VV_FMT_RGBA8: produce_kernel<VV_FMT_RGBA8><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_FP16: produce_kernel<VV_FMT_FP16><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_BF16: produce_kernel<VV_FMT_BF16><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_FP32: produce_kernel<VV_FMT_FP32><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs, const uint32_t* count,
-                                  uint32_t max_jobs, void* pool, int fmt, long long total_slots, int* status,
-                                  cudaStream_t s) {
+                                  uint32_t max_jobs, void* pool, int fmt, uint32_t* masks, long long total_slots,
+                                  int* status, cudaStream_t s) {
     if (max_jobs == 0) return cudaSuccess;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -552,16 +561,16 @@ cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs,
     const unsigned grid = (unsigned)std::min<long long>((long long)max_jobs, (long long)std::max(sms, 1) * 8);
     switch (fmt) {
         case VV_FMT_RGBA8:
-            produce_staged_kernel<VV_FMT_RGBA8><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            produce_staged_kernel<VV_FMT_RGBA8><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, masks, total_slots, status);
             break;
         case VV_FMT_FP16:
-            produce_staged_kernel<VV_FMT_FP16><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            produce_staged_kernel<VV_FMT_FP16><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, masks, total_slots, status);
             break;
         case VV_FMT_BF16:
-            produce_staged_kernel<VV_FMT_BF16><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            produce_staged_kernel<VV_FMT_BF16><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, masks, total_slots, status);
             break;
         case VV_FMT_FP32:
-            produce_staged_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, total_slots, status);
+            produce_staged_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, masks, total_slots, status);
             break;
         default: return cudaErrorInvalidValue;
     }

@@ -49,15 +49,17 @@ private:
 
 // jobs[i] = {slot, node level, i<<20 | j<<10 | k, 0}: produce the stored
 // brick of node (level, i, j, k) into brick-pool slot `slot`.
+// masks: the pool's empty-cell masks (32 words per slot), written for each
+// produced slot, or nullptr.
 cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs, int n, void* pool, int fmt,
-                                  long long total_slots, int* status, cudaStream_t s);
+                                  uint32_t* masks, long long total_slots, int* status, cudaStream_t s);
 
 // The same with the job count read on the device (at most max_jobs): a
 // count-independent launch for CUDA graphs.  Jobs and count should be in
 // device memory (launch_pull_staged puts them there).
 cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs, const uint32_t* count,
-                                  uint32_t max_jobs, void* pool, int fmt, long long total_slots, int* status,
-                                  cudaStream_t s);
+                                  uint32_t max_jobs, void* pool, int fmt, uint32_t* masks, long long total_slots,
+                                  int* status, cudaStream_t s);
 
 struct DedupeBuffers {
     uint32_t* first = nullptr;       // per node-pool grid cell, all 0xFFFFFFFF between calls

@@ -12,6 +12,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include "cellmask.cuh"
 #include "kernels.cuh"
 #include "lod_bound.h"
 
@@ -167,11 +168,14 @@ __device__ __forceinline__ float4 sample_brick(const RaycastParams& p, F3 uvw) {
 }
 
 // Trilinear sample when all 8 taps lie in the brick-pool slot whose first
-// texel per axis is base[]; returns false (and nothing) otherwise.  Same
-// arithmetic as sample_brick: only the texel addressing is shorter.
+// texel per axis is base[]: kInSlot (out = the sample, same arithmetic as
+// sample_brick, only the texel addressing is shorter) or, when the slot's
+// cell mask `cmask` (or nullptr) marks the taps' cell all zero, kEmptyCell
+// (out = 0, exactly what the taps give); kOutside (and nothing) otherwise.
+enum { kOutside = 0, kInSlot = 1, kEmptyCell = 2 };
 template <int FMT>
-__device__ __forceinline__ bool sample_in_slot(const RaycastParams& p, F3 uvw, const int base[3], uint32_t slot_texel0,
-                                               float4& out) {
+__device__ __forceinline__ int sample_in_slot(const RaycastParams& p, F3 uvw, const int base[3], uint32_t slot_texel0,
+                                              const uint32_t* cmask, float4& out) {
     const float* N = p.u.brick_pool_dimension;
     const float ta[3] = {uvw.x * N[0] - 0.5f, uvw.y * N[1] - 0.5f, uvw.z * N[2] - 0.5f};
     float f[3];
@@ -182,7 +186,14 @@ __device__ __forceinline__ bool sample_in_slot(const RaycastParams& p, F3 uvw, c
         f[a] = ta[a] - fi;
         l[a] = (int)fi - base[a];
     }
-    if ((unsigned)l[0] > 8u || (unsigned)l[1] > 8u || (unsigned)l[2] > 8u) return false;
+    if ((unsigned)l[0] > 8u || (unsigned)l[1] > 8u || (unsigned)l[2] > 8u) return kOutside;
+    if (cmask) {
+        const uint32_t c = (uint32_t)((l[2] * kCellsPerAxis + l[1]) * kCellsPerAxis + l[0]);
+        if ((__ldg(cmask + (c >> 5)) >> (c & 31u)) & 1u) {
+            out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            return kEmptyCell;
+        }
+    }
     const uint32_t i000 = slot_texel0 + (uint32_t)((l[2] * 10 + l[1]) * 10 + l[0]);
     const void* pool = p.bricks;
     const float4 v000 = Texel<FMT>::load(pool, i000), v100 = Texel<FMT>::load(pool, i000 + 1u);
@@ -197,7 +208,7 @@ __device__ __forceinline__ bool sample_in_slot(const RaycastParams& p, F3 uvw, c
         c = make_float4(c.x * k, c.y * k, c.z * k, c.w * k);
     }
     out = c;
-    return true;
+    return kInSlot;
 }
 
 
@@ -612,11 +623,14 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             int base[3] = {(int)((cur_bw >> 20) & 0x3FFu) - 1, (int)((cur_bw >> 10) & 0x3FFu) - 1,
                            (int)(cur_bw & 0x3FFu) - 1};
             uint32_t slot_texel0 = 0u;
+            const uint32_t* cmask = nullptr;  // the slot's empty-cell mask (not in footprint counts)
             if (base[0] >= 0 && base[1] >= 0 && base[2] >= 0 && base[0] % 10 == 0 && base[1] % 10 == 0 &&
                 base[2] % 10 == 0 && base[0] < p.slots[0] * 10 && base[1] < p.slots[1] * 10 &&
                 base[2] < p.slots[2] * 10) {
-                slot_texel0 = (((uint32_t)base[2] / 10u * (uint32_t)p.slots[1] + (uint32_t)base[1] / 10u) *
-                                   (uint32_t)p.slots[0] + (uint32_t)base[0] / 10u) * 1000u;
+                const uint32_t slot = ((uint32_t)base[2] / 10u * (uint32_t)p.slots[1] + (uint32_t)base[1] / 10u) *
+                                          (uint32_t)p.slots[0] + (uint32_t)base[0] / 10u;
+                slot_texel0 = slot * 1000u;
+                if (!COUNT && p.cell_mask) cmask = p.cell_mask + (size_t)slot * kCellMaskWords;
             } else {
                 base[0] = base[1] = base[2] = -100000;
             }
@@ -629,9 +643,11 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                     break;
                 }
                 float4 src;
-                if (COUNT || !sample_in_slot<FMT>(p, bpos, base, slot_texel0, src)) src = sample_brick<FMT, COUNT>(p, bpos);
+                const int in = COUNT ? kOutside : sample_in_slot<FMT>(p, bpos, base, slot_texel0, cmask, src);
+                if (in == kOutside) src = sample_brick<FMT, COUNT>(p, bpos);
                 src.w = 1.0f - (1.0f - src.w);
-                if (LIT) light_sample(p, bpos, s.dir, light_dir, src);
+                // shading adds rgb times finite factors: nothing to a zero sample
+                if (LIT && in != kEmptyCell) light_sample(p, bpos, s.dir, light_dir, src);
                 const float T = 1.0f - s.dst.w;
                 const bool go = vis.sample(kSampleBrick, src, bpos, T, s.nsamples);
                 s.dst = make_float4(T * src.x + s.dst.x, T * src.y + s.dst.y, T * src.z + s.dst.z, T * src.w + s.dst.w);

@@ -605,7 +605,8 @@ int GigaVoxelsRenderer::flush_device() {
     if (launch_pull(dh_fjobs_, d_fjobs_, n, (const uint4*)dh_fpatch_, (uint4*)d_fpatch_, patch_words,
                     ctx_->stream) != cudaSuccess ||
         cudaEventRecord(ev_flush_, ctx_->stream) != cudaSuccess ||
-        launch_produce_bricks(dterrain_->view(), d_fjobs_, (int)n, pool, d_.fmt, (long long)total_slots_,
+        launch_produce_bricks(dterrain_->view(), d_fjobs_, (int)n, pool, d_.fmt, ctx_cell_mask_rw(ctx_),
+                              (long long)total_slots_,
                               ctx_->d_status, ctx_->stream) != cudaSuccess ||
         launch_node_patch(d_fpatch_, (int)np, t.nodes, t.dim, ctx_->d_status, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
@@ -930,7 +931,7 @@ int GigaVoxelsRenderer::enqueue_uploads() {
                            d_def_patches_, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
     if (launch_produce_staged(dterrain_->view(), d_def_jobs_, d_def_counts_, def_job_cap_, pool, d_.fmt,
-                              (long long)total_slots_, ctx_->d_status, ctx_->stream) != cudaSuccess)
+                              ctx_cell_mask_rw(ctx_), (long long)total_slots_, ctx_->d_status, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
     const DeviceTree& t = ctx_->trees[0];
     if (launch_node_patch_staged(d_def_patches_, d_def_counts_ + 1, def_patch_cap_, t.nodes, t.dim, ctx_->d_status,
