@@ -84,10 +84,11 @@ VV_HD uint32_t float_bits(float f) {
     return b;
 #endif
 }
-// x * 2^e for a normal power-of-two scale (exact)
+// x * 2^e for a normal power-of-two scale (exact); on the device 2^e is built
+// from its exponent bits (e in [-126, 127])
 VV_HD float scale2(float x, int e) {
 #ifdef __CUDA_ARCH__
-    return ldexpf(x, e);
+    return x * __int_as_float((e + 127) << 23);
 #else
     return std::ldexp(x, e);
 #endif
@@ -132,7 +133,9 @@ VV_HD void clear_range(const Consts& k, V3 pos, int& lo, int& hi) {
     const float A = dot(a, a);
     if (!(A > 1e-12f)) return;
     const float ra = fast_rsqrt(A);
-    const float alen_lo = 1.0f / (ra * 1.0001f);
+    // a lower bound on |a| (the 1e-4 covers the approximate reciprocal square
+    // root and division, <= 2 ulp each on the device)
+    const float alen_lo = fast_div(1.0f, ra * 1.0001f);
     // j0: the smallest j with 2^j >= t = 4 rvh |w| / |a|
     const float t = 4.0f * k.rvh * k.wn * ra * 1.001f;
     int j0 = 0;
@@ -154,11 +157,12 @@ VV_HD void clear_range(const Consts& k, V3 pos, int& lo, int& hi) {
     int lo_level = j0;
     if (j0 > 0) {
         const float eps_c = u * (3.0f + 8.0f * k.rvh + amax + 2.0f * k.cmax) * 1.01f;
-        const float dsh = 2.0f * (1.01f * 1.7321f * eps_c / (0.316f * alen_lo) + 1.8f * u);
+        // upper bounds below: approximate quotients are raised by 1e-6 (> 2 ulp)
+        const float dsh = 2.0f * (fast_div(1.01f * 1.7321f * eps_c, 0.316f * alen_lo) * 1.000001f + 1.8f * u);
         if ((0.0051f - dsh - 13.2f * u) * k.lod * (1.0f - 2.0f * u) >= k.pixel_size * (1.0f + 1e-4f)) lo_level = 0;
     }
-    const float eps = 1.7321f * u * (2.0f + amax + 1.25f * alen_lo / k.wn + 2.0f * k.cmax) * 1.01f;
-    const float dmax = 2.0f * (1.34f * eps / alen_lo + 1.8f * u) * 1.01f;
+    const float eps = 1.7321f * u * (2.0f + amax + fast_div(1.25f * alen_lo, k.wn) * 1.000001f + 2.0f * k.cmax) * 1.01f;
+    const float dmax = 2.0f * (fast_div(1.34f * eps, alen_lo) * 1.000001f + 1.8f * u) * 1.01f;
     if (lo_level == 0) {  // whatever the deeper levels give, [0, j0) is shown
         lo = 0;
         hi = j0 - 1;
@@ -173,7 +177,7 @@ VV_HD void clear_range(const Consts& k, V3 pos, int& lo, int& hi) {
         const float vh2 = vh * vh;
         const float den = A + vh2 * k.W;
         const float Rlow = fast_div(2.0f * vh2 * S, den * den) * (1.0f - 1e-4f);
-        const float theta_up = 2.7f * vh * k.wn / alen_lo;
+        const float theta_up = fast_div(2.7f * vh * k.wn, alen_lo) * 1.000001f;
         const float x = 2.0f * Rlow;
         const float theta_lo = x * fast_rsqrt(x) * (1.0f - 1e-4f);
         if (!(theta_lo >= 5.0f * dmax)) continue;

@@ -44,6 +44,11 @@ __device__ __forceinline__ void set_status(int* status, int code) {
     if (status) atomicCAS(status, 0, code);
 }
 
+// 2^e for e in [-126, 127], exactly: the normal power of two built from its
+// exponent bits (ldexpf covers every case and costs more instructions).  Every
+// use below scales by a tree level, well inside that range.
+__device__ __forceinline__ float pow2i(int e) { return __int_as_float((e + 127) << 23); }
+
 // pow(x, 2^k) as k squarings (the sample-ratio powers of the shader).
 __device__ __forceinline__ float pow_pow2(float x, int k) {
     for (int i = 0; i < k; ++i) x = x * x;
@@ -476,7 +481,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
         bool is_const, loaded;
         if (RESUME && !COUNT && k.unit_box && prev_depth > 0 && prev_depth < kPathLevels && skip_lo == 0) {
             // the deepest level whose node holds both this and the last position
-            const float sc = ldexpf(1.0f, prev_depth);
+            const float sc = pow2i(prev_depth);
             const uint32_t nx = (uint32_t)(s.pos.x * sc), ny = (uint32_t)(s.pos.y * sc),
                            nz = (uint32_t)(s.pos.z * sc);
             const uint32_t diff = (nx ^ (prev_cell >> 20)) | (ny ^ ((prev_cell >> 10) & 0x3FFu)) |
@@ -490,9 +495,9 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                 s.nptr_y = (pp >> 10) & 0x3FFu;
                 s.nptr_z = pp & 0x3FFu;
                 depth = r;
-                vhalf = ldexpf(k.rvh, -r);
+                vhalf = k.rvh * pow2i(-r);
                 // cell and position in the cell at level r: exact (power-of-two scaling)
-                const float sr = ldexpf(1.0f, r);
+                const float sr = pow2i(r);
                 const F3 pr = f3(s.pos.x * sr, s.pos.y * sr, s.pos.z * sr);
                 ccx = (uint32_t)pr.x;
                 ccy = (uint32_t)pr.y;
@@ -505,7 +510,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                     if (wl.x & kResident) {
                         cur_bw = wl.y;
                         brick_depth = l;
-                        const float sl = ldexpf(1.0f, l);
+                        const float sl = pow2i(l);
                         const F3 pl = f3(s.pos.x * sl, s.pos.y * sl, s.pos.z * sl);
                         cur_brp = f3(pl.x - floorf(pl.x), pl.y - floorf(pl.y), pl.z - floorf(pl.z));
                         break;
@@ -569,7 +574,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             }
         }
         if (k.unit_box) {
-            const float sc = ldexpf(1.0f, -depth);
+            const float sc = pow2i(-depth);
             ext_min = f3((float)ccx * sc, (float)ccy * sc, (float)ccz * sc);
             ext_max = f3((float)(ccx + 1u) * sc, (float)(ccy + 1u) * sc, (float)(ccz + 1u) * sc);
             if (RESUME) {
@@ -579,7 +584,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
         }
         // ---- the leaf segment
         if (is_const) {
-            const float ratio = ldexpf(1.0f, k.L - depth);
+            const float ratio = pow2i(k.L - depth);
             const float step = k.RS * ratio;
             const float aw = (float)(node.y >> 24) / 255.0f;
             const float t = min_exit(s.pos, s.dir, ext_min, ext_max);
@@ -614,7 +619,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             const F3 bptr = f3((float)((cur_bw >> 20) & 0x3FFu) / k.pdim.x, (float)((cur_bw >> 10) & 0x3FFu) / k.pdim.y,
                                (float)(cur_bw & 0x3FFu) / k.pdim.z);
             F3 bpos = add(bptr, divv(mul(cur_brp, k.bdim), k.pdim));
-            const float ratio = ldexpf(1.0f, k.L - brick_depth);
+            const float ratio = pow2i(k.L - brick_depth);
             const F3 wstep = muls(muls(s.dir, k.RS), ratio);
             const float t = min_exit(s.pos, s.dir, ext_min, ext_max);
             const float step = k.RS * ratio;
