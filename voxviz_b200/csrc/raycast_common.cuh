@@ -183,14 +183,11 @@ __device__ __forceinline__ int sample_in_slot(const RaycastParams& p, F3 uvw, co
                                               const uint32_t* cmask, float4& out) {
     const float* N = p.u.brick_pool_dimension;
     const float ta[3] = {uvw.x * N[0] - 0.5f, uvw.y * N[1] - 0.5f, uvw.z * N[2] - 0.5f};
-    float f[3];
+    // the first tap per axis, floor(t) as an integer in one conversion (the
+    // weights below are only formed for a sample that is filtered)
     int l[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float fi = floorf(ta[a]);
-        f[a] = ta[a] - fi;
-        l[a] = (int)fi - base[a];
-    }
+    for (int a = 0; a < 3; ++a) l[a] = __float2int_rd(ta[a]) - base[a];
     if ((unsigned)l[0] > 8u || (unsigned)l[1] > 8u || (unsigned)l[2] > 8u) return kOutside;
     if (cmask) {
         const uint32_t c = (uint32_t)((l[2] * kCellsPerAxis + l[1]) * kCellsPerAxis + l[0]);
@@ -199,6 +196,9 @@ __device__ __forceinline__ int sample_in_slot(const RaycastParams& p, F3 uvw, co
             return kEmptyCell;
         }
     }
+    float f[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) f[a] = ta[a] - floorf(ta[a]);
     const uint32_t i000 = slot_texel0 + (uint32_t)((l[2] * 10 + l[1]) * 10 + l[0]);
     const void* pool = p.bricks;
     const float4 v000 = Texel<FMT>::load(pool, i000), v100 = Texel<FMT>::load(pool, i000 + 1u);
@@ -655,7 +655,10 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                 if (LIT && in != kEmptyCell) light_sample(p, bpos, s.dir, light_dir, src);
                 const float T = 1.0f - s.dst.w;
                 const bool go = vis.sample(kSampleBrick, src, bpos, T, s.nsamples);
-                s.dst = make_float4(T * src.x + s.dst.x, T * src.y + s.dst.y, T * src.z + s.dst.z, T * src.w + s.dst.w);
+                // a zero sample leaves dst as it is (T * 0 + dst == dst)
+                if (in != kEmptyCell)
+                    s.dst = make_float4(T * src.x + s.dst.x, T * src.y + s.dst.y, T * src.z + s.dst.z,
+                                        T * src.w + s.dst.w);
                 ++s.nsamples;
                 if (!go) return;
                 bpos = add(bpos, s.brick_step);
