@@ -125,7 +125,7 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-RAYCAST_VERSION = "v4"  # bumped whenever the ray-cast kernel changes; the ncu capture must match
+RAYCAST_VERSION = "v5"  # bumped whenever the ray-cast kernel changes; the ncu capture must match
 
 
 def ncu_traffic():
