@@ -2,10 +2,12 @@
 //
 // A persistent grid (resident CTAs per SM x SM count) pulls pixel tiles of
 // all views from a device work queue (one atomic counter; tiles numbered view
-// by view, row-major inside a view).  The CTA that takes a tile copies its
-// view's RaycastParams (uniforms + the pools of the view's octree) into
-// shared memory when the view changes and runs render_pixel, the vv_render
-// ray cast, on every pixel of the tile.  Tile shape and the march-loop
+// by view, row-major inside a view).  The views' RaycastParams (uniforms +
+// the pools of each view's octree) travel by value in the kernel's parameter
+// space, up to 92 views per launch (larger batches launch in chunks), so a
+// CTA reads its view's parameters from the constant bank as the single-view
+// ray cast does, and runs render_pixel, the vv_render ray cast, on every
+// pixel of the tile.  Tile shape and the march-loop
 // unroll (samples per loop trip) are template parameters; the compiled
 // variants are listed in kVariants and picked per batch by the autotuner.
 //
@@ -29,17 +31,26 @@ struct BatchView {
     int tile_begin;  // index of its first tile in the queue
 };
 
+// The views of one launch.  Kernel parameters may take 32,764 bytes.
+constexpr int kMaxLaunchViews = 92;  // 336 bytes each
+struct BatchParams {
+    int n;            // views
+    int total_tiles;  // tiles of all n views
+    BatchView v[kMaxLaunchViews];
+};
+static_assert(sizeof(BatchParams) <= 32000, "batch views must fit the kernel parameter space");
+
 namespace {
 
 template <int FMT, int TW, int TH, int STEPS>
-// at least 16 warps per SM: at most 128 registers per thread (the kernel
-// takes ~120: the view's parameters live in shared memory and many of them
-// in registers; 640 threads per SM and more spill)
-__global__ void __launch_bounds__(TW * TH, 512 / (TW * TH)) batch_raycast_kernel(const BatchView* __restrict__ views,
-                                                                                 int nviews,
-                                                                 unsigned* __restrict__ counter, int total_tiles) {
+// about 28 warps per SM (896 / tile threads CTAs): at most ~72 registers per
+// thread.  Copying a view's parameters to shared memory instead left ~120
+// registers per thread and spilled heavily above 16 warps per SM.
+__global__ void __launch_bounds__(TW * TH, 896 / (TW * TH))
+    batch_raycast_kernel(const __grid_constant__ BatchParams bp, unsigned* __restrict__ counter) {
     static_assert(TW % 8 == 0 && TH % 4 == 0, "a tile is made of 8x4 warp tiles");
-    __shared__ RaycastParams sp;
+    const BatchView* views = bp.v;
+    const int nviews = bp.n, total_tiles = bp.total_tiles;
     __shared__ int s_tile, s_view, s_tx, s_ty;
     __shared__ uint2 path_w[kPathLevels][TW * TH];
     __shared__ uint32_t path_p[kPathLevels][TW * TH];
@@ -47,7 +58,6 @@ __global__ void __launch_bounds__(TW * TH, 512 / (TW * TH)) batch_raycast_kernel
     // each warp covers an 8x4 block of the tile (coherent descents)
     const int wx = (warp % (TW / 8)) * 8 + (lane & 7);
     const int wy = (warp / (TW / 8)) * 4 + (lane >> 3);
-    int cur = -1;
     for (;;) {
         if (threadIdx.x == 0) {
             const int t = (int)atomicAdd(counter, 1u);
@@ -67,19 +77,12 @@ __global__ void __launch_bounds__(TW * TH, 512 / (TW * TH)) batch_raycast_kernel
         }
         __syncthreads();
         if (s_tile >= total_tiles) return;
-        const int v = s_view;
-        if (v != cur) {
-            const int* src = reinterpret_cast<const int*>(&views[v].p);
-            int* dst = reinterpret_cast<int*>(&sp);
-            for (int i = (int)threadIdx.x; i < (int)(sizeof(RaycastParams) / 4); i += TW * TH) dst[i] = src[i];
-            cur = v;
-        }
-        __syncthreads();
+        const RaycastParams& sp = views[s_view].p;
         const int px = s_tx * TW + wx, py = s_ty * TH + wy;
         if (px < sp.u.width && py < sp.u.height)
             render_pixel<FMT, false, STEPS, true>(sp, px, py,
                                                   PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], TW * TH});
-        // every thread is done with s_* and sp before thread 0 takes the next tile
+        // every thread is done with s_* before thread 0 takes the next tile
         __syncthreads();
     }
 }
@@ -91,7 +94,7 @@ constexpr Variant kVariants[] = {{8, 8, 1},   {8, 8, 2},   {8, 8, 4},   {16, 8, 
                                  {16, 16, 1}, {16, 16, 2}, {16, 16, 4}, {32, 8, 1}, {32, 8, 2}, {32, 8, 4}};
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
-using BatchKernel = void (*)(const BatchView*, int, unsigned*, int);
+using BatchKernel = void (*)(BatchParams, unsigned*);
 
 template <int FMT>
 BatchKernel kernel_for(int tw, int th, int steps) {
@@ -130,8 +133,9 @@ bool stream_capturing(cudaStream_t s) {
 
 }  // namespace
 
-// Shared by vv_render_batch and the autotuner: validate the views, stage
-// the per-view parameters and launch one persistent grid.
+// Shared by vv_render_batch and the autotuner: validate the views, fill the
+// launch parameters and launch one persistent grid per chunk of at most
+// kMaxLaunchViews views.
 static int batch_launch(vv_ctx* c, const vv_batch_view* views, int32_t n, const vv_batch_config* cfg) {
     if (!c || !views || n <= 0 || !cfg) return batch_fail(c, VV_ERR_ARG, "bad batch arguments");
     const int tw = cfg->tile_w, th = cfg->tile_h, steps = cfg->steps;
@@ -147,62 +151,12 @@ static int batch_launch(vv_ctx* c, const vv_batch_view* views, int32_t n, const 
     BatchKernel kern = find_kernel(fmt, tw, th, steps);
     if (!kern) return batch_fail(c, VV_ERR_ARG, "no compiled batch variant for this tile shape / steps");
     cudaSetDevice(c->device);
-    const bool capturing = stream_capturing(c->stream);
-    const size_t bytes = (size_t)n * sizeof(BatchView);
-    if (c->batch_ev_live && !capturing) {
-        // the previous launch's parameter copy must have read the staging
-        VV_CUDA(c, cudaEventSynchronize(c->batch_ev));
-        c->batch_ev_live = false;
-    }
-    int rc = ctx_ensure_host(c, &c->h_batch, &c->h_batch_cap, bytes);
+    // launch parameters are copied when the launch is made: one host block serves every chunk
+    int rc = ctx_ensure_host(c, &c->h_batch, &c->h_batch_cap, sizeof(BatchParams));
     if (rc) return rc;
-    rc = ctx_ensure(c, &c->d_batch, &c->d_batch_cap, bytes + 256, "batch views");
+    const int chunks = (n + kMaxLaunchViews - 1) / kMaxLaunchViews;
+    rc = ctx_ensure(c, &c->d_batch, &c->d_batch_cap, (size_t)chunks * 16, "batch queue counters");
     if (rc) return rc;
-    BatchView* hv = (BatchView*)c->h_batch;
-    long long tiles = 0;
-    for (int i = 0; i < n; ++i) {
-        const vv_batch_view& bv = views[i];
-        const vv_uniforms* u = &bv.u;
-        if (bv.tree < 0 || bv.tree >= VV_MAX_TREES) return batch_fail(c, VV_ERR_ARG, "bad tree index");
-        const DeviceTree& t = bv.ctx->trees[bv.tree];
-        if (!t.nodes) return batch_fail(c, VV_ERR_STATE, "node pool not uploaded");
-        const int W = u->width, H = u->height;
-        if (W <= 0 || H <= 0 || W > 16384 || H > 16384) return batch_fail(c, VV_ERR_ARG, "bad viewport");
-        if (u->jitter_tex_size != bv.ctx->jitter_size)
-            return batch_fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
-        if (!(u->ray_step_size > 0.0f)) return batch_fail(c, VV_ERR_ARG, "ray_step_size must be > 0");
-        if (u->compute_lighting) return batch_fail(c, VV_ERR_ARG, "the batched launch covers the unlit ray cast");
-        for (int a = 0; a < 3; ++a)
-            if (u->brick_pool_dimension[a] != (float)(bv.ctx->slots[a] * 10))
-                return batch_fail(c, VV_ERR_ARG, "brick_pool_dimension does not match the brick pool");
-        BatchView& v = hv[i];
-        std::memset(&v, 0, sizeof(v));
-        v.p.u = *u;
-        v.p.nodes = t.nodes;
-        for (int a = 0; a < 3; ++a) {
-            v.p.node_dim[a] = t.dim[a];
-            v.p.slots[a] = bv.ctx->slots[a];
-        }
-        v.p.bricks = bv.ctx->bricks;
-        v.p.cell_mask = ctx_cell_mask(bv.ctx);
-        v.p.jitter = bv.ctx->d_jitter;
-        v.p.color = (float4*)bv.color;
-        v.p.usage = (uint4*)bv.usage;
-        v.p.status = bv.ctx->d_status;
-        v.p.max_iter = vv_max_iterations(u);
-        v.tiles_x = (W + tw - 1) / tw;
-        v.tile_begin = (int)tiles;
-        tiles += (long long)v.tiles_x * ((H + th - 1) / th);
-        if (tiles > 0x7FFFFFFFLL) return batch_fail(c, VV_ERR_ARG, "batch has too many tiles");
-    }
-    unsigned* counter = (unsigned*)((char*)c->d_batch + ((bytes + 15) & ~(size_t)15));
-    VV_CUDA(c, cudaMemcpyAsync(c->d_batch, c->h_batch, bytes, cudaMemcpyHostToDevice, c->stream));
-    VV_CUDA(c, cudaMemsetAsync(counter, 0, sizeof(unsigned), c->stream));
-    if (!capturing) {
-        if (!c->batch_ev) VV_CUDA(c, cudaEventCreateWithFlags(&c->batch_ev, cudaEventDisableTiming));
-        VV_CUDA(c, cudaEventRecord(c->batch_ev, c->stream));
-        c->batch_ev_live = true;
-    }
     int per_sm = cfg->ctas_per_sm;
     if (per_sm <= 0) {
         VV_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tw * th, 0));
@@ -210,10 +164,54 @@ static int batch_launch(vv_ctx* c, const vv_batch_view* views, int32_t n, const 
     }
     int sms = 0;
     VV_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    const long long want = (long long)sms * per_sm;
-    const int grid = (int)std::max(1LL, std::min(want, tiles));
-    kern<<<grid, tw * th, 0, c->stream>>>((const BatchView*)c->d_batch, n, counter, (int)tiles);
-    VV_CUDA(c, cudaGetLastError());
+    BatchParams& bp = *(BatchParams*)c->h_batch;
+    for (int k = 0; k < chunks; ++k) {
+        const int first = k * kMaxLaunchViews, cnt = std::min(kMaxLaunchViews, n - first);
+        long long tiles = 0;
+        for (int i = 0; i < cnt; ++i) {
+            const vv_batch_view& bv = views[first + i];
+            const vv_uniforms* u = &bv.u;
+            if (bv.tree < 0 || bv.tree >= VV_MAX_TREES) return batch_fail(c, VV_ERR_ARG, "bad tree index");
+            const DeviceTree& t = bv.ctx->trees[bv.tree];
+            if (!t.nodes) return batch_fail(c, VV_ERR_STATE, "node pool not uploaded");
+            const int W = u->width, H = u->height;
+            if (W <= 0 || H <= 0 || W > 16384 || H > 16384) return batch_fail(c, VV_ERR_ARG, "bad viewport");
+            if (u->jitter_tex_size != bv.ctx->jitter_size)
+                return batch_fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
+            if (!(u->ray_step_size > 0.0f)) return batch_fail(c, VV_ERR_ARG, "ray_step_size must be > 0");
+            if (u->compute_lighting) return batch_fail(c, VV_ERR_ARG, "the batched launch covers the unlit ray cast");
+            for (int a = 0; a < 3; ++a)
+                if (u->brick_pool_dimension[a] != (float)(bv.ctx->slots[a] * 10))
+                    return batch_fail(c, VV_ERR_ARG, "brick_pool_dimension does not match the brick pool");
+            BatchView& v = bp.v[i];
+            std::memset(&v, 0, sizeof(v));
+            v.p.u = *u;
+            v.p.nodes = t.nodes;
+            for (int a = 0; a < 3; ++a) {
+                v.p.node_dim[a] = t.dim[a];
+                v.p.slots[a] = bv.ctx->slots[a];
+            }
+            v.p.bricks = bv.ctx->bricks;
+            v.p.cell_mask = ctx_cell_mask(bv.ctx);
+            v.p.jitter = bv.ctx->d_jitter;
+            v.p.color = (float4*)bv.color;
+            v.p.usage = (uint4*)bv.usage;
+            v.p.status = bv.ctx->d_status;
+            v.p.max_iter = vv_max_iterations(u);
+            v.tiles_x = (W + tw - 1) / tw;
+            v.tile_begin = (int)tiles;
+            tiles += (long long)v.tiles_x * ((H + th - 1) / th);
+            if (tiles > 0x7FFFFFFFLL) return batch_fail(c, VV_ERR_ARG, "batch has too many tiles");
+        }
+        bp.n = cnt;
+        bp.total_tiles = (int)tiles;
+        unsigned* counter = (unsigned*)((char*)c->d_batch + (size_t)k * 16);
+        VV_CUDA(c, cudaMemsetAsync(counter, 0, sizeof(unsigned), c->stream));
+        const long long want = (long long)sms * per_sm;
+        const int grid = (int)std::max(1LL, std::min(want, tiles));
+        kern<<<grid, tw * th, 0, c->stream>>>(bp, counter);
+        VV_CUDA(c, cudaGetLastError());
+    }
     return VV_OK;
 }
 

@@ -187,7 +187,6 @@ int vv_ctx_destroy(vv_ctx* c) {
         if (b) cudaFree(b);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->h_batch) cudaFreeHost(c->h_batch);
-    if (c->batch_ev) cudaEventDestroy(c->batch_ev);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     delete c;

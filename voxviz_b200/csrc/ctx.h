@@ -74,13 +74,12 @@ struct vv_ctx {
     size_t grid_words_cap = 0;
     void* h_stage = nullptr;
     size_t h_stage_cap = 0;
-    // batched launch: per-view parameters (pinned staging -> device) + queue
+    // batched launch: the launch-parameter block of the views (host) and one
+    // tile-queue counter per launch (device)
     void* h_batch = nullptr;
     size_t h_batch_cap = 0;
     void* d_batch = nullptr;
     size_t d_batch_cap = 0;
-    cudaEvent_t batch_ev = nullptr;  // recorded after the staging copy
-    bool batch_ev_live = false;
     // profiling
     bool profiling = false;
     bool timed = false;
