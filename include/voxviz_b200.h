@@ -50,7 +50,8 @@ typedef enum vv_status {
     VV_ERR_TIMEOUT = 4,  /* a bounded device wait or loop ran out           */
     VV_ERR_BOUNDS = 5,   /* a device-side index check failed                */
     VV_ERR_STATE = 6,    /* call out of order (e.g. render before upload)   */
-    VV_ERR_NODEV = 7     /* no CUDA device / extension not usable           */
+    VV_ERR_NODEV = 7,    /* no CUDA device / extension not usable           */
+    VV_ERR_IO = 8        /* a file is missing, unreadable or malformed      */
 } vv_status;
 
 /* Brick-pool texel formats. RGBA8 is GL_RGBA8 (GigaVoxelsBrickPool.cpp:45);
@@ -414,8 +415,74 @@ int vv_octree_produce_gradients(const vv_octree* tree, const uint32_t* xyz,
 /* Dense mip level (RGBA8, x fastest) for checking on small volumes. */
 int vv_octree_mip_level(const vv_octree* tree, int32_t level, uint32_t* out,
                         size_t out_words);
-/* Column heights of the leaf level (dim*dim int32, x fastest). */
+/* Column heights of the leaf level (dim*dim int32, x fastest).  This and
+ * vv_octree_mip_level need a terrain tree (VV_ERR_ARG for a file tree). */
 int vv_octree_heights(const vv_octree* tree, int32_t* out);
+
+/* ---- GigaVoxels dataset files: .gvx / .gvb / .gvp ------------------------
+ * A .gvx is the XML octree (a GigaVoxelsOctTree element with nested Node
+ * elements, 8 children each, depth-first), voxels_<level>.gvb beside it the
+ * level's bricks: int compressed, then per brick size_t dims[3], uint32
+ * border[3], and colours and gradients as (int compressed, uint32 bytes,
+ * payload).  A .gvp lists paged trees (OctTree elements with a TreeFile). */
+enum {
+    /* Store constant nodes' colours in their node words.  Without it a file
+     * tree renders as the reference renders it: Node::setConstantValue
+     * (GigaVoxelsOctTree.cpp:1611-1621) drops the colour, so constant nodes
+     * are transparent black. */
+    VV_GVX_CONSTANT_COLORS = 1,
+    /* Skip the gradient payloads (GigaVoxelsReader::SetLoadNormals(false)). */
+    VV_GVX_SKIP_GRADIENTS = 2
+};
+/* GigaVoxelsReader::LoadOctTreeFile (GigaVoxelsReader.cpp:373-514,541-563,
+ * bricks :106-221).  The tree pages like a terrain tree through
+ * vv_renderer_create; its bricks are kept on the host and, with
+ * device_paging, in device memory, from where paging copies them into pool
+ * slots.  A brick's node pointer is slot origin + the brick's border
+ * (BrickPool::uploadBrick, GigaVoxelsBrickPool.cpp:800-808).  Supported:
+ * brick size 8 (stored dims <= 10, border <= 2), uncompressed binary bricks,
+ * MaxDepth <= 11.  Errors: VV_ERR_IO (missing or malformed file, or one the
+ * reference rejects: depth or element mismatch, compression mismatch, empty
+ * payload, data after the last brick), VV_ERR_ARG (unsupported content);
+ * the message is in vv_last_error(NULL). */
+int vv_octree_load_gvx(const char* path, int32_t flags, vv_octree** out);
+/* Write tree.gvx and voxels_<level>.gvb into the existing directory `dir`,
+ * in the voxelizer's layout (Voxelizer.cu:2840-3058,
+ * VoxelBrickWriter.cu:509-818).  A terrain tree writes its 10^3 bricks with
+ * a 1-voxel border and, for depth <= 6, its gradients (unsigned bytes); the
+ * zero vector (128,128,128) otherwise or with VV_GVX_SKIP_GRADIENTS.  A file
+ * tree writes back what it read. */
+int vv_octree_save_gvx(const vv_octree* tree, const char* dir, int32_t flags);
+typedef struct vv_gvx_info {
+    int32_t file_backed;       /* 1 for a tree read from files */
+    int32_t max_depth;         /* MaxDepth: levels */
+    float origin[3];           /* X, Y, Z */
+    float delta[3];            /* DeltaX.. */
+    int32_t volume_size[3];    /* VolumeXSize.. */
+    int32_t brick_size[3];     /* BrickXSize.. */
+    int64_t bricks;            /* bricks held */
+    int32_t has_gradients;     /* gradient payloads loaded (unsigned) */
+    float ray_step_size;       /* getRayStepSize: one leaf voxel of the box */
+} vv_gvx_info;
+int vv_octree_gvx_info(const vv_octree* tree, vv_gvx_info* info);
+
+/* One paged tree of a .gvp (PagedOctTreeNode, GigaVoxelsReader.cpp:59-96). */
+typedef struct vv_gvp_tile {
+    float center[3];
+    float radius;
+    float size_meters[3];
+    char tree_file[1024];      /* read: the .gvp's directory joined; write: as given */
+} vv_gvp_tile;
+typedef struct vv_gvp_info {
+    int32_t compressed;
+    int32_t brick_size[3];
+    int32_t tiles;             /* tiles in the file */
+    float sphere_center[3];    /* BoundingSphere::expandBy over the tiles */
+    double sphere_radius;      /* -1 with no tiles */
+} vv_gvp_info;
+/* LoadGVP (GigaVoxelsReader.cpp:35-101): the first min(cap, tiles) tiles. */
+int vv_gvp_read(const char* path, vv_gvp_info* info, vv_gvp_tile* tiles, int32_t cap);
+int vv_gvp_write(const char* path, const vv_gvp_info* info, const vv_gvp_tile* tiles, int32_t n);
 
 /* ---- camera + uniform derivation ---------------------------------------- */
 

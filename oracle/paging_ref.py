@@ -25,8 +25,13 @@ CONSTANT = 0x40000000
 
 
 class PagingRef:
-    def __init__(self, words: np.ndarray, slots: tuple[int, int, int]):
+    def __init__(self, words: np.ndarray, slots: tuple[int, int, int], borders: dict | None = None):
+        """borders: grid cell -> (bx, by, bz), where a brick's 8^3 voxels
+        start in its slot (BrickPool::uploadBrick sets the node pointer to
+        slot origin + border, GigaVoxelsBrickPool.cpp:800-808); (1, 1, 1)
+        for cells not listed."""
         self.words = np.array(words, dtype=np.uint32, copy=True)  # (dz, dy, dx, 2)
+        self.borders = borders or {}
         self.sx, self.sy, self.sz = slots
         self.total = self.sx * self.sy * self.sz
         self.lru: OrderedDict[int, None] = OrderedDict((s, None) for s in range(self.total))
@@ -62,7 +67,8 @@ class PagingRef:
         self.slot_node[s] = n
         self.node_slot[n] = s
         x, y, z = s % self.sx, (s // self.sx) % self.sy, s // (self.sx * self.sy)
-        self.words[n[2], n[1], n[0], 1] = ((x * 10 + 1) << 20) | ((y * 10 + 1) << 10) | (z * 10 + 1)
+        bx, by, bz = self.borders.get(n, (1, 1, 1))
+        self.words[n[2], n[1], n[0], 1] = ((x * 10 + bx) << 20) | ((y * 10 + by) << 10) | (z * 10 + bz)
         self.words[n[2], n[1], n[0], 0] |= np.uint32(RESIDENT)
         self.lru.move_to_end(s)
         self.uploaded.append(n)

@@ -7,7 +7,9 @@ path (a missing library raises).
 The objects mirror the reference's host API:
 
 * :class:`Octree` - ``gv::GigaVoxelsOctTree`` built from a synthetic terrain
-  (VoxViz/GigaVoxels/GigaVoxelsOctTree.h:34-516)
+  (VoxViz/GigaVoxels/GigaVoxelsOctTree.h:34-516) or read from ``.gvx`` /
+  ``.gvb`` files (``GigaVoxelsReader``, VoxViz/GigaVoxels/GigaVoxelsReader.cpp);
+  :func:`read_gvp` reads a ``.gvp`` index of paged trees
 * :class:`Context` - device pools and the draw entry point
   (node pool: GigaVoxelsOctTreeNodePool.h, brick pool: GigaVoxelsBrickPool.h)
 * :class:`Renderer` - the ``"gv"`` ``vox::Renderer`` frame protocol
@@ -25,7 +27,8 @@ from ._native import (FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_FP16, VV_FMT_F
                       VV_PASS_ALL, VV_PASS_COMPACT, VV_PASS_RAYCAST, VV_PASS_SELECT, Camera, FrameOut,
                       NodePatch, OctreeInfo, Uniforms, VVError)
 
-__all__ = ["Octree", "Context", "Renderer", "Batch", "batch_variants", "make_camera", "look_at",
+__all__ = ["Octree", "Context", "Renderer", "Batch", "batch_variants", "make_camera", "look_at", "read_gvp",
+           "write_gvp",
            "compute_uniforms", "make_jitter", "pixel_size", "lib", "VVError", "Uniforms", "Camera", "FMT_NAMES",
            "TEXEL_BYTES"]
 
@@ -118,6 +121,30 @@ class Octree:
         _check(lib().vv_octree_build_terrain(C.byref(d), C.byref(h)), what="octree build")
         return cls(h.value)
 
+    @classmethod
+    def load_gvx(cls, path, constant_colors: bool = False, gradients: bool = True) -> "Octree":
+        """``GigaVoxelsReader::LoadOctTreeFile``: a tree.gvx and its voxels_<level>.gvb.
+
+        constant_colors=False renders constant nodes as the reference does
+        (transparent: ``Node::setConstantValue`` drops the colour); True keeps
+        their colours.  gradients=False skips the gradient payloads.
+        """
+        flags = (N.VV_GVX_CONSTANT_COLORS if constant_colors else 0) | (0 if gradients else N.VV_GVX_SKIP_GRADIENTS)
+        h = C.c_void_p()
+        _check(lib().vv_octree_load_gvx(str(path).encode(), flags, C.byref(h)), what="load gvx")
+        return cls(h.value)
+
+    def save_gvx(self, directory, gradients: bool = True) -> None:
+        """Write tree.gvx and voxels_<level>.gvb into an existing directory."""
+        _check(lib().vv_octree_save_gvx(self._h, str(directory).encode(), 0 if gradients else N.VV_GVX_SKIP_GRADIENTS),
+               what="save gvx")
+
+    @property
+    def gvx_info(self) -> N.GvxInfo:
+        i = N.GvxInfo()
+        _check(lib().vv_octree_gvx_info(self._h, C.byref(i)), what="gvx info")
+        return i
+
     def close(self) -> None:
         if self._h:
             lib().vv_octree_destroy(self._h)
@@ -180,6 +207,36 @@ class Octree:
         out = np.zeros((d, d), dtype=np.int32)
         _check(lib().vv_octree_heights(self._h, _ptr(out)), what="heights")
         return out
+
+
+def read_gvp(path) -> dict:
+    """``LoadGVP``: the paged-tree index (tiles with their bounding spheres)."""
+    info = N.GvpInfo()
+    _check(lib().vv_gvp_read(str(path).encode(), C.byref(info), None, 0), what="read gvp")
+    tiles = (N.GvpTile * max(info.tiles, 1))()
+    _check(lib().vv_gvp_read(str(path).encode(), C.byref(info), tiles, info.tiles), what="read gvp")
+    return {
+        "compressed": bool(info.compressed),
+        "brick_size": tuple(info.brick_size),
+        "sphere_center": tuple(info.sphere_center),
+        "sphere_radius": info.sphere_radius,
+        "tiles": [{"center": tuple(t.center), "radius": t.radius, "size_meters": tuple(t.size_meters),
+                   "tree_file": t.tree_file.decode()} for t in tiles[:info.tiles]],
+    }
+
+
+def write_gvp(path, tiles: Sequence[dict], compressed: bool = False, brick_size=(8, 8, 8)) -> None:
+    """Write a .gvp index; each tile dict has center, radius, size_meters and
+    tree_file (relative to the .gvp's directory)."""
+    info = N.GvpInfo(compressed=1 if compressed else 0)
+    info.brick_size[:] = list(brick_size)
+    arr = (N.GvpTile * max(len(tiles), 1))()
+    for a, t in zip(arr, tiles):
+        a.center[:] = list(t["center"])
+        a.radius = t["radius"]
+        a.size_meters[:] = list(t["size_meters"])
+        a.tree_file = str(t["tree_file"]).encode()
+    _check(lib().vv_gvp_write(str(path).encode(), C.byref(info), arr, len(tiles)), what="write gvp")
 
 
 # --------------------------------------------------------------- context ---

@@ -11,7 +11,8 @@ from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libvoxviz_b200.so"
 
-VV_OK, VV_ERR_ARG, VV_ERR_OOM, VV_ERR_CUDA, VV_ERR_TIMEOUT, VV_ERR_BOUNDS, VV_ERR_STATE, VV_ERR_NODEV = range(8)
+VV_OK, VV_ERR_ARG, VV_ERR_OOM, VV_ERR_CUDA, VV_ERR_TIMEOUT, VV_ERR_BOUNDS, VV_ERR_STATE, VV_ERR_NODEV, VV_ERR_IO = range(9)
+VV_GVX_CONSTANT_COLORS, VV_GVX_SKIP_GRADIENTS = 1, 2
 VV_FMT_RGBA8, VV_FMT_FP16, VV_FMT_BF16, VV_FMT_FP32 = range(4)
 VV_PASS_RAYCAST, VV_PASS_SELECT, VV_PASS_COMPACT, VV_PASS_ALL = 1, 2, 4, 7
 FMT_NAMES = {"rgba8": VV_FMT_RGBA8, "fp16": VV_FMT_FP16, "bf16": VV_FMT_BF16, "fp32": VV_FMT_FP32}
@@ -97,6 +98,39 @@ class OctreeInfo(C.Structure):
         ("root_is_constant", C.c_int32),
         ("root_word0", C.c_uint32),
         ("root_word1", C.c_uint32),
+    ]
+
+
+class GvxInfo(C.Structure):
+    _fields_ = [
+        ("file_backed", C.c_int32),
+        ("max_depth", C.c_int32),
+        ("origin", C.c_float * 3),
+        ("delta", C.c_float * 3),
+        ("volume_size", i3),
+        ("brick_size", i3),
+        ("bricks", C.c_int64),
+        ("has_gradients", C.c_int32),
+        ("ray_step_size", C.c_float),
+    ]
+
+
+class GvpTile(C.Structure):
+    _fields_ = [
+        ("center", C.c_float * 3),
+        ("radius", C.c_float),
+        ("size_meters", C.c_float * 3),
+        ("tree_file", C.c_char * 1024),
+    ]
+
+
+class GvpInfo(C.Structure):
+    _fields_ = [
+        ("compressed", C.c_int32),
+        ("brick_size", i3),
+        ("tiles", C.c_int32),
+        ("sphere_center", C.c_float * 3),
+        ("sphere_radius", C.c_double),
     ]
 
 
@@ -227,6 +261,11 @@ SIGNATURES = {
     "vv_octree_produce_bricks": (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
     "vv_octree_mip_level": (C.c_int, [P, C.c_int32, P, C.c_size_t]),
     "vv_octree_heights": (C.c_int, [P, P]),
+    "vv_octree_load_gvx": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(P)]),
+    "vv_octree_save_gvx": (C.c_int, [P, C.c_char_p, C.c_int32]),
+    "vv_octree_gvx_info": (C.c_int, [P, C.POINTER(GvxInfo)]),
+    "vv_gvp_read": (C.c_int, [C.c_char_p, C.POINTER(GvpInfo), C.POINTER(GvpTile), C.c_int32]),
+    "vv_gvp_write": (C.c_int, [C.c_char_p, C.POINTER(GvpInfo), C.POINTER(GvpTile), C.c_int32]),
     "vv_compute_uniforms": (C.c_int, [C.POINTER(OctreeInfo), C.POINTER(Camera), C.c_int32, C.c_int32, C.c_int32,
                                       C.c_float, C.c_float, C.POINTER(Uniforms)]),
     "vv_camera_pixel_size": (C.c_float, [C.POINTER(Camera)]),

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "ctx.h"
+#include "gvfile.h"
 #include "octree.h"
 #include "renderer.h"
 
@@ -54,7 +55,7 @@ int vv_octree_get_info(const vv_octree* t, vv_octree_info* info) {
     if (!t || !info) return VV_ERR_ARG;
     std::memset(info, 0, sizeof(*info));
     info->depth = t->tree->depth();
-    info->volume_dim = 8 << t->tree->depth();
+    info->volume_dim = t->tree->leaf_dim();
     info->node_count = (int64_t)t->tree->node_count();
     for (int a = 0; a < 3; ++a) info->pool_dim[a] = t->tree->pool_dim()[a];
     info->nonconst_count = (int64_t)t->tree->nonconst_count();
@@ -117,7 +118,7 @@ int vv_octree_produce_bricks(const vv_octree* t, const uint32_t* xyz, int32_t n,
 int vv_octree_produce_gradients(const vv_octree* t, const uint32_t* xyz, int32_t n, int32_t fmt, void* out) {
     if (!t || n < 0 || (n > 0 && (!xyz || !out))) return VV_ERR_ARG;
     if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return VV_ERR_ARG;
-    if (t->tree->depth() > 6) return VV_ERR_ARG;
+    if (t->tree->file_backed() ? !t->tree->file_has_normals() : t->tree->depth() > 6) return VV_ERR_ARG;
     const size_t tb = vv::texel_bytes(fmt);
     for (int32_t i = 0; i < n; ++i) {
         const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
@@ -137,7 +138,7 @@ int vv_octree_produce_gradients(const vv_octree* t, const uint32_t* xyz, int32_t
 }
 
 int vv_octree_mip_level(const vv_octree* t, int32_t level, uint32_t* out, size_t out_words) {
-    if (!t || !out || level < 0 || level > t->tree->depth()) return VV_ERR_ARG;
+    if (!t || !out || level < 0 || level > t->tree->depth() || !t->tree->has_volume()) return VV_ERR_ARG;
     const vv::TerrainVolume& v = t->tree->volume();
     const int d = v.mip(level).dim;
     if (out_words < (size_t)d * d * d) return VV_ERR_ARG;
@@ -149,9 +150,130 @@ int vv_octree_mip_level(const vv_octree* t, int32_t level, uint32_t* out, size_t
 }
 
 int vv_octree_heights(const vv_octree* t, int32_t* out) {
-    if (!t || !out) return VV_ERR_ARG;
+    if (!t || !out || !t->tree->has_volume()) return VV_ERR_ARG;
     const auto& h = t->tree->volume().heights();
     std::memcpy(out, h.data(), h.size() * sizeof(int32_t));
+    return VV_OK;
+}
+
+int vv_octree_load_gvx(const char* path, int32_t flags, vv_octree** out) {
+    if (!path || !out) {
+        vv::set_thread_error("vv_octree_load_gvx: path and out are required");
+        return VV_ERR_ARG;
+    }
+    *out = nullptr;
+    try {
+        vv::GvxFile f;
+        std::string err;
+        const int rc = vv::read_gvx(path, (flags & VV_GVX_SKIP_GRADIENTS) == 0, f, err);
+        if (rc) {
+            vv::set_thread_error(err);
+            return rc;
+        }
+        auto o = std::make_unique<vv_octree>();
+        o->tree = vv::GigaVoxelsOctTree::from_gvx(std::move(f), (flags & VV_GVX_CONSTANT_COLORS) != 0);
+        *out = o.release();
+        return VV_OK;
+    } catch (const std::bad_alloc&) {
+        vv::set_thread_error("vv_octree_load_gvx: out of host memory");
+        return VV_ERR_OOM;
+    } catch (const std::exception& e) {
+        vv::set_thread_error(std::string("vv_octree_load_gvx: ") + e.what());
+        return VV_ERR_ARG;
+    }
+}
+
+int vv_octree_save_gvx(const vv_octree* t, const char* dir, int32_t flags) {
+    if (!t || !dir) return VV_ERR_ARG;
+    try {
+        std::string err;
+        if (!t->tree->save_gvx(dir, (flags & VV_GVX_SKIP_GRADIENTS) == 0, err)) {
+            vv::set_thread_error(err);
+            return VV_ERR_IO;
+        }
+        return VV_OK;
+    } catch (const std::bad_alloc&) {
+        return VV_ERR_OOM;
+    }
+}
+
+int vv_octree_gvx_info(const vv_octree* t, vv_gvx_info* info) {
+    if (!t || !info) return VV_ERR_ARG;
+    std::memset(info, 0, sizeof(*info));
+    const vv::GvxHeader* h = t->tree->file_header();
+    info->file_backed = h ? 1 : 0;
+    info->max_depth = t->tree->depth() + 1;
+    for (int a = 0; a < 3; ++a) {
+        info->origin[a] = h ? h->origin[a] : 0.0f;
+        info->delta[a] = h ? h->delta[a] : 1.0f / (float)(8 << t->tree->depth());
+        info->volume_size[a] = h ? h->volume_size[a] : 8 << t->tree->depth();
+        info->brick_size[a] = h ? h->brick_size[a] : 8;
+    }
+    info->bricks = h ? (int64_t)t->tree->file_brick_count() : (int64_t)t->tree->nonconst_count();
+    info->has_gradients = h ? (t->tree->file_has_normals() ? 1 : 0) : (t->tree->depth() <= 6 ? 1 : 0);
+    info->ray_step_size = 1.0f / (float)t->tree->leaf_dim();
+    return VV_OK;
+}
+
+int vv_gvp_read(const char* path, vv_gvp_info* info, vv_gvp_tile* tiles, int32_t cap) {
+    if (!path || !info || cap < 0 || (cap > 0 && !tiles)) return VV_ERR_ARG;
+    try {
+        vv::GvpFile f;
+        std::string err;
+        const int rc = vv::read_gvp(path, f, err);
+        if (rc) {
+            vv::set_thread_error(err);
+            return rc;
+        }
+        std::memset(info, 0, sizeof(*info));
+        info->compressed = f.compressed ? 1 : 0;
+        for (int a = 0; a < 3; ++a) {
+            info->brick_size[a] = f.brick_size[a];
+            info->sphere_center[a] = f.sphere_center[a];
+        }
+        info->tiles = (int32_t)f.tiles.size();
+        info->sphere_radius = f.sphere_radius;
+        for (int32_t i = 0; i < cap && (size_t)i < f.tiles.size(); ++i) {
+            const vv::GvpTile& s = f.tiles[(size_t)i];
+            vv_gvp_tile& d = tiles[i];
+            std::memset(&d, 0, sizeof(d));
+            for (int a = 0; a < 3; ++a) {
+                d.center[a] = s.center[a];
+                d.size_meters[a] = s.size_meters[a];
+            }
+            d.radius = s.radius;
+            if (s.tree_file.size() >= sizeof(d.tree_file)) {
+                vv::set_thread_error("vv_gvp_read: a TreeFile path is longer than 1023 bytes");
+                return VV_ERR_ARG;
+            }
+            std::memcpy(d.tree_file, s.tree_file.c_str(), s.tree_file.size() + 1);
+        }
+        return VV_OK;
+    } catch (const std::bad_alloc&) {
+        return VV_ERR_OOM;
+    }
+}
+
+int vv_gvp_write(const char* path, const vv_gvp_info* info, const vv_gvp_tile* tiles, int32_t n) {
+    if (!path || !info || n < 0 || (n > 0 && !tiles)) return VV_ERR_ARG;
+    vv::GvpFile f;
+    f.compressed = info->compressed != 0;
+    for (int a = 0; a < 3; ++a) f.brick_size[a] = info->brick_size[a];
+    for (int32_t i = 0; i < n; ++i) {
+        vv::GvpTile t;
+        for (int a = 0; a < 3; ++a) {
+            t.center[a] = tiles[i].center[a];
+            t.size_meters[a] = tiles[i].size_meters[a];
+        }
+        t.radius = tiles[i].radius;
+        t.tree_file.assign(tiles[i].tree_file, strnlen(tiles[i].tree_file, sizeof(tiles[i].tree_file)));
+        f.tiles.push_back(std::move(t));
+    }
+    std::string err;
+    if (!vv::write_gvp(path, f, err)) {
+        vv::set_thread_error(err);
+        return VV_ERR_IO;
+    }
     return VV_OK;
 }
 
@@ -159,7 +281,8 @@ int vv_compute_uniforms(const vv_octree_info* tree, const vv_camera* cam, int32_
                         float lod_scalar, float alpha_stop, vv_uniforms* out) {
     if (!tree || !cam || !out || cam->width <= 0 || cam->height <= 0) return VV_ERR_ARG;
     const int slots[3] = {sx, sy, sz};
-    vv::compute_uniforms(tree->depth, tree->root_is_constant != 0, *cam, slots, lod_scalar, alpha_stop, *out);
+    vv::compute_uniforms(tree->depth, tree->volume_dim, tree->root_is_constant != 0, *cam, slots, lod_scalar,
+                         alpha_stop, *out);
     return VV_OK;
 }
 

@@ -138,6 +138,7 @@ const char* vv_status_string(int s) {
         case VV_ERR_BOUNDS: return "device index out of bounds";
         case VV_ERR_STATE: return "call out of order";
         case VV_ERR_NODEV: return "no CUDA device";
+        case VV_ERR_IO: return "file missing, unreadable or malformed";
         default: return "unknown status";
     }
 }

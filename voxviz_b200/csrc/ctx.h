@@ -25,6 +25,8 @@ int ctx_ensure_host(vv_ctx* c, void** ptr, size_t* cap, size_t bytes);
 // The pool's empty-cell masks when valid, else nullptr (no skipping).
 const uint32_t* ctx_cell_mask(const vv_ctx* c);
 uint32_t* ctx_cell_mask_rw(vv_ctx* c);
+// The message vv_last_error(NULL) returns on this thread.
+void set_thread_error(const std::string& msg);
 
 }  // namespace vv
 

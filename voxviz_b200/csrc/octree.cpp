@@ -132,19 +132,8 @@ std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<cons
         }
     }
     const size_t num_nodes = 8 * blocks;
-    // OctTreeNodePool::create3DTexture grid dimensions (NodePool.cpp:98-116).
-    size_t cube_root = (size_t)std::pow((double)num_nodes, 1.0 / 3.0);
-    if (cube_root % 2 != 0) {
-        --cube_root;
-        if (cube_root == 0) cube_root = 2;
-    }
-    size_t dx = cube_root, dy = cube_root, dz = cube_root;
-    while (dx * dy * dz < num_nodes) dx += 2;
-    if (dx > 1022 || dy > 1022 || dz > 1022)
-        throw std::runtime_error("node pool exceeds the 10-bit grid of the node encoding");
-    t->pool_dim_[0] = (int)dx;
-    t->pool_dim_[1] = (int)dy;
-    t->pool_dim_[2] = (int)dz;
+    t->set_pool_dim(num_nodes);
+    t->leaf_dim_ = 8 << L;
 
     t->level_.assign(num_nodes, -1);
     t->ci_.assign(num_nodes, 0);
@@ -153,7 +142,6 @@ std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<cons
     t->parent_.assign(num_nodes, kNoParent);
     t->word0_.assign(num_nodes, 0);
     t->word1_.assign(num_nodes, 0);
-    const size_t bx = dx / 2, by = dy / 2;
     size_t nonconst = 0;
     for (int d = 0; d <= L; ++d) {
         const LevelNodes& cur = lv[(size_t)d];
@@ -171,19 +159,210 @@ std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<cons
             } else {
                 ++nonconst;
             }
-            if (cur.first_child[q] != UINT32_MAX) {
-                size_t B = lv[(size_t)d + 1].nidx[cur.first_child[q]] / 8;
-                uint32_t x = (uint32_t)(2 * (B % bx));
-                uint32_t y = (uint32_t)(2 * ((B / bx) % by));
-                uint32_t z = (uint32_t)(2 * (B / (bx * by)));
-                w0 |= pack10(x, y, z);
-            }
+            if (cur.first_child[q] != UINT32_MAX) w0 |= t->child_pointer(lv[(size_t)d + 1].nidx[cur.first_child[q]] / 8);
             t->word0_[n] = w0;
             t->word1_[n] = w1;
         }
     }
     t->nonconst_ = nonconst;
     return t;
+}
+
+void GigaVoxelsOctTree::set_pool_dim(size_t num_nodes) {
+    size_t cube_root = (size_t)std::pow((double)num_nodes, 1.0 / 3.0);
+    if (cube_root % 2 != 0) {
+        --cube_root;
+        if (cube_root == 0) cube_root = 2;
+    }
+    size_t dx = cube_root, dy = cube_root, dz = cube_root;
+    while (dx * dy * dz < num_nodes) dx += 2;
+    if (dx > 1022 || dy > 1022 || dz > 1022)
+        throw std::runtime_error("node pool exceeds the 10-bit grid of the node encoding");
+    pool_dim_[0] = (int)dx;
+    pool_dim_[1] = (int)dy;
+    pool_dim_[2] = (int)dz;
+}
+
+// The child pointer of word0 for child block `block`: the block's first grid
+// cell, blocks laid x-major over the grid's 2x2x2 cells.
+uint32_t GigaVoxelsOctTree::child_pointer(size_t block) const {
+    const size_t bx = (size_t)pool_dim_[0] / 2, by = (size_t)pool_dim_[1] / 2;
+    return pack10((uint32_t)(2 * (block % bx)), (uint32_t)(2 * ((block / bx) % by)), (uint32_t)(2 * (block / (bx * by))));
+}
+
+std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::from_gvx(GvxFile&& f, bool constant_colors) {
+    std::unique_ptr<GigaVoxelsOctTree> t(new GigaVoxelsOctTree());
+    const size_t nn = f.nodes.size();
+    if (nn == 0 || nn % 8 != 0 || f.nodes[0].level != 0) throw std::runtime_error("the file has no root node");
+    t->depth_ = f.h.max_depth - 1;
+    const int vmax = std::max(f.h.volume_size[0], std::max(f.h.volume_size[1], f.h.volume_size[2]));
+    t->leaf_dim_ = vmax > 0 ? vmax : 8 << t->depth_;
+    t->set_pool_dim(nn);
+    auto st = std::make_unique<FileStore>();
+    st->h = f.h;
+    t->level_.assign(nn, -1);
+    t->ci_.assign(nn, 0);
+    t->cj_.assign(nn, 0);
+    t->ck_.assign(nn, 0);
+    t->parent_.assign(nn, kNoParent);
+    t->word0_.assign(nn, 0);
+    t->word1_.assign(nn, 0);
+    st->brick_of.assign(nn, -1);
+    st->brick_index.assign(nn, -1);
+    st->color.assign(nn, 0);
+    st->type.assign(nn, 0);
+    st->mip.assign(3 * nn, 0);
+    // global brick ids: the levels' bricks one after another
+    std::vector<size_t> first(f.bricks.size() + 1, 0);
+    for (size_t lv = 0; lv < f.bricks.size(); ++lv) first[lv + 1] = first[lv] + f.bricks[lv].size();
+    const size_t nb = first.back();
+    bool normals = nb > 0;
+    for (const auto& lv : f.bricks)
+        for (const GvxBrick& b : lv)
+            if (b.normals.empty()) normals = false;
+    st->texels.assign(nb * VV_BRICK_TEXELS, 0u);
+    if (normals) st->normals.assign(nb * VV_BRICK_TEXELS, 0u);
+    st->border.assign(3 * nb, 1);
+    st->dims.assign(3 * nb, 10);
+    size_t nonconst = 0;
+    for (size_t n = 0; n < nn; ++n) {
+        const GvxNode& r = f.nodes[n];
+        if (r.level < 0) continue;
+        t->level_[n] = r.level;
+        for (int a = 0; a < 3; ++a) st->mip[3 * n + a] = r.mip[a];
+        t->ci_[n] = (uint16_t)std::max(0, r.mip[0] / 8);
+        t->cj_[n] = (uint16_t)std::max(0, r.mip[1] / 8);
+        t->ck_[n] = (uint16_t)std::max(0, r.mip[2] / 8);
+        t->parent_[n] = r.parent;
+        st->type[n] = r.type;
+        st->color[n] = r.color;
+        uint32_t w0 = 0, w1 = 0;
+        if (r.type != kGvxNonConst) {
+            w0 |= kConstantBit;
+            if (constant_colors) w1 = r.color;
+        } else {
+            ++nonconst;
+            if (r.brick < 0 || (size_t)r.level >= f.bricks.size() || (size_t)r.brick >= f.bricks[(size_t)r.level].size())
+                throw std::runtime_error("a non-constant node has no brick");
+            st->brick_of[n] = (int32_t)(first[(size_t)r.level] + (size_t)r.brick);
+            st->brick_index[n] = r.brick;
+        }
+        if (r.child_block >= 0) w0 |= t->child_pointer((size_t)r.child_block);
+        t->word0_[n] = w0;
+        t->word1_[n] = w1;
+    }
+    for (size_t lv = 0; lv < f.bricks.size(); ++lv)
+        for (size_t i = 0; i < f.bricks[lv].size(); ++i) {
+            GvxBrick& b = f.bricks[lv][i];
+            const size_t id = first[lv] + i;
+            uint32_t* out = st->texels.data() + id * VV_BRICK_TEXELS;
+            uint32_t* nout = normals ? st->normals.data() + id * VV_BRICK_TEXELS : nullptr;
+            size_t q = 0;
+            for (int z = 0; z < b.dims[2]; ++z)
+                for (int y = 0; y < b.dims[1]; ++y)
+                    for (int x = 0; x < b.dims[0]; ++x, ++q) {
+                        const size_t o = (size_t)(z * 100 + y * 10 + x);
+                        std::memcpy(out + o, b.colors.data() + 4 * q, 4);
+                        if (nout)
+                            nout[o] = (uint32_t)b.normals[3 * q] | ((uint32_t)b.normals[3 * q + 1] << 8) |
+                                      ((uint32_t)b.normals[3 * q + 2] << 16);
+                    }
+            for (int a = 0; a < 3; ++a) {
+                st->border[3 * id + a] = b.border[a];
+                st->dims[3 * id + a] = b.dims[a];
+            }
+            std::vector<uint8_t>().swap(b.colors);
+            std::vector<uint8_t>().swap(b.normals);
+        }
+    t->nonconst_ = nonconst;
+    t->file_ = std::move(st);
+    return t;
+}
+
+bool GigaVoxelsOctTree::save_gvx(const std::string& dir, bool gradients, std::string& err) const {
+    GvxFile f;
+    const size_t nn = level_.size();
+    if (file_) {
+        f.h = file_->h;
+    } else {
+        f.h.max_depth = depth_ + 1;
+        for (int a = 0; a < 3; ++a) {
+            f.h.delta[a] = 1.0f / (float)(8 << depth_);
+            f.h.volume_size[a] = 8 << depth_;
+            f.h.brick_size[a] = 8;
+        }
+        f.h.binary = true;
+    }
+    f.h.compressed = false;
+    f.nodes.assign(nn, GvxNode());
+    std::vector<size_t> per_level((size_t)f.h.max_depth, 0);
+    std::vector<std::pair<int, int32_t>> brick_slot(nn, {-1, -1});  // (level, index) of node n's brick
+    for (size_t n = 0; n < nn; ++n) {
+        if (level_[n] < 0) continue;
+        GvxNode& r = f.nodes[n];
+        r.level = level_[n];
+        r.parent = parent_[n];
+        if (file_) {
+            for (int a = 0; a < 3; ++a) r.mip[a] = file_->mip[3 * n + a];
+        } else {
+            r.mip[0] = 8 * ci_[n];
+            r.mip[1] = 8 * cj_[n];
+            r.mip[2] = 8 * ck_[n];
+        }
+        if (has_children((uint32_t)n)) {
+            const uint32_t c = word0_[n] & 0x3FFFFFFFu & ~kConstantBit;
+            r.child_block = (int32_t)(index_of((c >> 20) & 0x3FFu, (c >> 10) & 0x3FFu, c & 0x3FFu) / 8);
+        }
+        if (is_constant((uint32_t)n)) {
+            r.type = file_ ? file_->type[n] : (uint8_t)(r.child_block >= 0 ? kGvxConst : kGvxLeafConst);
+            r.color = file_ ? file_->color[n] : word1_[n];
+        } else {
+            r.type = kGvxNonConst;
+            r.brick = file_ ? file_->brick_index[n] : (int32_t)per_level[(size_t)r.level];
+            per_level[(size_t)r.level] = std::max(per_level[(size_t)r.level], (size_t)r.brick + 1);
+            brick_slot[n] = {r.level, r.brick};
+        }
+    }
+    // node of each (level, brick index)
+    std::vector<std::vector<uint32_t>> node_of(per_level.size());
+    for (size_t lv = 0; lv < per_level.size(); ++lv) node_of[lv].assign(per_level[lv], kNoParent);
+    for (size_t n = 0; n < nn; ++n)
+        if (brick_slot[n].first >= 0) node_of[(size_t)brick_slot[n].first][(size_t)brick_slot[n].second] = (uint32_t)n;
+    const bool grads = gradients && (file_ ? file_has_normals() : depth_ <= 6);
+    auto source = [&](size_t lv, size_t i, GvxBrick& b) {
+        const uint32_t n = node_of[lv][i];
+        uint32_t tex[VV_BRICK_TEXELS], nrm[VV_BRICK_TEXELS];
+        if (file_) {
+            const size_t id = (size_t)file_->brick_of[n];
+            for (int a = 0; a < 3; ++a) {
+                b.dims[a] = file_->dims[3 * id + a];
+                b.border[a] = file_->border[3 * id + a];
+            }
+            std::memcpy(tex, file_->texels.data() + id * VV_BRICK_TEXELS, sizeof(tex));
+            if (grads) std::memcpy(nrm, file_->normals.data() + id * VV_BRICK_TEXELS, sizeof(nrm));
+        } else {
+            for (int a = 0; a < 3; ++a) {
+                b.dims[a] = 10;
+                b.border[a] = 1;
+            }
+            produce_brick_rgba8(n, tex);
+            if (grads) produce_gradient_brick(n, VV_FMT_RGBA8, nrm);
+        }
+        const size_t count = (size_t)b.dims[0] * b.dims[1] * b.dims[2];
+        b.colors.resize(4 * count);
+        b.normals.clear();
+        if (grads) b.normals.resize(3 * count);
+        size_t q = 0;
+        for (int z = 0; z < b.dims[2]; ++z)
+            for (int y = 0; y < b.dims[1]; ++y)
+                for (int x = 0; x < b.dims[0]; ++x, ++q) {
+                    const size_t o = (size_t)(z * 100 + y * 10 + x);
+                    std::memcpy(b.colors.data() + 4 * q, tex + o, 4);
+                    if (grads)
+                        for (int c = 0; c < 3; ++c) b.normals[3 * q + c] = (uint8_t)(nrm[o] >> (8 * c));
+                }
+    };
+    return write_gvx(dir, f, per_level, source, err);
 }
 
 void GigaVoxelsOctTree::grid_of(uint32_t n, uint32_t& x, uint32_t& y, uint32_t& z) const {
@@ -217,6 +396,12 @@ void GigaVoxelsOctTree::words_grid(uint32_t* out) const {
 }
 
 void GigaVoxelsOctTree::produce_brick_rgba8(uint32_t n, uint32_t* out) const {
+    if (file_) {
+        const int32_t k = file_->brick_of[n];
+        if (k < 0) std::memset(out, 0, VV_BRICK_TEXELS * sizeof(uint32_t));
+        else std::memcpy(out, file_->texels.data() + (size_t)k * VV_BRICK_TEXELS, VV_BRICK_TEXELS * sizeof(uint32_t));
+        return;
+    }
     const int d = level_[n];
     const int m = depth_ - d;
     const MipLevel& M = vol_->mip(m);
@@ -320,6 +505,23 @@ void GigaVoxelsOctTree::produce_brick(uint32_t n, int fmt, void* out) const {
 
 bool GigaVoxelsOctTree::produce_gradient_brick(uint32_t n, int fmt, void* out) const {
     if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return false;
+    if (file_) {
+        // the file's unsigned bytes (GradientsAreUnsigned is set for every
+        // file tree, GigaVoxelsReader.cpp:419-420); FP32 holds them as b/255
+        const int32_t k = file_->brick_of[n];
+        if (file_->normals.empty() || k < 0) return false;
+        const uint32_t* src = file_->normals.data() + (size_t)k * VV_BRICK_TEXELS;
+        if (fmt == VV_FMT_RGBA8) {
+            std::memcpy(out, src, VV_BRICK_TEXELS * sizeof(uint32_t));
+        } else {
+            float* o = (float*)out;
+            for (int t = 0; t < VV_BRICK_TEXELS; ++t) {
+                for (int c = 0; c < 3; ++c) o[4 * t + c] = (float)((src[t] >> (8 * c)) & 255u) / 255.0f;
+                o[4 * t + 3] = 0.0f;
+            }
+        }
+        return true;
+    }
     {
         std::lock_guard<std::mutex> lock(grads_mu_);
         if (!grads_) {

@@ -12,9 +12,11 @@
 #include <cstdint>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "gradients.h"
+#include "gvfile.h"
 #include "terrain.h"
 
 namespace vv {
@@ -33,8 +35,39 @@ public:
     // build does.
     static std::unique_ptr<GigaVoxelsOctTree> build(std::shared_ptr<const TerrainVolume> vol,
                                                     bool collapse);
+    // GigaVoxelsReader::LoadOctTreeFile (GigaVoxelsReader.cpp:541-563) from
+    // the records read_gvx produced.  Node::setConstantValue
+    // (GigaVoxelsOctTree.cpp:1611-1621) computes a constant node's colour
+    // but never stores it, so the reference renders constant nodes of a
+    // .gvx as transparent black: constant_colors = false keeps that,
+    // true stores the colour in word1 as the in-memory build does.
+    static std::unique_ptr<GigaVoxelsOctTree> from_gvx(GvxFile&& f, bool constant_colors);
+    // The tree as .gvx/.gvb files in dir (the offline voxelizer's layout).
+    // A terrain tree writes 10^3 bricks with a 1-voxel border and, when
+    // gradients is set and the tree is at most 6 levels deep, its
+    // gradients; a file tree writes back what it read.
+    bool save_gvx(const std::string& dir, bool gradients, std::string& err) const;
 
     int depth() const { return depth_; }                // L
+    // Voxels per axis the ray step is derived from: 8 << L for the terrain,
+    // the largest VolumeSize of a file tree (GigaVoxelsReader.cpp:430-440).
+    int leaf_dim() const { return leaf_dim_; }
+    bool has_volume() const { return vol_ != nullptr; }
+    bool file_backed() const { return file_ != nullptr; }
+    const GvxHeader* file_header() const { return file_ ? &file_->h : nullptr; }
+    // Brick store of a file tree: brick b's stored texels at the origin of a
+    // 10^3 RGBA8 block (1000 words from 1000 b), zero elsewhere.
+    size_t file_brick_count() const { return file_ ? file_->border.size() / 3 : 0; }
+    const uint32_t* file_texels() const { return file_ ? file_->texels.data() : nullptr; }
+    bool file_has_normals() const { return file_ && !file_->normals.empty(); }
+    int32_t file_brick(uint32_t n) const { return file_ ? file_->brick_of[n] : -1; }
+    // The node's 8^3 voxels start `border` texels into its slot: the brick
+    // pointer is slot origin + border (BrickPool::uploadBrick,
+    // GigaVoxelsBrickPool.cpp:800-808); (1,1,1) for every terrain brick.
+    void brick_border(uint32_t n, uint32_t b[3]) const {
+        const int32_t k = file_ ? file_->brick_of[n] : -1;
+        for (int a = 0; a < 3; ++a) b[a] = k < 0 ? 1u : file_->border[3 * (size_t)k + a];
+    }
     size_t node_count() const { return level_.size(); } // 8 per block
     const int* pool_dim() const { return pool_dim_; }
     const TerrainVolume& volume() const { return *vol_; }
@@ -71,6 +104,24 @@ public:
     bool produce_gradient_brick(uint32_t n, int fmt, void* out) const;
 
 private:
+    // Node-pool grid dimensions for num_nodes records
+    // (OctTreeNodePool::create3DTexture, GigaVoxelsOctTreeNodePool.cpp:98-116).
+    void set_pool_dim(size_t num_nodes);
+    uint32_t child_pointer(size_t block) const;
+
+    struct FileStore {
+        GvxHeader h;
+        std::vector<uint32_t> texels;       // 1000 RGBA8 per brick
+        std::vector<uint32_t> normals;      // 1000 per brick: unsigned x, y, z bytes (or empty)
+        std::vector<uint8_t> border, dims;  // 3 per brick
+        std::vector<int32_t> brick_of;      // per node: brick, -1 none
+        std::vector<int32_t> brick_index;   // per node: Brick attribute (index in its level)
+        std::vector<uint32_t> color;        // per node: constant colour as read
+        std::vector<uint8_t> type;          // per node: GvxNodeType
+        std::vector<int32_t> mip;           // 3 per node: MipMapX..
+    };
+    std::unique_ptr<FileStore> file_;
+    int leaf_dim_ = 8;
     mutable std::unique_ptr<GradientPyramid> grads_;
     mutable std::mutex grads_mu_;
     std::shared_ptr<const TerrainVolume> vol_;

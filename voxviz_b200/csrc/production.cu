@@ -145,6 +145,67 @@ __global__ void produce_staged_kernel(const __grid_constant__ DeviceTerrainView 
     }
 }
 
+// One CTA per job: store brick job.y into slot job.x.  The store holds
+// RGBA8, so an RGBA8 pool takes 16-byte words as they are (a slot and a
+// store brick are 4000 bytes, 16-byte aligned).
+template <int FMT>
+__device__ __forceinline__ void copy_one(const DeviceBrickStoreView& st, const uint4 job, void* __restrict__ pool,
+                                         uint32_t* __restrict__ masks, long long total_slots, int* status) {
+    __shared__ uint8_t zero[VV_BRICK_TEXELS];
+    if ((long long)job.x >= total_slots || job.y >= st.bricks) {
+        if (threadIdx.x == 0 && status) atomicCAS(status, 0, VV_ERR_BOUNDS);
+        return;
+    }
+    const uint32_t* src = st.texels + (size_t)job.y * VV_BRICK_TEXELS;
+    const size_t base = (size_t)job.x * VV_BRICK_TEXELS;
+    if (FMT == VV_FMT_RGBA8) {
+        const uint4* s4 = (const uint4*)src;
+        uint4* d4 = (uint4*)((uint32_t*)pool + base);
+        for (int q = threadIdx.x; q < VV_BRICK_TEXELS / 4; q += blockDim.x) {
+            const uint4 v = __ldg(s4 + q);
+            d4[q] = v;
+            zero[4 * q] = v.x == 0u;
+            zero[4 * q + 1] = v.y == 0u;
+            zero[4 * q + 2] = v.z == 0u;
+            zero[4 * q + 3] = v.w == 0u;
+        }
+    } else {
+        for (int q = threadIdx.x; q < VV_BRICK_TEXELS; q += blockDim.x) {
+            const uint32_t v = __ldg(src + q);
+            store_texel<FMT>(pool, base + (size_t)q, v);
+            zero[q] = v == 0u;
+        }
+    }
+    if (masks) {
+        __syncthreads();
+        write_cell_mask(zero, masks + (size_t)job.x * kCellMaskWords);
+        __syncthreads();
+    }
+}
+
+template <int FMT>
+__global__ void copy_kernel(const DeviceBrickStoreView st, const uint4* __restrict__ jobs, void* __restrict__ pool,
+                            uint32_t* __restrict__ masks, long long total_slots, int* status) {
+    copy_one<FMT>(st, jobs[blockIdx.x], pool, masks, total_slots, status);
+}
+
+template <int FMT>
+__global__ void copy_staged_kernel(const DeviceBrickStoreView st, const uint4* jobs, const volatile uint32_t* count,
+                                   uint32_t max_jobs, void* __restrict__ pool, uint32_t* __restrict__ masks,
+                                   long long total_slots, int* status) {
+    __shared__ uint32_t s_n;
+    if (threadIdx.x == 0) s_n = min(*count, max_jobs);
+    __syncthreads();
+    const uint32_t n = s_n;
+    __shared__ uint4 s_job;
+    for (uint32_t j = blockIdx.x; j < n; j += gridDim.x) {
+        if (threadIdx.x == 0) s_job = jobs[j];
+        __syncthreads();
+        copy_one<FMT>(st, s_job, pool, masks, total_slots, status);
+        __syncthreads();
+    }
+}
+
 __device__ __forceinline__ bool decode_cell(uint32_t id, int dx, int dy, int dz, uint32_t& g) {
     if (id == 0u) return false;
     const uint32_t x = ((id >> 20) & 0x3FFu) - 1u, y = ((id >> 10) & 0x3FFu) - 1u, z = (id & 0x3FFu) - 1u;
@@ -251,8 +312,8 @@ __device__ __forceinline__ uint32_t node_state(uint32_t g, const uint2* __restri
     const uint32_t blk = ((z >> 1) * ((uint32_t)dy >> 1) + (y >> 1)) * ((uint32_t)dx >> 1) + (x >> 1);
     const uint2 w = nodes[(size_t)blk * 8u + ((x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2))];
     if (w.x & 0x80000000u) {
-        // brick pointer = slot origin + border (1,1,1), 10 texels per slot
-        const uint32_t px = ((w.y >> 20) & 0x3FFu) - 1u, py = ((w.y >> 10) & 0x3FFu) - 1u, pz = (w.y & 0x3FFu) - 1u;
+        // brick pointer = slot origin + border (0..2 per axis), 10 texels per slot
+        const uint32_t px = (w.y >> 20) & 0x3FFu, py = (w.y >> 10) & 0x3FFu, pz = w.y & 0x3FFu;
         return ((pz / 10u) * (uint32_t)sy + py / 10u) * (uint32_t)sx + px / 10u;
     }
     return (w.x & 0x40000000u) ? 0xFFFFFFFFu : (0x80000000u | g);
@@ -571,6 +632,65 @@ cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs,
             break;
         case VV_FMT_FP32:
             produce_staged_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, masks, total_slots, status);
+            break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+DeviceBrickStore::~DeviceBrickStore() {
+    if (d_) cudaFree(d_);
+}
+
+cudaError_t DeviceBrickStore::upload(const uint32_t* texels, size_t bricks) {
+    if (d_) cudaFree(d_);
+    d_ = nullptr;
+    bricks_ = 0;
+    if (bricks > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    const size_t bytes = std::max<size_t>(bricks, 1) * VV_BRICK_TEXELS * sizeof(uint32_t);
+    cudaError_t e = cudaMalloc((void**)&d_, bytes);
+    if (e != cudaSuccess) {
+        d_ = nullptr;
+        return e;
+    }
+    bricks_ = bricks;
+    if (bricks) e = cudaMemcpy(d_, texels, bricks * VV_BRICK_TEXELS * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    return e;
+}
+
+cudaError_t launch_copy_bricks(const DeviceBrickStoreView& st, const uint4* jobs, int n, void* pool, int fmt,
+                               uint32_t* masks, long long total_slots, int* status, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    switch (fmt) {
+        case VV_FMT_RGBA8: copy_kernel<VV_FMT_RGBA8><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_FP16: copy_kernel<VV_FMT_FP16><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_BF16: copy_kernel<VV_FMT_BF16><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_FP32: copy_kernel<VV_FMT_FP32><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_staged(const DeviceBrickStoreView& st, const uint4* jobs, const uint32_t* count,
+                               uint32_t max_jobs, void* pool, int fmt, uint32_t* masks, long long total_slots,
+                               int* status, cudaStream_t s) {
+    if (max_jobs == 0) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned grid = (unsigned)std::min<long long>((long long)max_jobs, (long long)std::max(sms, 1) * 8);
+    switch (fmt) {
+        case VV_FMT_RGBA8:
+            copy_staged_kernel<VV_FMT_RGBA8><<<grid, 256, 0, s>>>(st, jobs, count, max_jobs, pool, masks, total_slots, status);
+            break;
+        case VV_FMT_FP16:
+            copy_staged_kernel<VV_FMT_FP16><<<grid, 256, 0, s>>>(st, jobs, count, max_jobs, pool, masks, total_slots, status);
+            break;
+        case VV_FMT_BF16:
+            copy_staged_kernel<VV_FMT_BF16><<<grid, 256, 0, s>>>(st, jobs, count, max_jobs, pool, masks, total_slots, status);
+            break;
+        case VV_FMT_FP32:
+            copy_staged_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(st, jobs, count, max_jobs, pool, masks, total_slots, status);
             break;
         default: return cudaErrorInvalidValue;
     }

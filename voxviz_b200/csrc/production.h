@@ -61,6 +61,37 @@ cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs,
                                   uint32_t max_jobs, void* pool, int fmt, uint32_t* masks, long long total_slots,
                                   int* status, cudaStream_t s);
 
+// The bricks of a tree read from files, resident in device memory: brick b
+// is the 10^3 RGBA8 block at texels + 1000 b.  Paging such a tree copies a
+// brick from here into its pool slot (a device-to-device gather) instead of
+// the host-to-PBO upload of BrickPool::uploadBrick
+// (GigaVoxelsBrickPool.cpp:729-813).
+struct DeviceBrickStoreView {
+    const uint32_t* texels;
+    uint32_t bricks;
+};
+
+class DeviceBrickStore {
+public:
+    ~DeviceBrickStore();
+    cudaError_t upload(const uint32_t* texels, size_t bricks);
+    DeviceBrickStoreView view() const { return DeviceBrickStoreView{d_, (uint32_t)bricks_}; }
+    size_t bytes() const { return bricks_ * 4000u; }
+
+private:
+    uint32_t* d_ = nullptr;
+    size_t bricks_ = 0;
+};
+
+// jobs[i] = {slot, brick, 0, 0}: copy store brick `brick` into pool slot
+// `slot`, in the pool's format, and write the slot's empty-cell mask (masks
+// may be nullptr).  The staged form reads the job count on the device.
+cudaError_t launch_copy_bricks(const DeviceBrickStoreView& st, const uint4* jobs, int n, void* pool, int fmt,
+                               uint32_t* masks, long long total_slots, int* status, cudaStream_t s);
+cudaError_t launch_copy_staged(const DeviceBrickStoreView& st, const uint4* jobs, const uint32_t* count,
+                               uint32_t max_jobs, void* pool, int fmt, uint32_t* masks, long long total_slots,
+                               int* status, cudaStream_t s);
+
 struct DedupeBuffers {
     uint32_t* first = nullptr;       // per node-pool grid cell, all 0xFFFFFFFF between calls
     size_t first_cells = 0;

@@ -64,7 +64,7 @@ void make_jitter(uint32_t seed, int size, uint8_t* out) {
     }
 }
 
-void compute_uniforms(int depth, bool root_is_constant, const vv_camera& cam, const int slots[3],
+void compute_uniforms(int depth, int leaf_dim, bool root_is_constant, const vv_camera& cam, const int slots[3],
                       float lod_scalar, float alpha_stop, vv_uniforms& u) {
     std::memset(&u, 0, sizeof(u));
     // The volume box is [0,1]^3: translation 0.5, scale 1 (:1655-1672).
@@ -82,7 +82,7 @@ void compute_uniforms(int depth, bool root_is_constant, const vv_camera& cam, co
     std::memcpy(u.camera_left, leftf, sizeof(leftf));
     // RayStepSize = getRayStepSize() * 0.5 with getRayStepSize = one leaf
     // voxel (GigaVoxelsReader.cpp:430-440; GigaVoxelsRenderer.cpp:1705).
-    const int N = 8 << depth;
+    const int N = leaf_dim > 0 ? leaf_dim : 8 << depth;
     const float leaf = (1.0f / (float)N) / (1.0f - 0.0f);
     const float rs = leaf * 0.5f;
     u.ray_step_size = rs;
@@ -202,8 +202,13 @@ int GigaVoxelsRenderer::init() {
     touch_seen_.assign(total_slots_, 0u);
     if (d_.device_paging) {
         device_paging_ = true;
-        dterrain_ = std::make_unique<DeviceTerrain>();
-        if (dterrain_->upload(tree_->volume()) != cudaSuccess) return VV_ERR_OOM;
+        if (tree_->file_backed()) {
+            dstore_ = std::make_unique<DeviceBrickStore>();
+            if (dstore_->upload(tree_->file_texels(), tree_->file_brick_count()) != cudaSuccess) return VV_ERR_OOM;
+        } else {
+            dterrain_ = std::make_unique<DeviceTerrain>();
+            if (dterrain_->upload(tree_->volume()) != cudaSuccess) return VV_ERR_OOM;
+        }
         const int* g = tree_->pool_dim();
         dd_.first_cells = (size_t)g[0] * g[1] * g[2];
         if (cudaMalloc((void**)&dd_.first, dd_.first_cells * 4) != cudaSuccess) return VV_ERR_OOM;
@@ -288,7 +293,8 @@ int GigaVoxelsRenderer::draw(const vv_camera& cam) {
         copy_pending_[cur_color_] = false;
     }
     d_color = color_buf_[cur_color_];
-    compute_uniforms(tree_->depth(), tree_->is_constant(0), cam, slots_, d_.lod_scalar, d_.alpha_stop, last_u_);
+    compute_uniforms(tree_->depth(), tree_->leaf_dim(), tree_->is_constant(0), cam, slots_, d_.lod_scalar,
+                     d_.alpha_stop, last_u_);
     vv_frame_out o;
     std::memset(&o, 0, sizeof(o));
     o.color = d_color;
@@ -437,6 +443,16 @@ int GigaVoxelsRenderer::evict_front(uint32_t& s) {
     return VV_OK;
 }
 
+// The device production job of node `node` into slot `slot`: the terrain
+// node's level and brick index, or the file tree's store brick.
+uint4 GigaVoxelsRenderer::production_job(uint32_t slot, uint32_t node) const {
+    if (tree_->file_backed()) return make_uint4(slot, (uint32_t)tree_->file_brick(node), 0u, 0u);
+    int ci, cj, ck;
+    tree_->origin(node, ci, cj, ck);
+    return make_uint4(slot, (uint32_t)tree_->level(node), ((uint32_t)ci << 20) | ((uint32_t)cj << 10) | (uint32_t)ck,
+                      0u);
+}
+
 int GigaVoxelsRenderer::upload_nodes(uint32_t n) {
     // BrickPool::update body (GigaVoxelsBrickPool.cpp:583-629): evict the
     // LRU front, upload into its slot, move it to the back.
@@ -459,7 +475,9 @@ int GigaVoxelsRenderer::upload_nodes(uint32_t n) {
     const uint32_t sx = s % (uint32_t)slots_[0], sy = (s / (uint32_t)slots_[0]) % (uint32_t)slots_[1],
                    sz = s / ((uint32_t)slots_[0] * (uint32_t)slots_[1]);
     // uploadBrick (:800-810): pointer = slot origin + border
-    w1_[n] = pack10(sx * 10 + 1, sy * 10 + 1, sz * 10 + 1);
+    uint32_t b[3];
+    tree_->brick_border(n, b);
+    w1_[n] = pack10(sx * 10 + b[0], sy * 10 + b[1], sz * 10 + b[2]);
     w0_[n] |= kBrickResidentBit;
     if (!touched_mark_[n]) {
         touched_mark_[n] = 1;
@@ -583,11 +601,8 @@ int GigaVoxelsRenderer::flush_device() {
         if (cudaHostGetDevicePointer((void**)&dh_fpatch_, h_fpatch_, 0) != cudaSuccess) return VV_ERR_CUDA;
     }
     for (size_t k = 0; k < n; ++k) {
-        const uint32_t i = keep_[k], node = pending_nodes_[i];
-        int ci, cj, ck;
-        tree_->origin(node, ci, cj, ck);
-        h_fjobs_[k] = make_uint4(pending_slots_[i], (uint32_t)tree_->level(node),
-                                 ((uint32_t)ci << 20) | ((uint32_t)cj << 10) | (uint32_t)ck, 0u);
+        const uint32_t i = keep_[k];
+        h_fjobs_[k] = production_job(pending_slots_[i], pending_nodes_[i]);
     }
     for (size_t k = 0; k < np; ++k) {
         const uint32_t t = touched_[k];
@@ -605,9 +620,10 @@ int GigaVoxelsRenderer::flush_device() {
     if (launch_pull(dh_fjobs_, d_fjobs_, n, (const uint4*)dh_fpatch_, (uint4*)d_fpatch_, patch_words,
                     ctx_->stream) != cudaSuccess ||
         cudaEventRecord(ev_flush_, ctx_->stream) != cudaSuccess ||
-        launch_produce_bricks(dterrain_->view(), d_fjobs_, (int)n, pool, d_.fmt, ctx_cell_mask_rw(ctx_),
-                              (long long)total_slots_,
-                              ctx_->d_status, ctx_->stream) != cudaSuccess ||
+        (dstore_ ? launch_copy_bricks(dstore_->view(), d_fjobs_, (int)n, pool, d_.fmt, ctx_cell_mask_rw(ctx_),
+                                      (long long)total_slots_, ctx_->d_status, ctx_->stream)
+                 : launch_produce_bricks(dterrain_->view(), d_fjobs_, (int)n, pool, d_.fmt, ctx_cell_mask_rw(ctx_),
+                                         (long long)total_slots_, ctx_->d_status, ctx_->stream)) != cudaSuccess ||
         launch_node_patch(d_fpatch_, (int)np, t.nodes, t.dim, ctx_->d_status, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
     touched_.clear();
@@ -891,11 +907,7 @@ int GigaVoxelsRenderer::stage_uploads() {
     uint32_t nj = 0;
     for (size_t k = keep.size(); k-- > 0;) {  // back to first-seen order
         const uint32_t i = keep[k];
-        const uint32_t node = pending_nodes_[i];
-        int ci, cj, ck;
-        tree_->origin(node, ci, cj, ck);
-        h_def_jobs_[nj++] = make_uint4(pending_slots_[i], (uint32_t)tree_->level(node),
-                                       ((uint32_t)ci << 20) | ((uint32_t)cj << 10) | (uint32_t)ck, 0u);
+        h_def_jobs_[nj++] = production_job(pending_slots_[i], pending_nodes_[i]);
     }
     uint32_t np = 0;
     for (uint32_t t : touched_) {
@@ -930,9 +942,12 @@ int GigaVoxelsRenderer::enqueue_uploads() {
     if (launch_pull_staged(counts, jobs, def_job_cap_, patches, def_patch_cap_, d_def_counts_, d_def_jobs_,
                            d_def_patches_, ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
-    if (launch_produce_staged(dterrain_->view(), d_def_jobs_, d_def_counts_, def_job_cap_, pool, d_.fmt,
-                              ctx_cell_mask_rw(ctx_), (long long)total_slots_, ctx_->d_status, ctx_->stream) != cudaSuccess)
-        return VV_ERR_CUDA;
+    const cudaError_t pe =
+        dstore_ ? launch_copy_staged(dstore_->view(), d_def_jobs_, d_def_counts_, def_job_cap_, pool, d_.fmt,
+                                     ctx_cell_mask_rw(ctx_), (long long)total_slots_, ctx_->d_status, ctx_->stream)
+                : launch_produce_staged(dterrain_->view(), d_def_jobs_, d_def_counts_, def_job_cap_, pool, d_.fmt,
+                                        ctx_cell_mask_rw(ctx_), (long long)total_slots_, ctx_->d_status, ctx_->stream);
+    if (pe != cudaSuccess) return VV_ERR_CUDA;
     const DeviceTree& t = ctx_->trees[0];
     if (launch_node_patch_staged(d_def_patches_, d_def_counts_ + 1, def_patch_cap_, t.nodes, t.dim, ctx_->d_status,
                                  ctx_->stream) != cudaSuccess)

@@ -13,8 +13,9 @@
 namespace vv {
 
 // GigaVoxelsRenderer::drawVolume uniform derivation
-// (GigaVoxelsRenderer.cpp:1630-1816) for a volume box [0,1]^3.
-void compute_uniforms(int depth, bool root_is_constant, const vv_camera& cam, const int slots[3],
+// (GigaVoxelsRenderer.cpp:1630-1816) for a volume box [0,1]^3; leaf_dim is
+// the voxel count per axis the ray step is one voxel of (8 << depth when 0).
+void compute_uniforms(int depth, int leaf_dim, bool root_is_constant, const vv_camera& cam, const int slots[3],
                       float lod_scalar, float alpha_stop, vv_uniforms& u);
 // Camera::getPixelSize (Camera.cpp:128-196) restated without GLU.
 float camera_pixel_size(const vv_camera& cam);
@@ -117,6 +118,8 @@ private:
     // device-side service
     bool device_paging_ = false;
     std::unique_ptr<DeviceTerrain> dterrain_;
+    std::unique_ptr<DeviceBrickStore> dstore_;  // file trees: every brick in device memory
+    uint4 production_job(uint32_t slot, uint32_t node) const;
     DedupeBuffers dd_;
     // Read-backs of the service go to mapped pinned memory, written by
     // kernels (dh_* are the device views), so that they do not wait behind
