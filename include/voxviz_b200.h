@@ -484,6 +484,7 @@ typedef struct vv_gvp_info {
 int vv_gvp_read(const char* path, vv_gvp_info* info, vv_gvp_tile* tiles, int32_t cap);
 int vv_gvp_write(const char* path, const vv_gvp_info* info, const vv_gvp_tile* tiles, int32_t n);
 
+
 /* ---- camera + uniform derivation ---------------------------------------- */
 
 /* vox::Camera essentials (VoxVizCore/Camera.h). */
@@ -606,6 +607,73 @@ int vv_renderer_residency(const vv_renderer* r, uint32_t* out_xyz,
 /* Uniforms of the last draw. */
 int vv_renderer_last_uniforms(const vv_renderer* r, vv_uniforms* out);
 vv_ctx* vv_renderer_ctx(vv_renderer* r);
+
+/* ---- paged scenes: the tiles of a .gvp ------------------------------------
+ * The reference's paged-scene path: each frame the cull visitor
+ * (GigaVoxelsRenderer.cpp:667-798) tests every tile's bounding sphere
+ * against the camera frustum (vox::Frustum, VoxVizCore/Frustum.cpp), stamps
+ * visible tiles with the frame, requests loads of visible unloaded tiles
+ * from the pager and lists the loaded ones farthest first (distance of the
+ * centre to the near plane minus the radius); the list is drawn in order and
+ * each tile blended over the colour with GL_SRC_ALPHA, GL_ONE_MINUS_SRC_ALPHA
+ * (:997-1090).  The pager (GigaVoxelsDatabasePager.cpp) loads requests
+ * sorted by last access (latest first) then distance (nearest first), merges
+ * loaded trees at the next update and unloads tiles unseen for more than
+ * stale_frames frames.  Each loaded tile is drawn by its own renderer (own
+ * context, brick pool of pool_bytes_per_tile and LRU; the reference shares
+ * one brick pool), with the camera mapped into the tile's box as drawVolume
+ * maps it (the box must be a cube). */
+typedef struct vv_scene vv_scene;
+enum {
+    VV_SCENE_HOST_ONLY = 1,    /* cull and page trees on the host; no drawing */
+    VV_SCENE_SYNCHRONOUS = 2   /* loads run inside vv_scene_update (no pager thread) */
+};
+typedef struct vv_scene_desc {
+    int32_t fmt;                  /* brick pool format of every tile */
+    int64_t pool_bytes_per_tile;  /* 0: every brick of a tile fits */
+    int32_t request_cap;          /* per tile (0: no cap) */
+    float lod_scalar;             /* 0: 1.0 */
+    float alpha_stop;             /* 0: 0.99 */
+    uint32_t jitter_seed;
+    int32_t device_paging;
+    int32_t load_flags;           /* VV_GVX_* for every tile */
+    int32_t stale_frames;         /* 0: 100, the reference's */
+    float far_dist;               /* camera far plane; 0: 10000, vox::Camera's */
+    int32_t flags;                /* VV_SCENE_* */
+    int32_t reserved[4];
+} vv_scene_desc;
+typedef struct vv_scene_tile_state {
+    int32_t loaded;               /* merged: drawn when visible */
+    int32_t pending;              /* requested or loaded, not merged yet */
+    int32_t visible;              /* inside the frustum at the last draw */
+    int32_t drawn_order;          /* position in the last render list, -1 */
+    int32_t failed;               /* its tree could not be loaded (not retried) */
+    float dist_to_near_plane;     /* last draw; minus the radius when drawn */
+    int64_t last_access;          /* frame of the last draw that saw it */
+} vv_scene_tile_state;
+typedef struct vv_scene_stats {
+    int32_t tiles, loaded, pending, drawn;
+    int64_t loads, unloads, load_failures;
+    float load_ms_avg, load_ms_max;
+} vv_scene_stats;
+/* ctx: the context the scene's colour lives in (NULL with VV_SCENE_HOST_ONLY). */
+int vv_scene_create(vv_ctx* ctx, const char* gvp_path, const vv_scene_desc* desc, vv_scene** out);
+void vv_scene_destroy(vv_scene* scene);
+/* Renderer::draw: cull, request loads, draw and blend.  The camera is in
+ * world coordinates (the .gvp's and the trees' units). */
+int vv_scene_draw(vv_scene* scene, const vv_camera* world_camera);
+/* Renderer::update: merge loaded trees, unload stale tiles, then the
+ * page-request service of every tile drawn by the last draw. */
+int vv_scene_update(vv_scene* scene);
+/* Block until the pager has no request left (loads still to be merged by
+ * the next update). */
+int vv_scene_wait_loads(vv_scene* scene);
+int vv_scene_read_color(vv_scene* scene, float* host_rgba);
+int vv_scene_tile_states(const vv_scene* scene, vv_scene_tile_state* out, int32_t cap);
+int vv_scene_get_stats(const vv_scene* scene, vv_scene_stats* out);
+/* The renderer of a loaded tile, owned by the scene (NULL otherwise); its
+ * colour is the tile's FragColor before blending. */
+vv_renderer* vv_scene_tile_renderer(vv_scene* scene, int32_t tile);
 
 #ifdef __cplusplus
 }

@@ -14,6 +14,8 @@ The objects mirror the reference's host API:
   (node pool: GigaVoxelsOctTreeNodePool.h, brick pool: GigaVoxelsBrickPool.h)
 * :class:`Renderer` - the ``"gv"`` ``vox::Renderer`` frame protocol
   (VoxViz/VoxVizCore/Renderer.h:20-110, GigaVoxelsRenderer.cpp)
+* :class:`Scene` - a paged scene of ``.gvx`` tiles listed by a ``.gvp``
+  (the cull visitor of GigaVoxelsRenderer.cpp and GigaVoxelsDatabasePager)
 """
 from __future__ import annotations
 
@@ -27,8 +29,8 @@ from ._native import (FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_FP16, VV_FMT_F
                       VV_PASS_ALL, VV_PASS_COMPACT, VV_PASS_RAYCAST, VV_PASS_SELECT, Camera, FrameOut,
                       NodePatch, OctreeInfo, Uniforms, VVError)
 
-__all__ = ["Octree", "Context", "Renderer", "Batch", "batch_variants", "make_camera", "look_at", "read_gvp",
-           "write_gvp",
+__all__ = ["Octree", "Context", "Renderer", "Batch", "Scene", "batch_variants", "make_camera", "look_at",
+           "read_gvp", "write_gvp",
            "compute_uniforms", "make_jitter", "pixel_size", "lib", "VVError", "Uniforms", "Camera", "FMT_NAMES",
            "TEXEL_BYTES"]
 
@@ -570,3 +572,88 @@ class Renderer:
         u = Uniforms()
         self._ck(lib().vv_renderer_last_uniforms(self._h, C.byref(u)), "uniforms")
         return u
+
+
+class _CtxRef:
+    def __init__(self, handle):
+        self.handle = C.c_void_p(handle)
+
+
+class _TileRenderer(Renderer):
+    """A loaded tile's renderer, owned by its scene."""
+
+    def __init__(self, handle: int, scene: "Scene"):
+        self._h = C.c_void_p(handle)
+        self.ctx = _CtxRef(lib().vv_renderer_ctx(self._h))
+        self._scene = scene
+
+    def close(self) -> None:
+        self._h = C.c_void_p()
+
+
+class Scene:
+    """Paged tiles of a .gvp: frustum culling, pager, back-to-front blending
+    (``vv_scene_*``).  Cameras are in world coordinates."""
+
+    def __init__(self, ctx: Context | None, gvp_path, fmt="rgba8", pool_bytes_per_tile: int = 0,
+                 request_cap: int = 0, lod_scalar: float = 1.0, alpha_stop: float = 0.99, jitter_seed: int = 7,
+                 device_paging: bool = False, constant_colors: bool = False, gradients: bool = True,
+                 stale_frames: int = 100, far_dist: float = 10000.0, host_only: bool = False,
+                 synchronous: bool = False):
+        d = N.SceneDesc(fmt=fmt_code(fmt), pool_bytes_per_tile=pool_bytes_per_tile, request_cap=request_cap,
+                        lod_scalar=lod_scalar, alpha_stop=alpha_stop, jitter_seed=jitter_seed,
+                        device_paging=1 if device_paging else 0,
+                        load_flags=(N.VV_GVX_CONSTANT_COLORS if constant_colors else 0)
+                        | (0 if gradients else N.VV_GVX_SKIP_GRADIENTS),
+                        stale_frames=stale_frames, far_dist=far_dist,
+                        flags=(N.VV_SCENE_HOST_ONLY if host_only else 0) | (N.VV_SCENE_SYNCHRONOUS if synchronous else 0))
+        h = C.c_void_p()
+        ch = ctx.handle if ctx is not None else None
+        _check(lib().vv_scene_create(ch, str(gvp_path).encode(), C.byref(d), C.byref(h)), ch, "scene create")
+        self._h = h
+        self.ctx = ctx
+        self._size = None
+
+    def close(self) -> None:
+        if self._h:
+            lib().vv_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc: int, what: str) -> None:
+        _check(rc, self.ctx.handle if self.ctx is not None else None, what)
+
+    def draw(self, cam: Camera) -> None:
+        self._size = (cam.height, cam.width)
+        self._ck(lib().vv_scene_draw(self._h, C.byref(cam)), "scene draw")
+
+    def update(self) -> None:
+        self._ck(lib().vv_scene_update(self._h), "scene update")
+
+    def wait_loads(self) -> None:
+        self._ck(lib().vv_scene_wait_loads(self._h), "scene wait loads")
+
+    def read_color(self) -> np.ndarray:
+        out = np.zeros(self._size + (4,), dtype=np.float32)
+        self._ck(lib().vv_scene_read_color(self._h, _ptr(out)), "scene read color")
+        return out
+
+    def tile_states(self) -> list[dict]:
+        n = self.stats()["tiles"]
+        arr = (N.SceneTileState * max(n, 1))()
+        self._ck(lib().vv_scene_tile_states(self._h, arr, n), "scene tile states")
+        return [{f: getattr(t, f) for f, _ in N.SceneTileState._fields_} for t in arr[:n]]
+
+    def stats(self) -> dict:
+        s = N.SceneStats()
+        self._ck(lib().vv_scene_get_stats(self._h, C.byref(s)), "scene stats")
+        return {f: getattr(s, f) for f, _ in N.SceneStats._fields_}
+
+    def tile_renderer(self, tile: int) -> Renderer | None:
+        h = lib().vv_scene_tile_renderer(self._h, tile)
+        return _TileRenderer(h, self) if h else None

@@ -13,6 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libvoxviz_b200.so"
 
 VV_OK, VV_ERR_ARG, VV_ERR_OOM, VV_ERR_CUDA, VV_ERR_TIMEOUT, VV_ERR_BOUNDS, VV_ERR_STATE, VV_ERR_NODEV, VV_ERR_IO = range(9)
 VV_GVX_CONSTANT_COLORS, VV_GVX_SKIP_GRADIENTS = 1, 2
+VV_SCENE_HOST_ONLY, VV_SCENE_SYNCHRONOUS = 1, 2
 VV_FMT_RGBA8, VV_FMT_FP16, VV_FMT_BF16, VV_FMT_FP32 = range(4)
 VV_PASS_RAYCAST, VV_PASS_SELECT, VV_PASS_COMPACT, VV_PASS_ALL = 1, 2, 4, 7
 FMT_NAMES = {"rgba8": VV_FMT_RGBA8, "fp16": VV_FMT_FP16, "bf16": VV_FMT_BF16, "fp32": VV_FMT_FP32}
@@ -131,6 +132,43 @@ class GvpInfo(C.Structure):
         ("tiles", C.c_int32),
         ("sphere_center", C.c_float * 3),
         ("sphere_radius", C.c_double),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("fmt", C.c_int32),
+        ("pool_bytes_per_tile", C.c_int64),
+        ("request_cap", C.c_int32),
+        ("lod_scalar", C.c_float),
+        ("alpha_stop", C.c_float),
+        ("jitter_seed", C.c_uint32),
+        ("device_paging", C.c_int32),
+        ("load_flags", C.c_int32),
+        ("stale_frames", C.c_int32),
+        ("far_dist", C.c_float),
+        ("flags", C.c_int32),
+        ("reserved", C.c_int32 * 4),
+    ]
+
+
+class SceneTileState(C.Structure):
+    _fields_ = [
+        ("loaded", C.c_int32),
+        ("pending", C.c_int32),
+        ("visible", C.c_int32),
+        ("drawn_order", C.c_int32),
+        ("failed", C.c_int32),
+        ("dist_to_near_plane", C.c_float),
+        ("last_access", C.c_int64),
+    ]
+
+
+class SceneStats(C.Structure):
+    _fields_ = [
+        ("tiles", C.c_int32), ("loaded", C.c_int32), ("pending", C.c_int32), ("drawn", C.c_int32),
+        ("loads", C.c_int64), ("unloads", C.c_int64), ("load_failures", C.c_int64),
+        ("load_ms_avg", C.c_float), ("load_ms_max", C.c_float),
     ]
 
 
@@ -266,6 +304,15 @@ SIGNATURES = {
     "vv_octree_gvx_info": (C.c_int, [P, C.POINTER(GvxInfo)]),
     "vv_gvp_read": (C.c_int, [C.c_char_p, C.POINTER(GvpInfo), C.POINTER(GvpTile), C.c_int32]),
     "vv_gvp_write": (C.c_int, [C.c_char_p, C.POINTER(GvpInfo), C.POINTER(GvpTile), C.c_int32]),
+    "vv_scene_create": (C.c_int, [P, C.c_char_p, C.POINTER(SceneDesc), C.POINTER(P)]),
+    "vv_scene_destroy": (None, [P]),
+    "vv_scene_draw": (C.c_int, [P, C.POINTER(Camera)]),
+    "vv_scene_update": (C.c_int, [P]),
+    "vv_scene_wait_loads": (C.c_int, [P]),
+    "vv_scene_read_color": (C.c_int, [P, P]),
+    "vv_scene_tile_states": (C.c_int, [P, C.POINTER(SceneTileState), C.c_int32]),
+    "vv_scene_get_stats": (C.c_int, [P, C.POINTER(SceneStats)]),
+    "vv_scene_tile_renderer": (P, [P, C.c_int32]),
     "vv_compute_uniforms": (C.c_int, [C.POINTER(OctreeInfo), C.POINTER(Camera), C.c_int32, C.c_int32, C.c_int32,
                                       C.c_float, C.c_float, C.POINTER(Uniforms)]),
     "vv_camera_pixel_size": (C.c_float, [C.POINTER(Camera)]),

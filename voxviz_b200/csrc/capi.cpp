@@ -9,17 +9,14 @@
 
 #include "ctx.h"
 #include "gvfile.h"
+#include "handles.h"
 #include "octree.h"
 #include "renderer.h"
+#include "scene.h"
 
-struct vv_octree {
-    std::shared_ptr<const vv::TerrainVolume> volume;
-    std::unique_ptr<vv::GigaVoxelsOctTree> tree;
-};
 
-struct vv_renderer {
-    std::unique_ptr<vv::GigaVoxelsRenderer> impl;
-    vv_ctx* ctx = nullptr;
+struct vv_scene {
+    std::unique_ptr<vv::PagedScene> impl;
 };
 
 extern "C" {
@@ -276,6 +273,72 @@ int vv_gvp_write(const char* path, const vv_gvp_info* info, const vv_gvp_tile* t
     }
     return VV_OK;
 }
+
+int vv_scene_create(vv_ctx* ctx, const char* gvp_path, const vv_scene_desc* d, vv_scene** out) {
+    if (!gvp_path || !d || !out) return VV_ERR_ARG;
+    *out = nullptr;
+    if (!ctx && !(d->flags & VV_SCENE_HOST_ONLY)) {
+        vv::set_thread_error("vv_scene_create: a context is required unless VV_SCENE_HOST_ONLY");
+        return VV_ERR_ARG;
+    }
+    if (!(d->flags & VV_SCENE_HOST_ONLY) && !vv::texel_bytes(d->fmt)) return VV_ERR_ARG;
+    try {
+        vv::GvpFile f;
+        std::string err;
+        const int rc = vv::read_gvp(gvp_path, f, err);
+        if (rc) {
+            vv::set_thread_error(err);
+            return rc;
+        }
+        auto sc = std::make_unique<vv_scene>();
+        sc->impl = std::make_unique<vv::PagedScene>(ctx, std::move(f), *d);
+        const int r = sc->impl->init();
+        if (r) return r;
+        *out = sc.release();
+        return VV_OK;
+    } catch (const std::bad_alloc&) {
+        return VV_ERR_OOM;
+    } catch (const std::exception& e) {
+        vv::set_thread_error(std::string("vv_scene_create: ") + e.what());
+        return VV_ERR_ARG;
+    }
+}
+
+void vv_scene_destroy(vv_scene* s) { delete s; }
+
+int vv_scene_draw(vv_scene* s, const vv_camera* cam) {
+    if (!s || !cam) return VV_ERR_ARG;
+    return s->impl->draw(*cam);
+}
+
+int vv_scene_update(vv_scene* s) {
+    if (!s) return VV_ERR_ARG;
+    return s->impl->update();
+}
+
+int vv_scene_wait_loads(vv_scene* s) {
+    if (!s) return VV_ERR_ARG;
+    return s->impl->wait_loads();
+}
+
+int vv_scene_read_color(vv_scene* s, float* host_rgba) {
+    if (!s || !host_rgba) return VV_ERR_ARG;
+    return s->impl->read_color(host_rgba);
+}
+
+int vv_scene_tile_states(const vv_scene* s, vv_scene_tile_state* out, int32_t cap) {
+    if (!s || cap < 0 || (cap > 0 && !out)) return VV_ERR_ARG;
+    s->impl->tile_states(out, cap);
+    return VV_OK;
+}
+
+int vv_scene_get_stats(const vv_scene* s, vv_scene_stats* out) {
+    if (!s || !out) return VV_ERR_ARG;
+    s->impl->stats(*out);
+    return VV_OK;
+}
+
+vv_renderer* vv_scene_tile_renderer(vv_scene* s, int32_t tile) { return s ? s->impl->tile_renderer(tile) : nullptr; }
 
 int vv_compute_uniforms(const vv_octree_info* tree, const vv_camera* cam, int32_t sx, int32_t sy, int32_t sz,
                         float lod_scalar, float alpha_stop, vv_uniforms* out) {

@@ -71,6 +71,9 @@ cudaError_t launch_node_patch(const vv_node_patch* patches, int n, uint2* nodes,
 cudaError_t launch_brick_scatter(const uint32_t* slots, int n, const void* src, void* pool,
                                  size_t brick_bytes, long long total_slots, int* status,
                                  cudaStream_t s);
+// glBlendFunc(GL_SRC_ALPHA, GL_ONE_MINUS_SRC_ALPHA) of one tile's colour
+// over the scene's, per channel in FP32: dst = src * src.a + dst * (1 - src.a).
+cudaError_t launch_blend_over(float4* dst, const float4* src, size_t n, cudaStream_t s);
 // Empty-cell masks (cellmask.cuh) of n slots (slots[i], or slot i when slots
 // is null) from the pool's current contents: 32 words per slot.
 cudaError_t launch_cell_masks(const uint32_t* slots, long long n, const void* pool, int fmt, long long total_slots,
