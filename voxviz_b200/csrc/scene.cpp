@@ -134,6 +134,7 @@ void PagedScene::load_requests(std::vector<Request>& reqs) {
         SceneTile& s = *tiles_[r.tile];
         {
             std::lock_guard<std::mutex> lock(mu_);
+            if (done_) break;          // the scene is being destroyed
             if (s.tree || s.loaded) {  // loaded already
                 s.on_request_list = false;
                 continue;
@@ -220,7 +221,10 @@ int PagedScene::merge_handled() {
         const int r = attach_tile(s);
         if (r) {
             s.load_failed = true;
-            s.error = "could not create the tile's renderer";
+            {
+                std::lock_guard<std::mutex> lock(mu_);
+                if (s.error.empty()) s.error = "could not create the tile's renderer";
+            }
             release_tile(s);
             if (!rc) rc = r;
             continue;
@@ -254,6 +258,7 @@ int PagedScene::attach_tile(SceneTile& s) {
     if (host_only_) return VV_OK;
     const float sx = s.box_max[0] - s.box_min[0], sy = s.box_max[1] - s.box_min[1], sz = s.box_max[2] - s.box_min[2];
     if (!(sx > 0.0f) || std::fabs(sy - sx) > 1e-5f * sx || std::fabs(sz - sx) > 1e-5f * sx) {
+        std::lock_guard<std::mutex> lock(mu_);
         s.error = "the tile's box is not a cube";
         return VV_ERR_ARG;
     }
@@ -290,7 +295,11 @@ void PagedScene::release_tile(SceneTile& s) {
     s.drawn = nullptr;
     if (s.ctx) vv_ctx_destroy(s.ctx);
     s.ctx = nullptr;
-    s.tree.reset();
+    std::unique_ptr<vv_octree> gone;
+    {
+        std::lock_guard<std::mutex> lock(mu_);
+        gone = std::move(s.tree);
+    }
 }
 
 // drawVolume's volume transform (GigaVoxelsRenderer.cpp:1655-1690): the
@@ -408,7 +417,7 @@ vv_renderer* PagedScene::tile_renderer(int t) {
 }
 
 void PagedScene::tile_states(vv_scene_tile_state* out, int cap) const {
-    std::lock_guard<std::mutex> lock(const_cast<std::mutex&>(mu_));
+    std::lock_guard<std::mutex> lock(mu_);
     for (int i = 0; i < cap && (size_t)i < tiles_.size(); ++i) {
         const SceneTile& s = *tiles_[(size_t)i];
         vv_scene_tile_state& o = out[i];
@@ -424,7 +433,7 @@ void PagedScene::tile_states(vv_scene_tile_state* out, int cap) const {
 }
 
 void PagedScene::stats(vv_scene_stats& st) const {
-    std::lock_guard<std::mutex> lock(const_cast<std::mutex&>(mu_));
+    std::lock_guard<std::mutex> lock(mu_);
     std::memset(&st, 0, sizeof(st));
     st.tiles = (int32_t)tiles_.size();
     for (const auto& t : tiles_) {
@@ -442,6 +451,7 @@ void PagedScene::stats(vv_scene_stats& st) const {
 
 std::string PagedScene::tile_error(int t) const {
     if (t < 0 || (size_t)t >= tiles_.size()) return std::string();
+    std::lock_guard<std::mutex> lock(mu_);
     return tiles_[(size_t)t]->error;
 }
 

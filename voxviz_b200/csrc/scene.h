@@ -46,10 +46,11 @@ struct Frustum {
 struct SceneTile {
     GvpTile info;
     std::atomic<uint64_t> last_access{0};   // PagedOctTreeNode::m_lastAccessFrameIndex
-    bool on_request_list = false;           // guarded by the scene's mutex
-    bool load_failed = false;
+    // guarded by the scene's mutex (the pager thread reads or writes them)
+    bool on_request_list = false;
+    std::atomic<bool> load_failed{false};
     std::string error;
-    std::unique_ptr<vv_octree> tree;        // merged (drawable) tree
+    std::unique_ptr<vv_octree> tree;        // merged (drawable) tree; set and reset under the mutex
     std::unique_ptr<vv_octree> loaded;      // loaded by the pager, not merged yet
     vv_ctx* ctx = nullptr;                  // the tile's device context and renderer
     std::unique_ptr<vv_renderer> renderer;
@@ -103,7 +104,7 @@ private:
     bool blended_once_ = false;
     bool host_only_ = false;
     // pager
-    std::mutex mu_;
+    mutable std::mutex mu_;
     std::condition_variable cv_, idle_cv_;
     std::vector<Request> requests_;
     std::vector<size_t> handled_;
