@@ -626,7 +626,9 @@ vv_ctx* vv_renderer_ctx(vv_renderer* r);
 typedef struct vv_scene vv_scene;
 enum {
     VV_SCENE_HOST_ONLY = 1,    /* cull and page trees on the host; no drawing */
-    VV_SCENE_SYNCHRONOUS = 2   /* loads run inside vv_scene_update (no pager thread) */
+    VV_SCENE_SYNCHRONOUS = 2,  /* loads run inside vv_scene_update (no pager thread) */
+    VV_SCENE_BATCHED = 4       /* the drawn tiles' ray casts as one batched launch
+                                  (vv_render_batch); results are the same */
 };
 typedef struct vv_scene_desc {
     int32_t fmt;                  /* brick pool format of every tile */

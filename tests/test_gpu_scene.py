@@ -101,3 +101,31 @@ def test_scene_blends_tiles_in_render_order(tiles, device_paging):
     assert st["loads"] == 4 and st["load_failures"] == 0
     assert drawn_total > 24 and len(orders) > 2 and solo_frames > 3
     assert np.abs(colour).sum() > 0
+
+
+def test_batched_scene_matches_per_tile_launches(tiles):
+    """VV_SCENE_BATCHED: the drawn tiles' ray casts as one persistent launch
+    give the same scene colour and the same page requests per tile."""
+    gvp, info = tiles
+    out = []
+    for batched in (False, True):
+        ctx = vv.Context(0)
+        sc = vv.Scene(ctx, gvp, pool_bytes_per_tile=300 * 1000 * 4, synchronous=True, device_paging=True,
+                      constant_colors=True, batched=batched)
+        frames = []
+        for cam in _path(16):
+            sc.draw(cam)
+            colour = sc.read_color()
+            sc.update()
+            drawn = [i for i, s in enumerate(sc.tile_states()) if s["drawn_order"] >= 0]
+            frames.append((colour, {i: sc.tile_renderer(i).last_requests() for i in drawn}))
+        assert ctx.device_status() == 0
+        out.append(frames)
+    multi = 0
+    for k, ((c0, r0), (c1, r1)) in enumerate(zip(*out)):
+        assert np.array_equal(c0, c1), f"colour differs at frame {k}"
+        assert r0.keys() == r1.keys()
+        for i in r0:
+            assert np.array_equal(r0[i], r1[i]), f"tile {i} requests differ at frame {k}"
+        multi += len(r0) > 1
+    assert multi > 3

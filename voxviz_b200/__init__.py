@@ -599,14 +599,15 @@ class Scene:
                  request_cap: int = 0, lod_scalar: float = 1.0, alpha_stop: float = 0.99, jitter_seed: int = 7,
                  device_paging: bool = False, constant_colors: bool = False, gradients: bool = True,
                  stale_frames: int = 100, far_dist: float = 10000.0, host_only: bool = False,
-                 synchronous: bool = False):
+                 synchronous: bool = False, batched: bool = False):
         d = N.SceneDesc(fmt=fmt_code(fmt), pool_bytes_per_tile=pool_bytes_per_tile, request_cap=request_cap,
                         lod_scalar=lod_scalar, alpha_stop=alpha_stop, jitter_seed=jitter_seed,
                         device_paging=1 if device_paging else 0,
                         load_flags=(N.VV_GVX_CONSTANT_COLORS if constant_colors else 0)
                         | (0 if gradients else N.VV_GVX_SKIP_GRADIENTS),
                         stale_frames=stale_frames, far_dist=far_dist,
-                        flags=(N.VV_SCENE_HOST_ONLY if host_only else 0) | (N.VV_SCENE_SYNCHRONOUS if synchronous else 0))
+                        flags=(N.VV_SCENE_HOST_ONLY if host_only else 0) | (N.VV_SCENE_SYNCHRONOUS if synchronous else 0)
+                        | (N.VV_SCENE_BATCHED if batched else 0))
         h = C.c_void_p()
         ch = ctx.handle if ctx is not None else None
         _check(lib().vv_scene_create(ch, str(gvp_path).encode(), C.byref(d), C.byref(h)), ch, "scene create")

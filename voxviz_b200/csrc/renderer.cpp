@@ -282,6 +282,12 @@ int GigaVoxelsRenderer::alloc_frame(int w, int h) {
 }
 
 int GigaVoxelsRenderer::draw(const vv_camera& cam) {
+    const int rc = prepare_draw(cam);
+    if (rc) return rc;
+    return finish_draw(VV_PASS_ALL);
+}
+
+int GigaVoxelsRenderer::prepare_draw(const vv_camera& cam) {
     int rc = start_readback();  // a read-back requested without a service since
     if (rc) return rc;
     rc = alloc_frame(cam.width, cam.height);
@@ -295,6 +301,12 @@ int GigaVoxelsRenderer::draw(const vv_camera& cam) {
     d_color = color_buf_[cur_color_];
     compute_uniforms(tree_->depth(), tree_->leaf_dim(), tree_->is_constant(0), cam, slots_, d_.lod_scalar,
                      d_.alpha_stop, last_u_);
+    frame_ = cam.frame;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::finish_draw(int passes) {
+    if (!d_color) return VV_ERR_STATE;
     vv_frame_out o;
     std::memset(&o, 0, sizeof(o));
     o.color = d_color;
@@ -303,9 +315,8 @@ int GigaVoxelsRenderer::draw(const vv_camera& cam) {
     o.requests = d_requests;
     o.request_count = d_count;
     o.request_cap = cap_;
-    o.compress_max_push = 4 * ((cam.frame % 3) + 1);  // (GigaVoxelsRenderer.cpp:2093-2098)
-    o.passes = VV_PASS_ALL;
-    frame_ = cam.frame;
+    o.compress_max_push = 4 * ((int)(frame_ % 3) + 1);  // (GigaVoxelsRenderer.cpp:2093-2098)
+    o.passes = passes;
     return vv_render(ctx_, 0, &last_u_, &o);
 }
 

@@ -30,6 +30,11 @@ public:
     ~GigaVoxelsRenderer();
     int init();                          // Renderer::init
     int draw(const vv_camera& cam);      // Renderer::draw
+    // draw() in two halves, for a ray cast made elsewhere (a batched launch
+    // over several renderers): prepare_draw sets up the frame buffers and
+    // uniforms, finish_draw runs the given passes of vv_render on them.
+    int prepare_draw(const vv_camera& cam);
+    int finish_draw(int passes);
     int update();                        // Renderer::postDraw + Renderer::update
     // The page-request service for a compacted list drawn elsewhere (device
     // pointers); uploads are applied at once, or staged when deferred.

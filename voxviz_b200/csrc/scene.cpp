@@ -99,12 +99,15 @@ PagedScene::~PagedScene() {
     for (auto& t : tiles_) release_tile(*t);
     if (d_color_) cudaFree(d_color_);
     if (ev_blended_) cudaEventDestroy(ev_blended_);
+    if (ev_cast_) cudaEventDestroy(ev_cast_);
 }
 
 int PagedScene::init() {
     if (!host_only_) {
         if (!ctx_) return VV_ERR_ARG;
-        if (cudaEventCreateWithFlags(&ev_blended_, cudaEventDisableTiming) != cudaSuccess) return VV_ERR_CUDA;
+        if (cudaEventCreateWithFlags(&ev_blended_, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_cast_, cudaEventDisableTiming) != cudaSuccess)
+            return VV_ERR_CUDA;
     }
     if (!(d_.flags & VV_SCENE_SYNCHRONOUS)) thread_ = std::thread([this] { loader_main(); });
     return VV_OK;
@@ -357,6 +360,7 @@ int PagedScene::draw(const vv_camera& cam) {
     }
     const size_t np = (size_t)width_ * height_;
     if (cudaMemsetAsync(d_color_, 0, np * 16, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    if ((d_.flags & VV_SCENE_BATCHED) && !render_list_.empty()) return draw_batched(cam);
     for (size_t t : render_list_) {
         SceneTile& s = *tiles_[t];
         vv_camera tc;
@@ -369,6 +373,50 @@ int PagedScene::draw(const vv_camera& cam) {
         if (cudaEventRecord(s.drawn, s.ctx->stream) != cudaSuccess ||
             cudaStreamWaitEvent(ctx_->stream, s.drawn, 0) != cudaSuccess)
             return VV_ERR_CUDA;
+        if (launch_blend_over((float4*)d_color_, (const float4*)s.renderer->impl->d_color, np, ctx_->stream) !=
+            cudaSuccess)
+            return VV_ERR_CUDA;
+    }
+    if (cudaEventRecord(ev_blended_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    blended_once_ = true;
+    return VV_OK;
+}
+
+// The drawn tiles' ray casts as one persistent launch on the scene's stream
+// (the batched kernel: one queue of pixel tiles over all views), then each
+// tile's selection and compaction on its own stream, and the blends.
+int PagedScene::draw_batched(const vv_camera& cam) {
+    const size_t np = (size_t)width_ * height_;
+    views_.resize(render_list_.size());
+    for (size_t k = 0; k < render_list_.size(); ++k) {
+        SceneTile& s = *tiles_[render_list_[k]];
+        vv_camera tc;
+        tile_camera(s, cam, tc);
+        if (blended_once_ && cudaStreamWaitEvent(s.ctx->stream, ev_blended_, 0) != cudaSuccess) return VV_ERR_CUDA;
+        GigaVoxelsRenderer& r = *s.renderer->impl;
+        int rc = r.prepare_draw(tc);
+        if (rc) return rc;
+        // the tile's pools and node words as its stream left them
+        if (cudaEventRecord(s.drawn, s.ctx->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ctx_->stream, s.drawn, 0) != cudaSuccess)
+            return VV_ERR_CUDA;
+        vv_batch_view& v = views_[k];
+        std::memset(&v, 0, sizeof(v));
+        v.ctx = s.ctx;
+        v.tree = 0;
+        v.u = r.last_uniforms();
+        v.color = r.d_color;
+        v.usage = r.d_usage;
+    }
+    const vv_batch_config cfg{8, 8, 1, 0};
+    int rc = vv_render_batch(ctx_, views_.data(), (int32_t)views_.size(), &cfg);
+    if (rc) return rc;
+    if (cudaEventRecord(ev_cast_, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
+    for (size_t t : render_list_) {
+        SceneTile& s = *tiles_[t];
+        if (cudaStreamWaitEvent(s.ctx->stream, ev_cast_, 0) != cudaSuccess) return VV_ERR_CUDA;
+        rc = s.renderer->impl->finish_draw(VV_PASS_SELECT | VV_PASS_COMPACT);
+        if (rc) return rc;
         if (launch_blend_over((float4*)d_color_, (const float4*)s.renderer->impl->d_color, np, ctx_->stream) !=
             cudaSuccess)
             return VV_ERR_CUDA;

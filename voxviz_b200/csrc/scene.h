@@ -101,6 +101,9 @@ private:
     int width_ = 0, height_ = 0;
     float* d_color_ = nullptr;
     cudaEvent_t ev_blended_ = nullptr;  // the last frame's blends are done
+    cudaEvent_t ev_cast_ = nullptr;     // the batched ray cast is done
+    std::vector<vv_batch_view> views_;
+    int draw_batched(const vv_camera& cam);
     bool blended_once_ = false;
     bool host_only_ = false;
     // pager
