@@ -28,7 +28,7 @@ HOST_CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
 CU_SOURCES = ["kernels.cu", "ctx.cu", "noalloc.cu", "production.cu", "adjoint.cu", "batch.cu"]
 CPP_SOURCES = ["terrain.cpp", "octree.cpp", "gradients.cpp", "gvfile.cpp", "renderer.cpp", "scene.cpp", "capi.cpp"]
 HEADERS = ["kernels.cuh", "cellmask.cuh", "ctx.h", "terrain.h", "octree.h", "gvfile.h", "scene.h", "handles.h", "renderer.h", "production.h", "raycast_common.cuh",
-           "lod_bound.h", "gradients.h"]
+           "lod_bound.h", "gradients.h", "fixed_div.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -32,7 +32,7 @@ struct BatchView {
 };
 
 // The views of one launch.  Kernel parameters may take 32,764 bytes.
-constexpr int kMaxLaunchViews = 92;  // 336 bytes each
+constexpr int kMaxLaunchViews = 90;  // 352 bytes each
 struct BatchParams {
     int n;            // views
     int total_tiles;  // tiles of all n views
@@ -186,6 +186,7 @@ static int batch_launch(vv_ctx* c, const vv_batch_view* views, int32_t n, const 
             BatchView& v = bp.v[i];
             std::memset(&v, 0, sizeof(v));
             v.p.u = *u;
+            set_divisors(v.p);
             v.p.nodes = t.nodes;
             for (int a = 0; a < 3; ++a) {
                 v.p.node_dim[a] = t.dim[a];

@@ -472,6 +472,7 @@ static int diff_params(vv_ctx* c, int32_t tree, const vv_uniforms* u, RaycastPar
     if (u->compute_lighting) return fail(c, VV_ERR_ARG, "the adjoint covers the unlit ray cast only");
     std::memset(&p, 0, sizeof(p));
     p.u = *u;
+    set_divisors(p);
     p.nodes = t.nodes;
     for (int a = 0; a < 3; ++a) {
         p.node_dim[a] = t.dim[a];
@@ -570,6 +571,7 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         RaycastParams p;
         std::memset(&p, 0, sizeof(p));
         p.u = *u;
+        set_divisors(p);
         p.nodes = t.nodes;
         p.node_dim[0] = t.dim[0];
         p.node_dim[1] = t.dim[1];
@@ -682,6 +684,7 @@ int vv_measure_footprint(vv_ctx* c, int32_t tree, const vv_uniforms* u, int64_t*
     RaycastParams p;
     std::memset(&p, 0, sizeof(p));
     p.u = *u;
+    set_divisors(p);
     p.nodes = t.nodes;
     for (int a = 0; a < 3; ++a) {
         p.node_dim[a] = t.dim[a];

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "../../include/voxviz_b200.h"
 
 namespace vv {
@@ -25,7 +27,19 @@ struct RaycastParams {
     uint32_t* node_touch;    // footprint mode: bit per node (block-linear index)
     uint32_t* brick_touch;   // footprint mode: bit per brick-pool slot
     const uint32_t* cell_mask;  // empty-cell masks of the pool (cellmask.cuh), or nullptr
+    // set_divisors: RN(1 / brick_pool_dimension) per axis (fixed_div.h), and
+    // 1 / ray_step_size when that is a power of two (else 0: divide)
+    float rpdim[3];
+    float rstep;
 };
+
+// The reciprocals of RaycastParams from its uniforms (host).
+inline void set_divisors(RaycastParams& p) {
+    for (int a = 0; a < 3; ++a) p.rpdim[a] = 1.0f / p.u.brick_pool_dimension[a];
+    int e = 0;
+    const float m = std::frexp(p.u.ray_step_size, &e);
+    p.rstep = (m == 0.5f) ? 1.0f / p.u.ray_step_size : 0.0f;
+}
 
 // Pyramid/compaction launch state.
 struct CompactParams {

@@ -13,6 +13,7 @@
 #include <cuda_fp16.h>
 
 #include "cellmask.cuh"
+#include "fixed_div.h"
 #include "kernels.cuh"
 #include "lod_bound.h"
 
@@ -216,6 +217,13 @@ __device__ __forceinline__ int sample_in_slot(const RaycastParams& p, F3 uvw, co
     return kInSlot;
 }
 
+
+// t / step for step = RS * 2^e.  With RS a power of two (rstep = 1 / RS)
+// the quotient is t times a power of two: the same real number, so the same
+// rounded result, as the division.
+__device__ __forceinline__ float div_step(const RaycastParams& p, float t, float step, int e) {
+    return p.rstep != 0.0f ? t * (p.rstep * pow2i(-e)) : t / step;
+}
 
 // ComputeMinRayBoxIntersection (GigaVoxelsNoLighting.frag:124-180): exit
 // time over the planes facing away from the ray, 4.0 if none, t == 0 ignored.
@@ -588,7 +596,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             const float step = k.RS * ratio;
             const float aw = (float)(node.y >> 24) / 255.0f;
             const float t = min_exit(s.pos, s.dir, ext_min, ext_max);
-            const int n = (int)(t / step) + 1;
+            const int n = (int)div_step(p, t, step, k.L - depth) + 1;
             if (aw < 0.005f) {
                 s.pos = add(s.pos, muls(s.dir, (float)n * step));
             } else {
@@ -616,14 +624,18 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
         } else {
             // lightDir = normalize(LightPosition - rayWorldPosition) at entry (:337)
             const F3 light_dir = LIT ? normalize3(sub(ld3(p.u.light_position), s.pos)) : f3(0.0f, 0.0f, 0.0f);
-            const F3 bptr = f3((float)((cur_bw >> 20) & 0x3FFu) / k.pdim.x, (float)((cur_bw >> 10) & 0x3FFu) / k.pdim.y,
-                               (float)(cur_bw & 0x3FFu) / k.pdim.z);
-            F3 bpos = add(bptr, divv(mul(cur_brp, k.bdim), k.pdim));
+            // the six quotients by the pool dimensions from their reciprocals (fixed_div.h)
+            const F3 bptr = f3(fixed_div((float)((cur_bw >> 20) & 0x3FFu), k.pdim.x, p.rpdim[0]),
+                               fixed_div((float)((cur_bw >> 10) & 0x3FFu), k.pdim.y, p.rpdim[1]),
+                               fixed_div((float)(cur_bw & 0x3FFu), k.pdim.z, p.rpdim[2]));
+            const F3 brb = mul(cur_brp, k.bdim);
+            F3 bpos = add(bptr, f3(fixed_div(brb.x, k.pdim.x, p.rpdim[0]), fixed_div(brb.y, k.pdim.y, p.rpdim[1]),
+                                   fixed_div(brb.z, k.pdim.z, p.rpdim[2])));
             const float ratio = pow2i(k.L - brick_depth);
             const F3 wstep = muls(muls(s.dir, k.RS), ratio);
             const float t = min_exit(s.pos, s.dir, ext_min, ext_max);
             const float step = k.RS * ratio;
-            const int n = (int)(t / step) + 1;
+            const int n = (int)div_step(p, t, step, k.L - brick_depth) + 1;
             // taps inside this brick's slot skip the general texel addressing
             int base[3] = {(int)((cur_bw >> 20) & 0x3FFu) - 1, (int)((cur_bw >> 10) & 0x3FFu) - 1,
                            (int)(cur_bw & 0x3FFu) - 1};
