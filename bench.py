@@ -444,13 +444,19 @@ def run_fit(args):
 
     import voxviz_b200 as vv
     from voxviz_b200 import diff, scene
+    from voxviz_b200 import dist as vdist
 
-    torch.cuda.set_device(0)
+    # data parallel over views: each rank renders its views, the texel
+    # gradient is summed over ranks (the one exchange step), every rank takes
+    # the same Adam step
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    vdist.init(timeout_s=900)
     t_setup = time.perf_counter()
     octree = vv.Octree.terrain(seed=TERRAIN_SEED, depth=FIT_DEPTH)
     heights = octree.heights()
     cams = [scene.seeded_view(FIT_VIEW_SEED + v, heights, FIT_SIZE, FIT_SIZE) for v in range(FIT_VIEWS)]
-    ctx = vv.Context(0)
+    ctx = vv.Context(local_rank)
     r = vv.Renderer(ctx, octree, fmt="fp32", pool_bytes=FIT_POOL_BYTES, preload_all=False, alpha_stop=ALPHA_STOP,
                     jitter_seed=JITTER_SEED, device_paging=True)
     passes = scene.converge_views(r, cams)
@@ -620,6 +626,8 @@ def run_fit(args):
                       "seconds": round(time.perf_counter() - t_fd, 1)}
     del traj_pool, vals_pool, got, g_ref
     # ---- the fit: Adam on every pool texel, L2 image loss ----
+    mine = vdist.views_of_rank(FIT_VIEWS, rank, world)
+    us_mine, target_mine = [us[v] for v in mine], target[mine]
     param.grad = None
     opt = torch.optim.Adam([param], lr=FIT_LR, fused=True)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -632,11 +640,15 @@ def run_fit(args):
     t0.record()
     for step in range(args.fit_steps):
         ev[0].record()
-        c = diff.render(param, ctx, slots, us)
+        c = diff.render(param, ctx, slots, us_mine)
         ev[1].record()
-        loss = ((c - target) ** 2).mean()
+        if world == 1:
+            loss = ((c - target) ** 2).mean()
+        else:  # this rank's share of the mean over all views
+            loss = ((c - target_mine) ** 2).sum() / target.numel()
         opt.zero_grad(set_to_none=True)
         loss.backward()
+        vdist.sum_gradients(param.grad)
         ev[2].record()
         opt.step()
         ev[3].record()
@@ -648,14 +660,17 @@ def run_fit(args):
     t1.record()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total_ms = t0.elapsed_time(t1)
+    total_ms = vdist.max_over_ranks(t0.elapsed_time(t1), "cuda")
     status |= diff.check_status(ctx)
-    losses = [float(x) for x in losses]
+    if losses:
+        lt = torch.stack(losses)
+        vdist.sum_gradients(lt)  # the loss over all views
+        losses = [float(x) for x in lt.cpu()]
     rays = FIT_VIEWS * FIT_SIZE * FIT_SIZE
     skip = min(3, max(0, args.fit_steps - 1))
-    f = float(np.mean(fwd_ms[skip:]))
-    b = float(np.mean(bwd_ms[skip:]))
-    a = float(np.mean(adam_ms[skip:]))
+    f = vdist.max_over_ranks(float(np.mean(fwd_ms[skip:])), "cuda")
+    b = vdist.max_over_ranks(float(np.mean(bwd_ms[skip:])), "cuda")
+    a = vdist.max_over_ranks(float(np.mean(adam_ms[skip:])), "cuda")
     out = {
         "workload": "fit", "metric": "Mrays/s fwd & fwd+bwd, 16x512^2 views, 2048^3 FP32 bricks",
         "value": round(rays / ((f + b) / 1e3) / 1e6, 2), "unit": "Mrays/s (fwd+bwd)",
@@ -671,12 +686,17 @@ def run_fit(args):
         "config": {"workload": f"fBm terrain {octree.info.volume_dim}^3 (depth {FIT_DEPTH}), FP32 bricks, "
                                f"{FIT_VIEWS} seeded {FIT_SIZE}x{FIT_SIZE} views, targets from bricks + N(0,{FIT_SIGMA})",
                    "pool_slots": list(slots), "resident_bricks": st["resident_bricks"], "paging_passes": passes,
-                   "evictions": st["evictions_total"], "params": int(param.numel()), "data": "synthetic"},
-        "clocks": clk, "setup_s": round(setup_s, 1),
+                   "evictions": st["evictions_total"], "params": int(param.numel()), "data": "synthetic",
+                   "parallelism": f"views over {world} ranks, texel gradient all-reduced" if world > 1
+                   else "single GPU"},
+        "n_gpus": world, "clocks": clk, "setup_s": round(setup_s, 1),
     }
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     r.close()
     ctx.close()
+    vdist.barrier()
+    vdist.shutdown()
 
 
 BATCH_DEPTHS, BATCH_VIEWS, BATCH_SIDE = (7, 8, 9, 10), 64, (256, 2048)
