@@ -141,6 +141,10 @@ typedef struct vv_frame_out {
 #define VV_PASS_SELECT 2
 #define VV_PASS_COMPACT 4
 #define VV_PASS_ALL 7
+/* With VV_PASS_RAYCAST: colour as RGBA8 unorm, round(clamp(c, 0, 1) * 255)
+ * per channel (r in the low byte), into `color` read as uint32_t[H][W]:
+ * 4 bytes per pixel instead of 16 (the display format of the frame). */
+#define VV_PASS_COLOR_RGBA8 8
 
 typedef struct vv_ctx vv_ctx;
 
@@ -526,6 +530,9 @@ typedef struct vv_renderer_desc {
     int32_t device_paging;     /* 1: de-duplicate requests and produce bricks
                                   on the GPU (same policy and results; the
                                   host keeps only the LRU list)             */
+    int32_t color_rgba8;       /* 1: the frame's colour as RGBA8 unorm
+                                  (VV_PASS_COLOR_RGBA8), 4 bytes per pixel;
+                                  read_color then returns bytes             */
 } vv_renderer_desc;
 
 typedef struct vv_renderer_stats {

@@ -26,7 +26,8 @@ import numpy as np
 
 from . import _native as N
 from ._native import (FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_FP16, VV_FMT_FP32, VV_FMT_RGBA8,  # noqa: F401
-                      VV_PASS_ALL, VV_PASS_COMPACT, VV_PASS_RAYCAST, VV_PASS_SELECT, Camera, FrameOut,
+                      VV_PASS_ALL, VV_PASS_COLOR_RGBA8, VV_PASS_COMPACT, VV_PASS_RAYCAST, VV_PASS_SELECT, Camera,
+                      FrameOut,
                       NodePatch, OctreeInfo, Uniforms, VVError)
 
 __all__ = ["Octree", "Context", "Renderer", "Batch", "Scene", "batch_variants", "make_camera", "look_at",
@@ -472,11 +473,12 @@ class Renderer:
 
     def __init__(self, ctx: Context, octree: Octree, fmt="rgba8", pool_bytes: int = 0, preload_all: bool = True,
                  request_cap: int = 0, lod_scalar: float = 1.0, alpha_stop: float = 0.99, jitter_seed: int = 7,
-                 producer_threads: int = 0, device_paging: bool = False):
+                 producer_threads: int = 0, device_paging: bool = False, color_rgba8: bool = False):
         d = N.RendererDesc(fmt=fmt_code(fmt), pool_bytes=pool_bytes, preload_all=1 if preload_all else 0,
                            request_cap=request_cap, lod_scalar=lod_scalar, alpha_stop=alpha_stop,
                            jitter_seed=jitter_seed, max_width=0, max_height=0, producer_threads=producer_threads,
-                           device_paging=1 if device_paging else 0)
+                           device_paging=1 if device_paging else 0, color_rgba8=1 if color_rgba8 else 0)
+        self.color_rgba8 = bool(color_rgba8)
         h = C.c_void_p()
         _check(lib().vv_renderer_create(ctx.handle, octree.handle, C.byref(d), C.byref(h)), ctx.handle,
                "renderer create")
@@ -529,10 +531,12 @@ class Renderer:
         return dict(zip(["color", "usage", "mask", "requests", "request_count"], [p.value for p in ptrs]))
 
     def read_color(self, out: np.ndarray | None = None) -> np.ndarray:
-        """Last frame's colour (H,W,4) float32, into `out` (e.g. pinned) if given."""
+        """Last frame's colour (H,W,4): float32, or uint8 for an RGBA8 renderer;
+        into `out` (e.g. pinned) if given."""
         if out is None:
             u = self.last_uniforms()
-            out = np.zeros((u.height, u.width, 4), dtype=np.float32)
+            out = np.zeros((u.height, u.width, 4), dtype=np.uint8 if getattr(self, "color_rgba8", False)
+                           else np.float32)
         self._ck(lib().vv_renderer_read_color(self._h, _ptr(out)), "read color")
         return out
 

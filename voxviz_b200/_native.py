@@ -16,6 +16,7 @@ VV_GVX_CONSTANT_COLORS, VV_GVX_SKIP_GRADIENTS = 1, 2
 VV_SCENE_HOST_ONLY, VV_SCENE_SYNCHRONOUS, VV_SCENE_BATCHED = 1, 2, 4
 VV_FMT_RGBA8, VV_FMT_FP16, VV_FMT_BF16, VV_FMT_FP32 = range(4)
 VV_PASS_RAYCAST, VV_PASS_SELECT, VV_PASS_COMPACT, VV_PASS_ALL = 1, 2, 4, 7
+VV_PASS_COLOR_RGBA8 = 8
 FMT_NAMES = {"rgba8": VV_FMT_RGBA8, "fp16": VV_FMT_FP16, "bf16": VV_FMT_BF16, "fp32": VV_FMT_FP32}
 TEXEL_BYTES = {VV_FMT_RGBA8: 4, VV_FMT_FP16: 8, VV_FMT_BF16: 8, VV_FMT_FP32: 16}
 
@@ -209,6 +210,7 @@ class RendererDesc(C.Structure):
         ("max_height", C.c_int32),
         ("producer_threads", C.c_int32),
         ("device_paging", C.c_int32),
+        ("color_rgba8", C.c_int32),
     ]
 
 

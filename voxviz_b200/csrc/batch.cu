@@ -32,7 +32,7 @@ struct BatchView {
 };
 
 // The views of one launch.  Kernel parameters may take 32,764 bytes.
-constexpr int kMaxLaunchViews = 90;  // 352 bytes each
+constexpr int kMaxLaunchViews = 88;  // 360 bytes each
 struct BatchParams {
     int n;            // views
     int total_tiles;  // tiles of all n views

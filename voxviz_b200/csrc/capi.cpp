@@ -424,7 +424,7 @@ int vv_renderer_frame_buffers(vv_renderer* r, float** color, uint32_t** usage, u
 
 int vv_renderer_read_color(vv_renderer* r, float* host_rgba) {
     if (!r || !host_rgba || !r->impl->d_color) return VV_ERR_ARG;
-    const size_t bytes = (size_t)r->impl->width * r->impl->height * 16;
+    const size_t bytes = (size_t)r->impl->width * r->impl->height * r->impl->color_bytes();
     if (cudaMemcpyAsync(host_rgba, r->impl->d_color, bytes, cudaMemcpyDeviceToHost, r->ctx->stream) != cudaSuccess)
         return VV_ERR_CUDA;
     if (cudaStreamSynchronize(r->ctx->stream) != cudaSuccess) return VV_ERR_CUDA;

@@ -583,6 +583,7 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         p.slots[2] = c->slots[2];
         p.jitter = c->d_jitter;
         p.color = (float4*)out->color;
+        p.color8 = (out->passes & VV_PASS_COLOR_RGBA8) ? 1 : 0;
         p.usage = usage;
         p.status = c->d_status;
         p.max_iter = vv_max_iterations(u);

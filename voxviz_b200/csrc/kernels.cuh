@@ -31,6 +31,7 @@ struct RaycastParams {
     // 1 / ray_step_size when that is a power of two (else 0: divide)
     float rpdim[3];
     float rstep;
+    int color8;              // colour as RGBA8 unorm: color is read as uint32_t[H*W]
 };
 
 // The reciprocals of RaycastParams from its uniforms (host).

@@ -218,6 +218,15 @@ __device__ __forceinline__ int sample_in_slot(const RaycastParams& p, F3 uvw, co
 }
 
 
+// A colour as RGBA8 unorm: round(clamp(c, 0, 1) * 255) per channel, to the
+// nearest (ties to even); NaN stores 0.
+__device__ __forceinline__ uint32_t unorm8(float c) {
+    return __float2uint_rn(__fmul_rn(fminf(fmaxf(c, 0.0f), 1.0f), 255.0f));
+}
+__device__ __forceinline__ uint32_t pack_unorm8(float4 c) {
+    return unorm8(c.x) | (unorm8(c.y) << 8) | (unorm8(c.z) << 16) | (unorm8(c.w) << 24);
+}
+
 // t / step for step = RS * 2^e.  With RS a power of two (rstep = 1 / RS)
 // the quotient is t times a power of two: the same real number, so the same
 // rounded result, as the division.
@@ -732,7 +741,10 @@ __device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int
     F3 pos;
     if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s))
         walk<FMT, COUNT, UsageVisitor, STEPS, RESUME, LIT>(p, k, s, vis, path);
-    if (p.color) p.color[pix] = s.dst;
+    if (p.color) {
+        if (p.color8) ((uint32_t*)p.color)[pix] = pack_unorm8(s.dst);
+        else p.color[pix] = s.dst;
+    }
 }
 
 }  // namespace rc

@@ -269,8 +269,8 @@ int GigaVoxelsRenderer::alloc_frame(int w, int h) {
     const size_t np = (size_t)w * h;
     cap_ = d_.request_cap > 0 ? d_.request_cap : (int)np;
     // two colour buffers: a frame's read-back may run while the next is drawn
-    if (cudaMalloc((void**)&color_buf_[0], np * 16) != cudaSuccess) return VV_ERR_OOM;
-    if (cudaMalloc((void**)&color_buf_[1], np * 16) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMalloc((void**)&color_buf_[0], np * color_bytes()) != cudaSuccess) return VV_ERR_OOM;
+    if (cudaMalloc((void**)&color_buf_[1], np * color_bytes()) != cudaSuccess) return VV_ERR_OOM;
     d_color = color_buf_[cur_color_];
     if (cudaMalloc((void**)&d_usage, np * 48) != cudaSuccess) return VV_ERR_OOM;
     if (cudaMalloc((void**)&d_mask, np * 4) != cudaSuccess) return VV_ERR_OOM;
@@ -316,7 +316,7 @@ int GigaVoxelsRenderer::finish_draw(int passes) {
     o.request_count = d_count;
     o.request_cap = cap_;
     o.compress_max_push = 4 * ((int)(frame_ % 3) + 1);  // (GigaVoxelsRenderer.cpp:2093-2098)
-    o.passes = passes;
+    o.passes = passes | (d_.color_rgba8 ? VV_PASS_COLOR_RGBA8 : 0);
     return vv_render(ctx_, 0, &last_u_, &o);
 }
 
@@ -347,7 +347,7 @@ int GigaVoxelsRenderer::start_readback() {
     void* host = readback_host_;
     readback_host_ = nullptr;
     if (cudaStreamWaitEvent(copy_stream_, ev_drawn_, 0) != cudaSuccess) return VV_ERR_CUDA;
-    if (cudaMemcpyAsync(host, color_buf_[readback_buf_], (size_t)width * height * 16, cudaMemcpyDeviceToHost,
+    if (cudaMemcpyAsync(host, color_buf_[readback_buf_], (size_t)width * height * color_bytes(), cudaMemcpyDeviceToHost,
                         copy_stream_) != cudaSuccess)
         return VV_ERR_CUDA;
     if (cudaEventRecord(ev_copied_[readback_buf_], copy_stream_) != cudaSuccess) return VV_ERR_CUDA;

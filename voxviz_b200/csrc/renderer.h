@@ -51,6 +51,7 @@ public:
     int read_color_async(void* host);
     int wait_readback();
     void stats(vv_renderer_stats& s) const;
+    size_t color_bytes() const { return d_.color_rgba8 ? 4 : 16; }  // per pixel
 
     vv_ctx* ctx() { return ctx_; }
     const vv_uniforms& last_uniforms() const { return last_u_; }
