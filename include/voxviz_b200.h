@@ -301,7 +301,9 @@ typedef struct vv_batch_view {
     int32_t tree;           /* node pool index in that context            */
     int32_t pad;
     vv_uniforms u;          /* the view's uniforms (as for vv_render)     */
-    float* color;           /* device, 4 floats per pixel, or NULL        */
+    float* color;           /* device, 4 floats per pixel, or NULL: the
+                               batched launch always writes float4 colour
+                               (no RGBA8 form, unlike VV_PASS_COLOR_RGBA8) */
     uint32_t* usage;        /* device, 12 words per pixel, or NULL        */
 } vv_batch_view;
 
@@ -342,7 +344,13 @@ int vv_batch_autotune(vv_ctx* ctx, const vv_batch_view* views, int32_t n, int32_
  * VV_NOALLOC_MAX_PIXELS (2^21, enough for 1920x1080); larger frames return
  * VV_ERR_ARG.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress, with that device current); make that first
- * call before any stream capture.  All calls share the one array: calls that
+ * call before any stream capture.  That first call may also be the one that
+ * loads the library's device code on that device (CUDA loads modules
+ * lazily by default), which can allocate device memory and block; make it
+ * once at start-up, outside the code that must not allocate.  The address
+ * is kept for the life of the process: after cudaDeviceReset (or anything
+ * else that destroys the device's primary context) the kept address is
+ * stale, so do not call this entry point again in that process.  All calls share the one array: calls that
  * overlap on the GPU (different streams, or different host threads on the
  * same device) race and must be serialised by the caller.  It calls no
  * cudaMalloc, cudaFree or allocating library routine.  Errors: VV_ERR_ARG,

@@ -91,6 +91,7 @@ class _Stream:
         self.i = 0
         self.name = None
         self.attrs = {}
+        self.elements = sum(1 for t in self.tokens if t[0] == "start")
 
     def next(self):
         if self.i >= len(self.tokens):
@@ -223,6 +224,9 @@ def load_gvx(path, constant_colors=False, load_normals=True) -> dict:
                     b = to_int(a.get("Brick"))
                     if b < 0:
                         raise GvxError("negative Brick")
+                    if b >= xs.elements:
+                        # more bricks than the file has elements: a gap for sure
+                        raise GvxError("Brick index beyond the file's element count")
                     lst = brick_nodes[level]
                     if b >= len(lst):
                         lst.extend([None] * (b + 1 - len(lst)))

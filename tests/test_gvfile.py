@@ -207,6 +207,8 @@ CASES = {
     "Brick index twice": (lambda d: _edit_text(d, 'Brick="1"', 'Brick="0"'), N.VV_ERR_IO),
     "Brick index gap": (lambda d: _edit_text(d, 'Brick="1"', 'Brick="100"'), N.VV_ERR_IO),
     "negative Brick": (lambda d: _edit_text(d, 'Brick="1"', 'Brick="-1"'), N.VV_ERR_IO),
+    # rejected before the index list is sized by it (it would take 8 GB)
+    "huge Brick index": (lambda d: _edit_text(d, 'Brick="1"', 'Brick="2000000000"'), N.VV_ERR_IO),
 }
 
 

@@ -81,6 +81,45 @@ def test_noalloc_compaction_matches_render_passes_twice_in_a_row():
     assert n2 > 50
 
 
+@pytest.mark.parametrize("w,h", [(1, 1), (1, 9), (9, 1), (2, 3), (5, 5), (64, 2)])
+def test_noalloc_compaction_on_degenerate_frames(w, h):
+    # one-level pyramids (1x1: no level 1, the count read from the mask),
+    # and frames where only one dimension halves
+    sc = helpers.Scene(seed=2, depth=5)
+    g = helpers.GpuScene(sc)
+    u = sc.uniforms(sc.view(5, w, h, frame=3))
+    usage = _usage_for(g, u)
+    cap = w * h
+    _same(_existing(g, u, usage, cap, 8), _noalloc(u, usage, cap, 8), cap)
+
+
+def test_noalloc_without_requests_or_count():
+    import torch
+    sc = helpers.Scene(seed=2, depth=5)
+    g = helpers.GpuScene(sc)
+    u = sc.uniforms(sc.view(7, 200, 120, frame=1))
+    usage = _usage_for(g, u)
+    m_ref, r_ref, c_ref = _existing(g, u, usage, 200 * 120, 4)
+    # cap 0: mask and count only, no request written
+    m0, r0, c0 = _noalloc(u, usage, 0, 4)
+    assert np.array_equal(m0.cpu().numpy(), m_ref.cpu().numpy())
+    assert int(c0.item()) == int(c_ref.item())
+    assert bool((r0 == -1).all())
+    # no count pointer: mask and requests only
+    dev = usage.device
+    mask = torch.full((u.height, u.width), -1, dtype=torch.int32, device=dev)
+    req = torch.full((200 * 120, 4), -1, dtype=torch.int32, device=dev)
+    rc = vv.lib().vv_compact_requests_noalloc(C.c_void_p(usage.data_ptr()), C.c_void_p(mask.data_ptr()), u.width,
+                                              u.height, C.c_void_p(req.data_ptr()), None, 200 * 120, 4,
+                                              C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == N.VV_OK, vv.lib().vv_last_error(None)
+    torch.cuda.synchronize()
+    n = int(c_ref.item())
+    assert np.array_equal(mask.cpu().numpy(), m_ref.cpu().numpy())
+    assert np.array_equal(req[:n].cpu().numpy(), r_ref[:n].cpu().numpy())
+    assert bool((req[n:] == -1).all())
+
+
 def test_noalloc_rejects_frames_beyond_its_array():
     import torch
     t = torch.zeros(16, dtype=torch.int32, device="cuda")

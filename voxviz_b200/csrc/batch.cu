@@ -4,7 +4,8 @@
 // all views from a device work queue (one atomic counter; tiles numbered view
 // by view, row-major inside a view).  The views' RaycastParams (uniforms +
 // the pools of each view's octree) travel by value in the kernel's parameter
-// space, up to 92 views per launch (larger batches launch in chunks), so a
+// space, up to kMaxLaunchViews views per launch (88 with the 360-byte view
+// record; larger batches launch in chunks), so a
 // CTA reads its view's parameters from the constant bank as the single-view
 // ray cast does, and runs render_pixel, the vv_render ray cast, on every
 // pixel of the tile.  Tile shape and the march-loop

@@ -31,6 +31,7 @@ public:
     enum Token { kStart, kEnd, kDone, kError };
 
     explicit XmlStream(std::string text) : s_(std::move(text)) {}
+    size_t size() const { return s_.size(); }
 
     Token next() {
         if (failed_) return kError;
@@ -317,6 +318,15 @@ struct GvxLoader {
             const int b = to_int(xs.attr("Brick"));
             if (b < 0) {
                 err = "negative Brick index at depth " + std::to_string(level);
+                return false;
+            }
+            // brick indices of a level are 0..n-1 for its n non-constant
+            // nodes, and every node takes at least one "<Node" of the text:
+            // a larger index can only be a corrupt file (and would size the
+            // index list by it)
+            if ((size_t)b >= xs.size() / 5 + 1) {
+                err = "Brick index " + std::to_string(b) + " at depth " + std::to_string(level) +
+                      " exceeds the number of nodes the file can hold";
                 return false;
             }
             n.brick = b;

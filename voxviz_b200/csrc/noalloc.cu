@@ -32,7 +32,10 @@ uint32_t* g_scratch_ptr[1024] = {};
 
 // Device address of the scratch array on the current device.  The array's
 // name is only a host-side stand-in; the address comes from
-// cudaGetSymbolAddress, once per device, with that device current.
+// cudaGetSymbolAddress, once per device, with that device current.  The
+// first lookup can load the module on that device (lazy loading), which may
+// allocate; the kept address does not survive a reset of the device's
+// primary context (cudaDeviceReset).
 int scratch_address(uint32_t** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
