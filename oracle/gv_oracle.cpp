@@ -309,21 +309,24 @@ struct Shader {
         pos += dir * ((T)numSteps * step);
     }
     // :230-282
-    void TraverseConstant(vec4<T> constValue, vec3<T>& pos, const vec3<T>& dir, T rayStepSize, T sampleRatio,
-                          int ratioLog2, const vec3<T>& mn, const vec3<T>& mx, vec4<T>& dst) const {
+    // Returns the step count and the samples composited (the control flow of
+    // the segment, for the trace): (numSteps << 32) | composited.
+    uint64_t TraverseConstant(vec4<T> constValue, vec3<T>& pos, const vec3<T>& dir, T rayStepSize, T sampleRatio,
+                              int ratioLog2, const vec3<T>& mn, const vec3<T>& mx, vec4<T>& dst) const {
         T timeToExit = ComputeMinRayBoxIntersection(pos, dir, mn, mx);
         if (constValue.a < (T)0.005f) {
             AdvanceRay(pos, dir, timeToExit, rayStepSize);
-            return;
+            return ((uint64_t)(uint32_t)((int)(timeToExit / rayStepSize) + 1) << 32) | 0xFFFFFFFFu;
         }
         int numSteps = (int)(timeToExit / rayStepSize) + 1;
+        const uint64_t steps0 = (uint64_t)(uint32_t)numSteps << 32;
         vec3<T> worldRayStep = dir * rayStepSize;
         for (int i = 0; i < numSteps; ++i) {
             pos += worldRayStep;
             if (dst.a > AlphaStop) {
                 numSteps -= (i + 1);
                 pos += dir * ((T)numSteps * rayStepSize);
-                return;
+                return steps0 | (uint32_t)i;
             }
             vec4<T> src = constValue;
             src.a = (T)1 - pow_pow2((T)1 - src.a, ratioLog2);
@@ -333,6 +336,7 @@ struct Shader {
             record(false, src, dst, pos);
             composite(dst, src);
         }
+        return steps0 | (uint32_t)numSteps;
     }
     // The adjoint's tape: every composited sample with the transmittance
     // before it (and for brick samples the brick-pool coordinate).
@@ -358,20 +362,21 @@ struct Shader {
         dst.a = k * src.a + dst.a;
     }
     // :311-359 (no lighting: sampleRatio is reset to 1 before the loop)
-    void TraverseBrick(vec3<T>& pos, const vec3<T>& dir, const vec3<T>& worldRayStep, vec3<T> curBrickRayPos,
-                       const vec3<T>& brickRayStep, T sampleRatio, const vec3<T>& mn, const vec3<T>& mx,
-                       vec4<T>& dst) const {
+    uint64_t TraverseBrick(vec3<T>& pos, const vec3<T>& dir, const vec3<T>& worldRayStep, vec3<T> curBrickRayPos,
+                           const vec3<T>& brickRayStep, T sampleRatio, const vec3<T>& mn, const vec3<T>& mx,
+                           vec4<T>& dst) const {
         // GigaVoxels.frag :337: lightDir at entry (lighting only)
         const vec3<T> lightDir = ComputeLighting ? normalize(LightPosition - pos) : vec3<T>{0, 0, 0};
         T timeToExit = ComputeMinRayBoxIntersection(pos, dir, mn, mx);
         T rayStepSize = RayStepSize * sampleRatio;
         int numSteps = (int)(timeToExit / rayStepSize) + 1;
+        const uint64_t steps0 = (uint64_t)(uint32_t)numSteps << 32;
         for (int i = 0; i < numSteps; ++i) {
             pos += worldRayStep;
             if (dst.a > AlphaStop) {
                 numSteps -= (i + 1);
                 pos += dir * ((T)numSteps * rayStepSize);
-                return;
+                return steps0 | (uint32_t)i;
             }
             vec4<T> src = texture(curBrickRayPos);
             src.a = (T)1 - pow_pow2((T)1 - src.a, 0);
@@ -380,6 +385,7 @@ struct Shader {
             composite(dst, src);
             curBrickRayPos += brickRayStep;
         }
+        return steps0 | (uint32_t)numSteps;
     }
     // GigaVoxels.frag shading (:293-312): k_Ambient 0.05, k_Diffuse =
     // k_Specular = 1, k_Shininess 100 with pow(x, 100) restated as
@@ -476,10 +482,26 @@ struct Shader {
     }
 
     // main (:490-751)
-    void main(int px, int py, vec4<T>& FragColor, uint32_t NodeUsageList[12]) const {
+    // FNV-1a over 64-bit words: the trace of a pixel's control flow.
+    static void mix(uint64_t& h, uint64_t v) {
+        for (int b = 0; b < 8; ++b) {
+            h ^= (v >> (8 * b)) & 0xFFu;
+            h *= 1099511628211ull;
+        }
+    }
+
+    // `trace` (may be NULL) receives a hash of the pixel's control flow:
+    // whether it has a fragment and starts inside, and per leaf segment the
+    // node, its depth and flags, the brick's depth, the step count and the
+    // samples composited, then the loop's iteration count.  Two runs with
+    // equal traces took the same decisions (descent, LOD, step counts, early
+    // termination); the colour then differs only by the arithmetic.
+    void main(int px, int py, vec4<T>& FragColor, uint32_t NodeUsageList[12], uint64_t* trace = nullptr) const {
         for (int i = 0; i < 12; ++i) NodeUsageList[i] = 0u;
         vec4<T> dst{0, 0, 0, 0};
         FragColor = dst;
+        uint64_t th = 1469598103934665603ull;
+        if (trace) *trace = th;
         vec3<T> rayWorldPosition;
         if (!RayPosition(px, py, rayWorldPosition)) return;
         vec3<T> rayDir = normalize(rayWorldPosition - CameraPosition);
@@ -487,6 +509,8 @@ struct Shader {
         T jitterOffset = (T)jitter[jy * JitterTexSize + jx] / (T)255;
         rayWorldPosition += (rayDir * RayStepSize) * jitterOffset;
         bool in = inside(rayWorldPosition, VolExtentMin, VolExtentMax);
+        mix(th, in ? 3u : 2u);
+        int iterations = 0;
         if (in) {
             int curListIndex = 0, curComponentIndex = 0;
             const int pcx = px % 2, pcy = py % 2;
@@ -511,7 +535,6 @@ struct Shader {
             int curDepth = 0, curBrickDepth = 0;
             uint32_t childNodePtr[3] = {0, 0, 0};
             int nodeListTraversalCount = 0, pushedNodeCount = 0;
-            int iterations = 0;
             while (in) {
                 if (++iterations > max_iter) {
                     flag(VV_ERR_TIMEOUT);
@@ -537,8 +560,11 @@ struct Shader {
                         T sampleRatio = std::ldexp((T)1, k);
                         vec4<T> cv{(T)(node_g & 255u) / (T)255, (T)((node_g >> 8) & 255u) / (T)255,
                                    (T)((node_g >> 16) & 255u) / (T)255, (T)(node_g >> 24) / (T)255};
-                        TraverseConstant(cv, rayWorldPosition, rayDir, RayStepSize * sampleRatio, sampleRatio, k,
-                                         nodeExtentMin, nodeExtentMax, dst);
+                        const uint64_t seg = TraverseConstant(cv, rayWorldPosition, rayDir, RayStepSize * sampleRatio,
+                                                              sampleRatio, k, nodeExtentMin, nodeExtentMax, dst);
+                        mix(th, ((uint64_t)nodeUsage[0] << 40) | ((uint64_t)nodeUsage[1] << 20) | nodeUsage[2]);
+                        mix(th, (uint64_t)curDepth | (1u << 8) | ((uint64_t)brickIsLoaded << 9));
+                        mix(th, seg);
                     } else {
                         vec3<T> ptr((T)((curBrickPtr_g >> 20u) & 0x3FFu) / BrickPoolDimension.x,
                                     (T)((curBrickPtr_g >> 10u) & 0x3FFu) / BrickPoolDimension.y,
@@ -548,8 +574,11 @@ struct Shader {
                         vec3<T> worldRayStep = rayDir;
                         worldRayStep *= RayStepSize;
                         worldRayStep *= sampleRatio;
-                        TraverseBrick(rayWorldPosition, rayDir, worldRayStep, curBrickRayPos, brickRayStep,
-                                      sampleRatio, nodeExtentMin, nodeExtentMax, dst);
+                        const uint64_t seg = TraverseBrick(rayWorldPosition, rayDir, worldRayStep, curBrickRayPos,
+                                                           brickRayStep, sampleRatio, nodeExtentMin, nodeExtentMax, dst);
+                        mix(th, ((uint64_t)nodeUsage[0] << 40) | ((uint64_t)nodeUsage[1] << 20) | nodeUsage[2]);
+                        mix(th, (uint64_t)curDepth | ((uint64_t)brickIsLoaded << 9) | ((uint64_t)curBrickDepth << 16));
+                        mix(th, seg);
                     }
                     if (nodeListTraversalCount >= startPushingNodes && nodeListTraversalCount < stopPushingNodes &&
                         pushedNodeCount < MaxNodesToPushThisFrame) {
@@ -604,6 +633,8 @@ struct Shader {
                 }
             }
         }
+        mix(th, (uint64_t)iterations);
+        if (trace) *trace = th;
         FragColor = dst;
     }
 
@@ -625,7 +656,7 @@ int max_iterations(const vv_uniforms* u) {
 
 template <typename T>
 int run_raycast(const vv_uniforms* u, const oracle_scene* s, int row0, int row1, void* color, uint32_t* usage,
-                int threads, int32_t* status) {
+                int threads, int32_t* status, uint64_t* trace = nullptr) {
     Shader<T> sh;
     sh.init(u);
     sh.nodes = s->nodes;
@@ -654,8 +685,8 @@ int run_raycast(const vv_uniforms* u, const oracle_scene* s, int row0, int row1,
         for (int x = 0; x < W; ++x) {
             vec4<T> c;
             uint32_t lst[12];
-            sh.main(x, y, c, lst);
             const size_t pix = (size_t)y * W + x;
+            sh.main(x, y, c, lst, trace ? trace + pix : nullptr);
             if (color) {
                 T* o = (T*)color + 4 * pix;
                 o[0] = c.r;
@@ -719,6 +750,13 @@ int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, i
 }
 
 int oracle_max_iterations(const vv_uniforms* u) { return max_iterations(u); }
+
+int oracle_raycast_trace(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
+                         void* color, uint32_t* usage, uint64_t* trace, int threads, int32_t* status) {
+    if (!u || !s || row0 < 0 || row1 > u->height || row0 > row1) return VV_ERR_ARG;
+    if (precision == 64) return run_raycast<double>(u, s, row0, row1, color, usage, threads, status, trace);
+    return run_raycast<float>(u, s, row0, row1, color, usage, threads, status, trace);
+}
 
 namespace {
 

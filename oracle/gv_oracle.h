@@ -24,6 +24,13 @@ typedef struct oracle_scene {
 int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
                    void* color, uint32_t* usage, int threads, int32_t* status);
 int oracle_max_iterations(const vv_uniforms* u);
+/* oracle_raycast plus `trace` (one uint64 per pixel of the full image, may
+ * be NULL): a hash of each pixel's control flow (fragment, inside test, per
+ * leaf segment the node, depth, flags, step count and samples composited,
+ * then the iteration count).  Equal traces in the binary32 and binary64 runs
+ * mean the same decisions were taken. */
+int oracle_raycast_trace(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
+                         void* color, uint32_t* usage, uint64_t* trace, int threads, int32_t* status);
 /* The binary32 ray cast's sample sequence from `traj` re-evaluated in
  * binary64 with texel values from `vals` (same layout): 4 doubles per pixel
  * for rows [row0,row1) of a full-image buffer. */

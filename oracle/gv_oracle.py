@@ -51,6 +51,9 @@ def load() -> C.CDLL:
     lib.oracle_raycast.restype = C.c_int
     lib.oracle_raycast.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_int, C.c_int, C.c_int,
                                    C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]
+    lib.oracle_raycast_trace.restype = C.c_int
+    lib.oracle_raycast_trace.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_int, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]
     lib.oracle_max_iterations.restype = C.c_int
     lib.oracle_max_iterations.argtypes = [C.POINTER(Uniforms)]
     lib.oracle_backward.restype = C.c_int
@@ -107,6 +110,32 @@ def raycast(u, scene: Scene, precision: int = 32, rows=None, threads: int = 0, w
     if rc != 0:
         raise RuntimeError(f"oracle_raycast failed: {rc}")
     return color, usage, st.value
+
+
+def raycast_trace(u, scene: Scene, precision: int = 32, rows=None, threads: int = 0):
+    """Returns (color, trace (H,W) uint64, status): the ray cast's colour and
+    a hash per pixel of its control flow (see oracle_raycast_trace); rows
+    outside `rows` keep the trace of an empty pixel (0)."""
+    lib = load()
+    W, H = u.width, u.height
+    r0, r1 = (0, H) if rows is None else rows
+    color = np.zeros((H, W, 4), dtype=np.float64 if precision == 64 else np.float32)
+    trace = np.zeros((H, W), dtype=np.uint64)
+    st = C.c_int32(0)
+    rc = lib.oracle_raycast_trace(C.byref(u), C.byref(scene.s), precision, r0, r1, _p(color), None, _p(trace),
+                                  threads, C.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"oracle_raycast_trace failed: {rc}")
+    return color, trace, st.value
+
+
+def flip_pixels(u, scene: Scene, rows=None, threads: int = 0):
+    """Pixels whose binary64 ray cast takes other decisions than the binary32
+    one (a descent, LOD choice, step count or early termination flips).
+    Returns (flips (H,W) bool, fp64 colour, fp32 colour)."""
+    c32, t32, _ = raycast_trace(u, scene, 32, rows, threads)
+    c64, t64, _ = raycast_trace(u, scene, 64, rows, threads)
+    return t32 != t64, c64, c32
 
 
 def backward(u, scene: Scene, dl_dcolor: np.ndarray, rows=None, grad: np.ndarray | None = None) -> np.ndarray:

@@ -37,23 +37,39 @@ class PagingRef:
         self.lru: OrderedDict[int, None] = OrderedDict((s, None) for s in range(self.total))
         self.slot_node: dict[int, tuple] = {}
         self.node_slot: dict[tuple, int] = {}
-        self.parent: dict[tuple, tuple] = {}
-        self.valid: set[tuple] = {(0, 0, 0)}
         self._derive_tree()
 
     def _derive_tree(self) -> None:
-        stack = [(0, 0, 0)]
-        while stack:
-            n = stack.pop()
-            w0 = int(self.words[n[2], n[1], n[0], 0])
-            c = ((w0 >> 20) & 1023, (w0 >> 10) & 1023, w0 & 1023)
-            if c == (0, 0, 0):
-                continue
-            for k in range(8):
-                ch = (c[0] + (k & 1), c[1] + ((k >> 1) & 1), c[2] + (k >> 2))
-                self.parent[ch] = n
-                self.valid.add(ch)
-                stack.append(ch)
+        """Parent of every node reachable from the root (flat grid index,
+        -1 for the root and for cells no reachable node points at), level by
+        level from the root's child pointer (NodeTree::getNode,
+        GigaVoxelsOctTree.cpp:56-73, walks the same pointers)."""
+        dz, dy, dx, _ = self.words.shape
+        self.dims = (dx, dy, dz)
+        n = dx * dy * dz
+        w0 = self.words[..., 0].reshape(-1)
+        self.parent_flat = np.full(n, -1, dtype=np.int64)
+        self.valid_flat = np.zeros(n, dtype=bool)
+        self.valid_flat[0] = True
+        offs = np.array([(k & 1) + ((k >> 1) & 1) * dx + (k >> 2) * dx * dy for k in range(8)], dtype=np.int64)
+        level = np.array([0], dtype=np.int64)
+        while level.size:
+            c = w0[level]
+            has = (c & np.uint32(0x3FFFFFFF)) != 0
+            par = level[has]
+            c = c[has].astype(np.int64)
+            base = ((c >> 20) & 1023) + ((c >> 10) & 1023) * dx + (c & 1023) * dx * dy
+            ch = (base[:, None] + offs[None, :]).reshape(-1)
+            self.parent_flat[ch] = np.repeat(par, 8)
+            self.valid_flat[ch] = True
+            level = ch
+
+    def _flat(self, n) -> int:
+        return n[0] + n[1] * self.dims[0] + n[2] * self.dims[0] * self.dims[1]
+
+    def _cell(self, f: int) -> tuple:
+        dx, dy, _ = self.dims
+        return (f % dx, (f // dx) % dy, f // (dx * dy))
 
     def is_constant(self, n) -> bool:
         return bool(int(self.words[n[2], n[1], n[0], 0]) & CONSTANT)
@@ -80,19 +96,25 @@ class PagingRef:
         if not self.is_constant((0, 0, 0)):
             self._upload((0, 0, 0))
 
+    def distinct_nodes(self, requests: np.ndarray) -> list:
+        """The compacted list's node ids decoded (the +1 of
+        AddToNodeUsageList removed), zeros and cells outside the tree dropped,
+        each node once in first-seen order."""
+        v = np.asarray(requests, dtype=np.uint32).reshape(-1)
+        v = v[v != 0].astype(np.int64)
+        x, y, z = ((v >> 20) & 1023) - 1, ((v >> 10) & 1023) - 1, (v & 1023) - 1
+        dx, dy, dz = self.dims
+        ok = (x >= 0) & (x < dx) & (y >= 0) & (y < dy) & (z >= 0) & (z < dz)
+        f = (x + y * dx + z * dx * dy)[ok]
+        f = f[self.valid_flat[f]]
+        _, first = np.unique(f, return_index=True)
+        return [self._cell(int(c)) for c in f[np.sort(first)]]
+
     def update(self, requests: np.ndarray) -> list:
         """Service one frame's compacted list (n x 4 words); returns uploads."""
         self.uploaded = []
-        seen = set()
         queue = []
-        for v in np.asarray(requests, dtype=np.uint32).reshape(-1):
-            v = int(v)
-            if v == 0:
-                continue
-            n = (((v >> 20) & 1023) - 1, ((v >> 10) & 1023) - 1, (v & 1023) - 1)
-            if n not in self.valid or n in seen:
-                continue
-            seen.add(n)
+        for n in self.distinct_nodes(requests):
             if n in self.node_slot:
                 self.lru.move_to_end(self.node_slot[n])
             elif not self.is_constant(n):
@@ -103,9 +125,11 @@ class PagingRef:
             if n in self.node_slot:
                 continue
             self._upload(n)
-            p = self.parent.get(n)
-            if p is not None and not self.is_constant(p) and p not in self.node_slot:
-                self._upload(p)
+            pf = int(self.parent_flat[self._flat(n)])
+            if pf >= 0:
+                p = self._cell(pf)
+                if not self.is_constant(p) and p not in self.node_slot:
+                    self._upload(p)
         return list(self.uploaded)
 
     def residency(self) -> dict:

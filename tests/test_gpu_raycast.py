@@ -70,15 +70,28 @@ def test_float_brick_formats_match_oracle(fmt):
     assert np.abs(got["color"] - ref["color"]).max() <= TOL
 
 
-def test_error_vs_fp64_oracle_reported_bounds(cfg1):
-    sc, g = cfg1
-    u = sc.uniforms(sc.view(3, 512, 512))
-    got = g.render(u)
-    ref64 = helpers.oracle_frame(u, sc.oracle_scene(), precision=64)
-    err = np.abs(got["color"].astype(np.float64) - ref64["color"])
-    rms = float(np.sqrt((err ** 2).mean()))
+@pytest.mark.parametrize("fmt,view", [("rgba8", 3), ("rgba8", 8), ("fp16", 5), ("bf16", 6), ("fp32", 7)])
+def test_error_vs_fp64_oracle_within_bound_except_decision_flips(fmt, view):
+    """Colour within 1/255 of the binary64 oracle on every pixel whose
+    binary64 run takes the same decisions (descent, LOD, step counts, early
+    termination) as the binary32 run; the pixels over 1/255 are all decision
+    flips, and on the binary32 sample sequence the binary64 colour is within
+    1/255 everywhere."""
+    from oracle import gv_oracle as go
+    sc = helpers.Scene(seed=1, depth=5, fmt=fmt)
+    g = helpers.GpuScene(sc)
+    u = sc.uniforms(sc.view(view, 512, 512))
+    got = g.render(u, passes=vv.VV_PASS_RAYCAST)["color"].astype(np.float64)
+    osc = sc.oracle_scene()
+    flips, c64, _ = go.flip_pixels(u, osc)
+    err = np.abs(got - c64).max(-1)
+    assert err[~flips].max() <= TOL, err[~flips].max()
+    assert not ((err > TOL) & ~flips).any()
+    assert flips.mean() < 0.01, flips.mean()
+    fixed = np.abs(got - go.fixed_path(u, osc)).max()
+    assert fixed <= TOL, fixed
+    rms = float(np.sqrt((np.abs(got - c64) ** 2).mean()))
     assert rms < TOL, rms
-    assert (err.max(-1) > TOL).mean() < 0.03
 
 
 def test_miss_only_view_is_empty(cfg1):

@@ -132,3 +132,42 @@ def test_fp32_oracle_close_to_fp64():
     # the colour error is reported as max and RMS, the RMS stays below 1/255.
     assert (err.max(-1) > 1 / 255).mean() < 0.03
     assert np.sqrt((err ** 2).mean()) < 1 / 255
+
+
+def test_fp32_fp64_differences_beyond_1_255_are_decision_flips():
+    """Between the binary32 and binary64 oracles, every pixel that differs by
+    more than 1/255 took other decisions (its control-flow trace differs);
+    the others agree within 1/255, and so does binary64 along the binary32
+    sample sequence everywhere."""
+    from tests import helpers
+    sc = helpers.Scene(seed=1, depth=5)
+    osc = sc.oracle_scene()
+    for view in (3, 4, 8):
+        u = sc.uniforms(sc.view(view, 256, 256))
+        flips, c64, c32 = go.flip_pixels(u, osc)
+        err = np.abs(c32.astype(np.float64) - c64).max(-1)
+        assert not ((err > 1 / 255) & ~flips).any()
+        assert err[~flips].max() <= 1 / 255
+        assert np.abs(c32.astype(np.float64) - go.fixed_path(u, osc)).max() <= 1 / 255
+        # the trace sees the decisions: equal colours where traces are equal
+        # in a run against itself
+        _, t_again, _ = go.raycast_trace(u, osc, 32)
+        _, t32, _ = go.raycast_trace(u, osc, 32)
+        assert np.array_equal(t_again, t32)
+
+
+def test_trace_changes_with_early_termination():
+    """The trace records where the march stops: a lower alpha stop changes
+    the trace of the pixels it cuts short and leaves misses unchanged."""
+    from tests import helpers
+    sc = helpers.Scene(seed=1, depth=5)
+    osc = sc.oracle_scene()
+    u1 = sc.uniforms(sc.view(3, 128, 128), alpha=0.99)
+    u2 = sc.uniforms(sc.view(3, 128, 128), alpha=0.5)
+    c1, t1, _ = go.raycast_trace(u1, osc, 32)
+    c2, t2, _ = go.raycast_trace(u2, osc, 32)
+    changed = np.any(c1 != c2, axis=-1)
+    assert changed.any()
+    assert (t1 != t2)[changed].all()
+    miss = ~np.any(c1 != 0, axis=-1) & ~np.any(c2 != 0, axis=-1)
+    assert miss.any() and (t1 == t2)[miss].all()
