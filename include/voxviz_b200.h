@@ -259,6 +259,11 @@ int vv_ctx_last_times(vv_ctx* ctx, float* raycast_ms, float* compact_ms);
  * kernel; used for the algorithmic bytes of the roofline). */
 int vv_measure_footprint(vv_ctx* ctx, int32_t tree, const vv_uniforms* u,
                          int64_t* nodes, int64_t* bricks);
+/* The same for n draws of one batch: the distinct entries and slots of the
+ * union of their reads (no reference counterpart: the roofline of a batched
+ * launch). */
+int vv_measure_footprint_views(vv_ctx* ctx, int32_t tree, const vv_uniforms* us, int32_t n,
+                               int64_t* nodes, int64_t* bricks);
 
 /* ---- differentiable ray cast --------------------------------------------- */
 
@@ -619,6 +624,12 @@ int vv_renderer_last_requests(const vv_renderer* r, uint32_t* out, int32_t cap,
  * out_slot[i]; returns the count in *n. */
 int vv_renderer_residency(const vv_renderer* r, uint32_t* out_xyz,
                           uint32_t* out_slot, int64_t cap, int64_t* n);
+/* The brick pool's slots in LRU order, least recently used first: the order
+ * of BrickPool::m_loadedBricks (GigaVoxelsBrickPool.h:66, moved by
+ * notifyUsed GigaVoxelsBrickPool.cpp:406-424 and BrickPool::update :561-682),
+ * which eviction takes from the front.  Writes min(cap, slots) entries and
+ * the slot count to *n. */
+int vv_renderer_lru_order(vv_renderer* r, uint32_t* out, int64_t cap, int64_t* n);
 /* Uniforms of the last draw. */
 int vv_renderer_last_uniforms(const vv_renderer* r, vv_uniforms* out);
 vv_ctx* vv_renderer_ctx(vv_renderer* r);

@@ -89,6 +89,23 @@ class PagingRef:
         self.lru.move_to_end(s)
         self.uploaded.append(n)
 
+    def set_state(self, lru_order, xyz, slot) -> None:
+        """Start from a given paging state: the LRU order (slots, least
+        recently used first) and the resident nodes' slots.  The node words
+        passed to the constructor must already carry that residency."""
+        order = [int(s) for s in np.asarray(lru_order).reshape(-1)]
+        if sorted(order) != list(range(self.total)):
+            raise ValueError("the LRU order is not a permutation of the slots")
+        self.lru = OrderedDict((s, None) for s in order)
+        self.slot_node, self.node_slot = {}, {}
+        for p, s in zip(np.asarray(xyz).reshape(-1, 3), np.asarray(slot).reshape(-1)):
+            n = (int(p[0]), int(p[1]), int(p[2]))
+            self.slot_node[int(s)] = n
+            self.node_slot[n] = int(s)
+
+    def lru_order(self) -> np.ndarray:
+        return np.fromiter(self.lru.keys(), dtype=np.uint32, count=len(self.lru))
+
     def init(self, preload_all: bool) -> None:
         self.uploaded = []
         if preload_all:

@@ -51,6 +51,7 @@ def test_paged_camera_path_matches_oracle_and_policy(fmt, device_paging):
         xyz, slot = r.residency()
         got = {tuple(int(v) for v in p): int(s) for p, s in zip(xyz, slot)}
         assert got == sim.residency(), f"residency differs after frame {cam.frame}"
+        assert np.array_equal(r.lru_order(), sim.lru_order()), f"LRU order differs after frame {cam.frame}"
         st = r.stats()
         evicted = st["evictions_total"]
     assert evicted > 0, "the pool was never full: the check did not exercise eviction"

@@ -38,6 +38,7 @@ def _check_policy(r, ctx, sim, frame):
     xyz, slot = r.residency()
     got = {(int(p[0]), int(p[1]), int(p[2])): int(s) for p, s in zip(xyz, slot)}
     assert got == sim.residency(), f"residency differs from the policy after frame {frame}"
+    assert np.array_equal(r.lru_order(), sim.lru_order()), f"LRU order differs from the policy after frame {frame}"
     return words
 
 

@@ -380,6 +380,13 @@ class Context:
         self._ck(lib().vv_measure_footprint(self._h, tree, C.byref(u), C.byref(n), C.byref(b)), "footprint")
         return n.value, b.value
 
+    def footprint_union(self, us: Sequence[Uniforms], tree: int = 0) -> tuple[int, int]:
+        """The footprint of the union of several draws' reads."""
+        arr = (Uniforms * len(us))(*us)
+        n, b = C.c_int64(), C.c_int64()
+        self._ck(lib().vv_measure_footprint_views(self._h, tree, arr, len(us), C.byref(n), C.byref(b)), "footprint")
+        return n.value, b.value
+
     def render(self, u: Uniforms, color=0, usage=0, mask=0, requests=0, request_count=0, request_cap=0,
                compress_max_push=4, passes=VV_PASS_ALL, tree: int = 0) -> None:
         """One draw; every buffer argument is a device pointer (int) or 0."""
@@ -571,6 +578,14 @@ class Renderer:
         slot = np.zeros(n.value, dtype=np.uint32)
         self._ck(lib().vv_renderer_residency(self._h, _ptr(xyz), _ptr(slot), n.value, C.byref(n)), "residency")
         return xyz, slot
+
+    def lru_order(self) -> np.ndarray:
+        """The brick pool's slots, least recently used first."""
+        n = C.c_int64(0)
+        self._ck(lib().vv_renderer_lru_order(self._h, None, 0, C.byref(n)), "lru order")
+        out = np.zeros(n.value, dtype=np.uint32)
+        self._ck(lib().vv_renderer_lru_order(self._h, _ptr(out), n.value, C.byref(n)), "lru order")
+        return out
 
     def last_uniforms(self) -> Uniforms:
         u = Uniforms()

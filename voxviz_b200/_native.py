@@ -293,6 +293,8 @@ SIGNATURES = {
     "vv_ctx_last_times": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "vv_measure_footprint": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int64)]),
+    "vv_measure_footprint_views": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.c_int32, C.POINTER(C.c_int64),
+                                             C.POINTER(C.c_int64)]),
     "vv_octree_build_terrain": (C.c_int, [C.POINTER(TerrainDesc), C.POINTER(P)]),
     "vv_octree_destroy": (None, [P]),
     "vv_octree_get_info": (C.c_int, [P, C.POINTER(OctreeInfo)]),
@@ -335,6 +337,7 @@ SIGNATURES = {
     "vv_renderer_read_lists": (C.c_int, [P, P, P]),
     "vv_renderer_last_requests": (C.c_int, [P, P, C.c_int32, i32p]),
     "vv_renderer_residency": (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),
+    "vv_renderer_lru_order": (C.c_int, [P, P, C.c_int64, C.POINTER(C.c_int64)]),
     "vv_renderer_last_uniforms": (C.c_int, [P, C.POINTER(Uniforms)]),
     "vv_renderer_ctx": (P, [P]),
 }

@@ -475,6 +475,16 @@ int vv_renderer_residency(const vv_renderer* r, uint32_t* out_xyz, uint32_t* out
     return VV_OK;
 }
 
+int vv_renderer_lru_order(vv_renderer* r, uint32_t* out, int64_t cap, int64_t* n) {
+    if (!r || !n || cap < 0) return VV_ERR_ARG;
+    std::vector<uint32_t> order;
+    const int rc = r->impl->lru_order(order);
+    if (rc) return rc;
+    *n = (int64_t)order.size();
+    if (out) std::memcpy(out, order.data(), (size_t)std::min<int64_t>(cap, (int64_t)order.size()) * 4);
+    return VV_OK;
+}
+
 int vv_renderer_last_uniforms(const vv_renderer* r, vv_uniforms* out) {
     if (!r || !out) return VV_ERR_ARG;
     *out = r->impl->last_uniforms();

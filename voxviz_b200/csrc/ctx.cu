@@ -672,44 +672,55 @@ int vv_ctx_last_times(vv_ctx* c, float* raycast_ms, float* compact_ms) {
     return VV_OK;
 }
 
-int vv_measure_footprint(vv_ctx* c, int32_t tree, const vv_uniforms* u, int64_t* nodes, int64_t* bricks) {
-    if (!c || !u || tree < 0 || tree >= VV_MAX_TREES) return fail(c, VV_ERR_ARG, "bad footprint arguments");
+int vv_measure_footprint_views(vv_ctx* c, int32_t tree, const vv_uniforms* us, int32_t n, int64_t* nodes,
+                               int64_t* bricks) {
+    if (!c || !us || n <= 0 || tree < 0 || tree >= VV_MAX_TREES) return fail(c, VV_ERR_ARG, "bad footprint arguments");
     const DeviceTree& t = c->trees[tree];
     if (!t.nodes || !c->bricks) return fail(c, VV_ERR_STATE, "pools not ready");
-    if (u->jitter_tex_size != c->jitter_size) return fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
+    for (int32_t i = 0; i < n; ++i)
+        if (us[i].jitter_tex_size != c->jitter_size)
+            return fail(c, VV_ERR_ARG, "jitter_tex_size does not match the table");
     cudaSetDevice(c->device);
     const size_t nwords = (t.cells + 31) / 32, bwords = ((size_t)c->total_slots + 31) / 32;
     uint32_t* bits = nullptr;
     VV_CUDA(c, cudaMalloc(&bits, (nwords + bwords) * 4));
-    cudaMemsetAsync(bits, 0, (nwords + bwords) * 4, c->stream);
-    RaycastParams p;
-    std::memset(&p, 0, sizeof(p));
-    p.u = *u;
-    set_divisors(p);
-    p.nodes = t.nodes;
-    for (int a = 0; a < 3; ++a) {
-        p.node_dim[a] = t.dim[a];
-        p.slots[a] = c->slots[a];
+    cudaError_t e = cudaMemsetAsync(bits, 0, (nwords + bwords) * 4, c->stream);
+    // one counting ray cast per view into the same touch bitmaps: the union
+    for (int32_t i = 0; i < n && e == cudaSuccess; ++i) {
+        RaycastParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.u = us[i];
+        set_divisors(p);
+        p.nodes = t.nodes;
+        for (int a = 0; a < 3; ++a) {
+            p.node_dim[a] = t.dim[a];
+            p.slots[a] = c->slots[a];
+        }
+        p.bricks = c->bricks;
+        p.jitter = c->d_jitter;
+        p.status = c->d_status;
+        p.max_iter = vv_max_iterations(&us[i]);
+        p.u.compute_lighting = 0;  // lighting reads the same slots of the gradient pool
+        p.node_touch = bits;
+        p.brick_touch = bits + nwords;
+        e = launch_raycast_any(c, p);
     }
-    p.bricks = c->bricks;
-    p.jitter = c->d_jitter;
-    p.status = c->d_status;
-    p.max_iter = vv_max_iterations(u);
-    p.u.compute_lighting = 0;  // lighting reads the same slots of the gradient pool
-    p.node_touch = bits;
-    p.brick_touch = bits + nwords;
-    cudaError_t e = launch_raycast_any(c, p);
     std::vector<uint32_t> h(nwords + bwords);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), bits, h.size() * 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(bits);
     if (e != cudaSuccess) return cuda_fail(c, e, "footprint");
-    int64_t n = 0, b = 0;
-    for (size_t i = 0; i < nwords; ++i) n += __builtin_popcount(h[i]);
+    int64_t nn = 0, b = 0;
+    for (size_t i = 0; i < nwords; ++i) nn += __builtin_popcount(h[i]);
     for (size_t i = 0; i < bwords; ++i) b += __builtin_popcount(h[nwords + i]);
-    if (nodes) *nodes = n;
+    if (nodes) *nodes = nn;
     if (bricks) *bricks = b;
     return VV_OK;
+}
+
+int vv_measure_footprint(vv_ctx* c, int32_t tree, const vv_uniforms* u, int64_t* nodes, int64_t* bricks) {
+    if (!u) return fail(c, VV_ERR_ARG, "bad footprint arguments");
+    return vv_measure_footprint_views(c, tree, u, 1, nodes, bricks);
 }
 
 }  // extern "C"

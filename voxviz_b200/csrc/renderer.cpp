@@ -998,6 +998,21 @@ void GigaVoxelsRenderer::stats(vv_renderer_stats& s) const {
     s.unique_nodes = unique_;
 }
 
+int GigaVoxelsRenderer::lru_order(std::vector<uint32_t>& out) {
+    int rc = flush_touches();
+    if (rc) return rc;
+    const uint32_t n = total_slots_;
+    out.resize(n);
+    const uint32_t* d = order_.order[order_.cur];
+    if (cudaMemcpyAsync(out.data(), d + head_, (size_t)(n - head_) * 4, cudaMemcpyDeviceToHost, ctx_->stream) !=
+            cudaSuccess ||
+        (head_ && cudaMemcpyAsync(out.data() + (n - head_), d, (size_t)head_ * 4, cudaMemcpyDeviceToHost,
+                                  ctx_->stream) != cudaSuccess) ||
+        cudaStreamSynchronize(ctx_->stream) != cudaSuccess)
+        return VV_ERR_CUDA;
+    return VV_OK;
+}
+
 void GigaVoxelsRenderer::residency(std::vector<uint32_t>& xyz, std::vector<uint32_t>& slot) const {
     xyz.clear();
     slot.clear();

@@ -60,6 +60,9 @@ public:
     // when the device-side service did not need it on the host).
     int last_requests(std::vector<uint32_t>& out);
     void residency(std::vector<uint32_t>& xyz, std::vector<uint32_t>& slot) const;
+    // The brick pool's slots, least recently used first (pending host
+    // touches applied first).
+    int lru_order(std::vector<uint32_t>& out);
 
     float* d_color = nullptr;
     uint32_t* d_usage = nullptr;
