@@ -282,6 +282,28 @@ int vv_render_forward_ckpt(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, floa
                            void* ckpt, int32_t per_ray);
 int vv_backward(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl_dcolor,
                 const void* ckpt, int32_t per_ray, float* grad_texels);
+/* Where vv_backward_ex adds the gradient.  `grad` holds 1000 texels per row,
+ * 4 floats per texel, or 4 doubles with VV_GRAD_F64 (a binary64 reduction of
+ * the per-sample contributions, for gradient checks).  With slot_map NULL
+ * row = brick-pool slot (the dense layout of vv_backward).  With a slot map
+ * (device, one int32 per pool slot, set to -1 by the caller before the
+ * first call) the gradient is sparse: the first sample that reaches a slot
+ * claims the next row (counter `rows_used`, device int32, zeroed by the
+ * caller) and writes it into the map, so only touched slots take rows; the
+ * caller zeroes the first `rows_cap` rows.  Running out of rows sets
+ * VV_ERR_OOM in the device status (vv_ctx_device_status) and drops the
+ * contributions that found no row.  Row order depends on timing; the map
+ * tells which slot each row holds. */
+#define VV_GRAD_F64 1
+typedef struct vv_grad_desc {
+    void* grad;
+    int32_t flags;
+    int32_t rows_cap;
+    int32_t* slot_map;
+    int32_t* rows_used;
+} vv_grad_desc;
+int vv_backward_ex(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl_dcolor,
+                   const void* ckpt, int32_t per_ray, const vv_grad_desc* g);
 /* Use caller-owned device memory (e.g. a torch tensor) as the brick pool:
  * slots_x*slots_y*slots_z*1000 texels of `fmt` at `texels`; the context does
  * not free it.  Replaces vv_brickpool_create for differentiable use. */

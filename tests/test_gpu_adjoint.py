@@ -5,9 +5,14 @@ torch.autograd.Function.
 * dL/d(texel) matches the oracle's binary64 adjoint of the same binary32
   ray cast to 1e-3 relative (per texel, for texels above 1e-3 of the largest
   gradient; FP32 atomics are the only difference);
-* the autograd gradient matches central finite differences (h = 1e-3) of
-  the loss, reduced in float64 on the GPU, within the FP32 rounding of the
-  perturbed forward (stated below);
+* binary64 accumulation (VV_GRAD_F64) and the sparse gradient (rows per
+  touched slot) give the dense gradient;
+* with binary64 accumulation the gradient matches central differences
+  (h = 1e-3) of the binary64 functional along the fixed control flow within
+  1e-3 relative on random texels;
+* the autograd gradient matches central differences of the binary32 GPU
+  forward within 1e-3 relative plus that forward's rounding, probes that
+  change the control flow set aside;
 * a few Adam steps through the Function reduce an L2 image loss.
 """
 import numpy as np
@@ -78,7 +83,145 @@ def test_backward_matches_fp64_oracle(fp32_scene, per_ray):
     assert np.abs(got - ref).max() <= 1e-5 * scale
 
 
-def test_autograd_matches_finite_differences(fp32_scene):
+def _backward_variants(g, u, ck, per_ray, dl_t, n_slots):
+    """The adjoint of one view four ways: dense float, dense binary64, and
+    sparse rows (slot map) in float and in binary64; the sparse ones are
+    scattered back to slots.  Returns {name: (slots, 1000, 4) float64} and
+    the rows each sparse call claimed."""
+    dev = torch.device("cuda", 0)
+    out, rows = {}, {}
+    dense = torch.zeros((n_slots, 1000, 4), dtype=torch.float32, device=dev)
+    g.ctx.backward(u, dl_t.data_ptr(), ck.data_ptr(), per_ray, dense.data_ptr())
+    out["dense_f32"] = dense.double()
+    d64 = torch.zeros((n_slots, 1000, 4), dtype=torch.float64, device=dev)
+    g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), per_ray, d64.data_ptr(), f64=True)
+    out["dense_f64"] = d64
+    for f64 in (False, True):
+        cap = n_slots
+        rowbuf = torch.zeros((cap, 1000, 4), dtype=torch.float64 if f64 else torch.float32, device=dev)
+        smap = torch.full((n_slots,), -1, dtype=torch.int32, device=dev)
+        used = torch.zeros(1, dtype=torch.int32, device=dev)
+        g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), per_ray, rowbuf.data_ptr(), f64=f64,
+                          slot_map=smap.data_ptr(), rows_used=used.data_ptr(), rows_cap=cap)
+        torch.cuda.synchronize()
+        n = int(used.item())
+        m = smap.cpu().numpy()
+        assert set(np.unique(m[m >= 0])) == set(range(n))       # rows 0..n-1, one slot each
+        full = torch.zeros((n_slots, 1000, 4), dtype=torch.float64, device=dev)
+        sl = torch.from_numpy(np.nonzero(m >= 0)[0]).to(dev)
+        full[sl] = rowbuf[smap[sl].long()].double()
+        out["rows_f64" if f64 else "rows_f32"] = full
+        rows["rows_f64" if f64 else "rows_f32"] = n
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in out.items()}, rows
+
+
+def test_backward_binary64_and_sparse_rows(fp32_scene):
+    """vv_backward_ex: binary64 accumulation and the sparse gradient (rows
+    claimed by touched slots) give the dense gradient; the binary64 one
+    matches the oracle's binary64 adjoint to float rounding of the
+    per-sample contributions."""
+    from oracle import gv_oracle as go
+    sc, g = fp32_scene
+    n_slots = int(np.prod(sc.slots))
+    for seed, (w, h) in ((5, (96, 64)), (8, (160, 120))):
+        u = sc.uniforms(sc.view(seed, w, h))
+        _, ck = _ckpt_color(g, u, 16)
+        rng = np.random.default_rng(seed)
+        dl = rng.standard_normal((h, w, 4)).astype(np.float32)
+        dl_t = torch.from_numpy(dl).cuda()
+        got, rows = _backward_variants(g, u, ck, 16, dl_t, n_slots)
+        assert g.ctx.device_status() == 0
+        ref = go.backward(u, sc.oracle_scene(), dl)
+        scale = np.abs(ref).max()
+        touched = np.abs(ref).reshape(n_slots, -1).max(axis=1) > 0
+        for name, v in got.items():
+            assert np.array_equal(v != 0, ref != 0), name
+            assert np.abs(v - ref).max() <= 1e-5 * scale, (name, np.abs(v - ref).max() / scale)
+        for name, n in rows.items():
+            assert n >= int(touched.sum()) and n <= n_slots
+        # binary64 accumulation: relative error 1e-5 even on texels far below the largest
+        big = np.abs(ref) > 1e-6 * scale
+        rel = np.abs(got["dense_f64"] - ref)[big] / np.abs(ref)[big]
+        assert rel.max() <= 1e-3, rel.max()
+
+
+def test_sparse_rows_report_overflow(fp32_scene):
+    """Fewer rows than touched slots: VV_ERR_OOM in the device status."""
+    sc, g = fp32_scene
+    u = sc.uniforms(sc.view(5, 96, 64))
+    _, ck = _ckpt_color(g, u, 16)
+    dl_t = torch.ones((64, 96, 4), dtype=torch.float32, device="cuda")
+    n_slots = int(np.prod(sc.slots))
+    rowbuf = torch.zeros((2, 1000, 4), dtype=torch.float32, device="cuda")
+    smap = torch.full((n_slots,), -1, dtype=torch.int32, device="cuda")
+    used = torch.zeros(1, dtype=torch.int32, device="cuda")
+    g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), 16, rowbuf.data_ptr(), slot_map=smap.data_ptr(),
+                      rows_used=used.data_ptr(), rows_cap=2)
+    g.ctx.synchronize()
+    from voxviz_b200 import _native as N
+    assert g.ctx.device_status(clear=True) == N.VV_ERR_OOM
+    assert int((smap >= 0).sum()) == 2
+
+
+def test_gradient_matches_central_differences_of_binary64_functional(fp32_scene):
+    """The adjoint against central differences (h = 1e-3): dL/d(texel) of
+    F = sum over pixels of dL/dc * c (dL/dc held at the forward's value, so
+    its texel gradient is exactly what the adjoint returns) with c composited
+    in binary64 along the binary32 sample sequence (the control flow the
+    adjoint holds fixed), at 96 random texels with a non-zero gradient, not
+    only the largest.  The GPU reduces its per-sample contributions in
+    binary64 (VV_GRAD_F64).  Every texel within 1e-3 relative."""
+    from oracle import gv_oracle as go
+    sc, g = fp32_scene
+    n_slots = int(np.prod(sc.slots))
+    us = [sc.uniforms(sc.view(s, 128, 96)) for s in (3, 5)]
+    rng = np.random.default_rng(0)
+    targets = rng.uniform(0, 1, (2, 96, 128, 4))
+    grad = torch.zeros((n_slots, 1000, 4), dtype=torch.float64, device="cuda")
+    dls = []
+    for u, t in zip(us, targets):
+        c, ck = _ckpt_color(g, u, 16)
+        dl = (2.0 * (c.double().cpu().numpy() - t)).astype(np.float32)
+        dls.append(dl)
+        g.ctx.backward_ex(u, torch.from_numpy(dl).cuda().data_ptr(), ck.data_ptr(), 16, grad.data_ptr(), f64=True)
+    g.ctx.synchronize()
+    assert g.ctx.device_status() == 0
+    an_all = grad.cpu().numpy()
+    nz = np.argwhere(an_all != 0)
+    pick = nz[rng.choice(len(nz), size=96, replace=False)]
+    traj = sc.oracle_scene()
+    vals_pool = np.array(sc.pool, copy=True)
+    flat = vals_pool.view(np.float32).reshape(-1)
+    vals = sc.oracle_scene(pool=vals_pool)
+    h = np.float32(1e-3)
+    rel = []
+    for s_, t_, ch in pick:
+        i = (int(s_) * 1000 + int(t_)) * 4 + int(ch)
+        old = flat[i]
+        flat[i] = old + h
+        up = float(flat[i])
+        f1 = sum(float((dl.astype(np.float64) * go.fixed_path(u, traj, vals)).sum()) for u, dl in zip(us, dls))
+        flat[i] = old - h
+        dn = float(flat[i])
+        f2 = sum(float((dl.astype(np.float64) * go.fixed_path(u, traj, vals)).sum()) for u, dl in zip(us, dls))
+        flat[i] = old
+        fd = (f1 - f2) / (up - dn)
+        an = float(an_all[s_, t_, ch])
+        rel.append(abs(fd - an) / abs(an))
+    rel = np.array(rel)
+    assert rel.max() <= 1e-3, (rel.max(), np.median(rel))
+
+
+def test_autograd_gradient_within_fp32_forward_resolution(fp32_scene):
+    """The autograd gradient against central differences (h = 1e-3) of the
+    binary32 GPU forward with the loss reduced in binary64 on the GPU.  A
+    probe whose +-h renders change the control flow (a ray's composited
+    sample count moves: the alpha stop crossed) has no derivative there and
+    is set aside (counted); on the others the difference is within 1e-3
+    relative plus the forward's binary32 resolution (each affected pixel's
+    colour is rounded to 2^-24 relative per channel: |dL/dc| * ulp(c) per
+    pixel, summed, over 2h)."""
     from voxviz_b200 import diff
     sc, g = fp32_scene
     ctx = vv.Context(0)
@@ -96,29 +239,48 @@ def test_autograd_matches_finite_differences(fp32_scene):
     loss64(c).backward()
     assert diff.check_status(ctx) == 0
     grad = pool.grad.detach().double()
+    dlc = (2.0 * (c.detach().double() - target.double())).abs()
+
+    def samples(p):
+        # composited sample count per pixel of every view (the checkpoint header)
+        diff.attach_pool(ctx, p, sc.slots)
+        out = []
+        for u in us:
+            col = torch.empty((96, 128, 4), dtype=torch.float32, device="cuda")
+            ck = torch.empty(vv.Context.ckpt_bytes(128, 96, 4), dtype=torch.uint8, device="cuda")
+            ctx.forward_ckpt(u, col.data_ptr(), ck.data_ptr(), 4)
+            hdr = ck[: 96 * 128 * 8].view(torch.int32).view(96, 128, 2)[..., 1].clone()
+            out.append((col, hdr))
+        return out
+
     flat = grad.abs().flatten()
-    idx = torch.topk(flat, 64).indices.cpu().numpy()
+    nz = torch.nonzero(flat).flatten().cpu().numpy()
+    idx = rng.choice(nz, size=64, replace=False)
     h = 1e-3
-    fd, an = [], []
+    base = pool.detach().clone()
+    n_flip, checked = 0, 0
     with torch.no_grad():
-        base = pool.detach().clone()
+        r0 = samples(base)
         for i in idx:
             p1 = base.clone().flatten()
             p1[i] += h
             p2 = base.clone().flatten()
             p2[i] -= h
-            l1 = loss64(diff.render(p1.view_as(base), ctx, sc.slots, us))
-            l2 = loss64(diff.render(p2.view_as(base), ctx, sc.slots, us))
-            fd.append(float((l1 - l2) / (2 * h)))
-            an.append(float(grad.flatten()[i]))
-    fd, an = np.array(fd), np.array(an)
-    # FP32 rounding of the perturbed colours: |dc| <= 2^-24 per channel of
-    # the affected pixels, so the FD itself carries ~1e-3 relative noise on
-    # the largest gradients; a control-flow change (a ray crossing the
-    # alpha stop) shows as a jump, which these texels do not cause.
-    rel = np.abs(fd - an) / np.abs(an)
-    assert np.median(rel) <= 1e-3, np.median(rel)
-    assert (rel <= 1e-2).mean() >= 0.95, rel
+            r1, r2 = samples(p1.view_as(base)), samples(p2.view_as(base))
+            if any(not torch.equal(a[1], b[1]) or not torch.equal(a[1], c_[1]) for a, b, c_ in zip(r0, r1, r2)):
+                n_flip += 1
+                continue
+            c1 = torch.stack([a[0] for a in r1])
+            c2 = torch.stack([a[0] for a in r2])
+            fd = float((loss64(c1) - loss64(c2)) / (2 * h))
+            an = float(grad.flatten()[i])
+            # binary32 resolution of the two renders, on the pixels that changed
+            changed = (c1 != c2)
+            ulp = torch.abs(torch.stack([c1, c2])).max(0).values.double() * 2.0 ** -23
+            floor = float((dlc * ulp)[changed].sum()) / (2 * h)
+            assert abs(fd - an) <= 1e-3 * abs(an) + floor, (i, fd, an, floor)
+            checked += 1
+    assert checked >= 48, (checked, n_flip)
     assert diff.check_status(ctx) == 0
 
 

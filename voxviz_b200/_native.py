@@ -233,6 +233,14 @@ class RendererStats(C.Structure):
     ]
 
 
+class GradDesc(C.Structure):
+    _fields_ = [("grad", C.c_void_p), ("flags", C.c_int32), ("rows_cap", C.c_int32), ("slot_map", C.c_void_p),
+                ("rows_used", C.c_void_p)]
+
+
+VV_GRAD_F64 = 1
+
+
 class BatchView(C.Structure):
     _fields_ = [
         ("ctx", C.c_void_p),
@@ -285,6 +293,7 @@ SIGNATURES = {
     "vv_ckpt_bytes": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "vv_render_forward_ckpt": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32]),
     "vv_backward": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32, P]),
+    "vv_backward_ex": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32, C.POINTER(GradDesc)]),
     "vv_brickpool_attach": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "vv_batch_variants": (C.c_int32, [C.POINTER(BatchConfig), C.c_int32]),
     "vv_render_batch": (C.c_int, [P, C.POINTER(BatchView), C.c_int32, C.POINTER(BatchConfig)]),

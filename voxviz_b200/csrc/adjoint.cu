@@ -74,9 +74,75 @@ struct ReplayVisitor {
     __device__ __forceinline__ void fail(int) {}
 };
 
+// The row of the gradient that holds `slot`: the slot itself (dense), or,
+// with a slot map, the row claimed by the first sample that reaches the
+// slot (-1 in the map: unclaimed; -2: being claimed; -3: no row left).
+// The claiming thread never waits, so a waiting thread's bound is never
+// reached on valid data; reaching it, or running out of rows, sets the
+// device status and drops the contribution.
+__device__ __forceinline__ int grad_row(const GradTarget& gt, uint32_t slot, int* status) {
+    if (!gt.slot_map) return (int)slot;
+    int* m = gt.slot_map + slot;
+    int r = *(volatile int*)m;
+    if (r >= 0) return r;
+    if (r == -1 && atomicCAS(m, -1, -2) == -1) {
+        const int nr = atomicAdd(gt.rows_used, 1);
+        if (nr >= gt.rows_cap) {
+            atomicExch(m, -3);
+            set_status(status, VV_ERR_OOM);
+            return -1;
+        }
+        __threadfence();
+        atomicExch(m, nr);
+        return nr;
+    }
+    for (int i = 0; i < (1 << 22); ++i) {
+        r = *(volatile int*)m;
+        if (r >= 0) return r;
+        if (r == -3) return -1;
+        __nanosleep(64);
+    }
+    set_status(status, VV_ERR_TIMEOUT);
+    return -1;
+}
+
+// gradient += d at texel `i` of row `row`: lanes of a warp adding to the same
+// texel are summed by shuffles first and the sum goes out in one atomic
+// (coherent rays often sample the same brick cells at once).
+__device__ __forceinline__ void add_texel(const GradTarget& gt, int row, uint32_t t, float4 d) {
+    const uint64_t key = ((uint64_t)(uint32_t)row << 10) | t;
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, key);
+    const int leader = __ffs(peers) - 1;
+    const int lane = threadIdx.x & 31;
+    if (__popc(peers) > 1) {
+        // sum over the peers in lane order (a fixed order for a fixed set)
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (unsigned m = peers; m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            s.x += __shfl_sync(peers, d.x, src);
+            s.y += __shfl_sync(peers, d.y, src);
+            s.z += __shfl_sync(peers, d.z, src);
+            s.w += __shfl_sync(peers, d.w, src);
+        }
+        d = s;
+    }
+    if (lane != leader) return;
+    const size_t i = (size_t)row * 1000u + t;
+    if (gt.f64) {
+        double* g = (double*)gt.grad + 4 * i;
+        atomicAdd(g + 0, (double)d.x);
+        atomicAdd(g + 1, (double)d.y);
+        atomicAdd(g + 2, (double)d.z);
+        atomicAdd(g + 3, (double)d.w);
+    } else {
+        atomicAdd((float4*)gt.grad + i, d);
+    }
+}
+
 // dL/d texel += w_j * d for the 8 taps of the sample at uvw (the addressing
 // of sample_brick, clamps included: clamped taps share a texel).
-__device__ __forceinline__ void scatter_texels(const RaycastParams& p, F3 uvw, float4 d, float4* grad) {
+__device__ __forceinline__ void scatter_texels(const RaycastParams& p, F3 uvw, float4 d, const GradTarget& gt) {
     const float* N = p.u.brick_pool_dimension;
     const Axis ax = axis_taps(uvw.x, N[0], p.slots[0] * 10);
     const Axis ay = axis_taps(uvw.y, N[1], p.slots[1] * 10);
@@ -91,8 +157,9 @@ __device__ __forceinline__ void scatter_texels(const RaycastParams& p, F3 uvw, f
         const int sy = by ? ay.s1 : ay.s0, ly = by ? ay.l1 : ay.l0;
         const int sz = bz ? az.s1 : az.s0, lz = bz ? az.l1 : az.l0;
         const uint32_t slot = ((uint32_t)sz * SY + (uint32_t)sy) * SX + (uint32_t)sx;
-        const uint32_t i = slot * 1000u + (uint32_t)((lz * 10 + ly) * 10 + lx);
-        atomicAdd(grad + i, make_float4(w * d.x, w * d.y, w * d.z, w * d.w));
+        const int row = grad_row(gt, slot, p.status);
+        if (row < 0) continue;
+        add_texel(gt, row, (uint32_t)((lz * 10 + ly) * 10 + lx), make_float4(w * d.x, w * d.y, w * d.z, w * d.w));
     }
 }
 
@@ -140,7 +207,7 @@ __global__ void __launch_bounds__(128, 7) forward_ckpt_kernel(const __grid_const
 template <int FMT>
 __global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
                                                        const Ckpt* ckpt, int per_ray, const float4* dl_dcolor,
-                                                       float4* grad) {
+                                                       const GradTarget gt) {
     int px, py;
     pixel_of(px, py);
     const vv_uniforms& u = p.u;
@@ -181,7 +248,7 @@ __global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant_
             for (int j = rv.n - 1; j >= 0; --j) {
                 const float t = rv.T[j];
                 const float4 sv = rv.src[j];
-                if (rv.brick[j]) scatter_texels(p, rv.bpos[j], make_float4(g.x * t, g.y * t, g.z * t, g.w * t), grad);
+                if (rv.brick[j]) scatter_texels(p, rv.bpos[j], make_float4(g.x * t, g.y * t, g.z * t, g.w * t), gt);
                 g.w = g.w - (g.x * sv.x + g.y * sv.y + g.z * sv.z + g.w * sv.w);
             }
         }
@@ -208,7 +275,7 @@ cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int
 }
 
 cudaError_t launch_backward(int fmt, const RaycastParams& p, const void* ckpt, int per_ray, const float4* dl_dcolor,
-                            float4* grad, cudaStream_t s) {
+                            const GradTarget& grad, cudaStream_t s) {
     const int W = p.u.width, H = p.u.height;
     const int2* hdr = (const int2*)ckpt;
     const Ckpt* ck = (const Ckpt*)((const char*)ckpt + (size_t)W * H * sizeof(int2));

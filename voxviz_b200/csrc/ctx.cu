@@ -500,14 +500,32 @@ int vv_render_forward_ckpt(vv_ctx* c, int32_t tree, const vv_uniforms* u, float*
 
 int vv_backward(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* dl_dcolor, const void* ckpt,
                 int32_t per_ray, float* grad_texels) {
+    vv_grad_desc g;
+    std::memset(&g, 0, sizeof(g));
+    g.grad = grad_texels;
+    return vv_backward_ex(c, tree, u, dl_dcolor, ckpt, per_ray, &g);
+}
+
+int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* dl_dcolor, const void* ckpt,
+                   int32_t per_ray, const vv_grad_desc* g) {
     RaycastParams p;
     int rc = diff_params(c, tree, u, p);
     if (rc) return rc;
-    if (!ckpt || per_ray <= 0 || !dl_dcolor || !grad_texels) return fail(c, VV_ERR_ARG, "bad backward buffers");
-    if (((uintptr_t)grad_texels & 15u) != 0 || ((uintptr_t)dl_dcolor & 15u) != 0)
-        return fail(c, VV_ERR_ARG, "gradient buffers must be 16-byte aligned");
+    if (!ckpt || per_ray <= 0 || !dl_dcolor || !g || !g->grad) return fail(c, VV_ERR_ARG, "bad backward buffers");
+    if ((g->flags & ~VV_GRAD_F64) != 0) return fail(c, VV_ERR_ARG, "unknown gradient flags");
+    const uintptr_t align = (g->flags & VV_GRAD_F64) ? 32u : 16u;
+    if (((uintptr_t)g->grad & (align - 1)) != 0 || ((uintptr_t)dl_dcolor & 15u) != 0)
+        return fail(c, VV_ERR_ARG, "gradient buffers must be aligned to a texel (16 bytes, 32 for binary64)");
+    if (g->slot_map && (!g->rows_used || g->rows_cap <= 0))
+        return fail(c, VV_ERR_ARG, "a slot map needs a row counter and a row capacity");
     cudaSetDevice(c->device);
-    VV_CUDA(c, launch_backward(c->fmt, p, ckpt, per_ray, (const float4*)dl_dcolor, (float4*)grad_texels, c->stream));
+    GradTarget gt;
+    gt.grad = g->grad;
+    gt.f64 = (g->flags & VV_GRAD_F64) ? 1 : 0;
+    gt.slot_map = g->slot_map;
+    gt.rows_used = g->rows_used;
+    gt.rows_cap = g->slot_map ? g->rows_cap : 0;
+    VV_CUDA(c, launch_backward(c->fmt, p, ckpt, per_ray, (const float4*)dl_dcolor, gt, c->stream));
     return VV_OK;
 }
 

@@ -62,8 +62,19 @@ cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s);
 // Differentiable forward (colour + per-ray checkpoints) and its adjoint.
 size_t ckpt_bytes(int w, int h, int per_ray);
 cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int per_ray, cudaStream_t s);
+// Where the adjoint adds dL/d(texel): `grad` holds 4 floats (or, with f64,
+// 4 doubles) per texel, 1000 texels per row; row = brick-pool slot (dense,
+// slot_map NULL) or the row the slot map assigns (claimed on first touch
+// from rows_used, at most rows_cap rows).
+struct GradTarget {
+    void* grad;
+    int f64;
+    int* slot_map;
+    int* rows_used;
+    int rows_cap;
+};
 cudaError_t launch_backward(int fmt, const RaycastParams& p, const void* ckpt, int per_ray, const float4* dl_dcolor,
-                            float4* grad, cudaStream_t s);
+                            const GradTarget& grad, cudaStream_t s);
 cudaError_t launch_select(const uint4* usage, uint32_t* mask, uint32_t* level0, int w, int h,
                           cudaStream_t s);
 cudaError_t launch_compact(const CompactParams& p, cudaStream_t s);
