@@ -348,15 +348,17 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
             "loss": "sum(colour^2); bwd = elementwise dL/dc + slot-map reset + row zeroing + adjoint kernel"}
 
 
-BATCH16_VIEWS, BATCH16_POOL_BYTES = 16, 4 << 30
+# 1,040,502 FP16 slots (8000 B each, 102x101x101): near the 102^3 slots 10-bit
+# brick pointers address, enough for the 16 views' bricks to converge
+BATCH16_VIEWS, BATCH16_POOL_BYTES = 16, 8_324_000_000
 
 
 def batched_fp16_leg(vv, octree, cams, device, peak):
     """The batched FP16-pool forward on the paged 8192^3 terrain: 16 1080p
     frames spread over the path rendered by one persistent launch (autotuned
-    tile shape and samples per loop trip) from a 4 GiB FP16 brick pool
-    (536,870 slots) with paging run over the 16 views until it converges (or
-    for 12 passes), against the same views as per-view launches."""
+    tile shape and samples per loop trip) from an 8.3 GB FP16 brick pool
+    (1,040,502 slots) with paging run over the 16 views until it converges
+    (or for 12 passes), against the same views as per-view launches."""
     import torch
 
     ctx = vv.Context(device)
@@ -540,6 +542,8 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(WIDTH * HEIGHT * 16 + 8 + requests / args.steps * 4 * 4)},
         "roofline": roofline,
         "kernels": {"raycast_ms_mean": round(ray_mean, 3),
+                    "raycast_ms_min_median_max": [round(float(np.min(ray_ms)), 3), round(float(np.median(ray_ms)), 3),
+                                                  round(float(np.max(ray_ms)), 3)],
                     "raycast_mrays_s": round(WIDTH * HEIGHT / (ray_mean / 1e3) / 1e6, 1),
                     "select_compact_ms_mean": round(float(np.mean(cmp_ms)), 3)},
         "paging": {"bricks_uploaded_per_frame": round(uploads / args.steps, 1),
@@ -754,6 +758,7 @@ def run_fit(args):
     # the per-brick gradient reduction of the checks in binary64 on the GPU
     g_gpu = torch.zeros(param.shape, dtype=torch.float64, device="cuda")
     g_ref = np.zeros((used, 1000, 4), dtype=np.float64)
+    g_abs = np.zeros((used, 1000, 4), dtype=np.float64)  # magnitude of the summed terms
     dl_np = {}
     for v, r0, r1 in bands:
         ctx.forward_ckpt(us[v], col.data_ptr(), ck.data_ptr(), per_ray)
@@ -761,7 +766,7 @@ def run_fit(args):
         dl[r0:r1] = 2.0 * (col[r0:r1] - target[v, r0:r1])
         ctx.backward_ex(us[v], dl.data_ptr(), ck.data_ptr(), per_ray, g_gpu.data_ptr(), f64=True)
         torch.cuda.synchronize()
-        go.backward(us[v], osc, dl.cpu().numpy(), rows=(r0, r1), grad=g_ref)
+        go.backward(us[v], osc, dl.cpu().numpy(), rows=(r0, r1), grad=g_ref, grad_abs=g_abs)
         dl_np[v] = dl[r0:r1].double().cpu().numpy()  # dL/dcolour of the band (held fixed)
     outside = int(torch.count_nonzero(g_gpu[used:]))
     if outside:
@@ -770,10 +775,16 @@ def run_fit(args):
     scale = float(np.abs(g_ref).max()) if bands else 0.0
     big = np.abs(g_ref) > 1e-3 * scale
     host_rel = (np.abs(got - g_ref)[big] / np.abs(g_ref)[big]) if bands else np.zeros(0)
+    nzr = g_ref != 0
+    within = np.abs(got - g_ref)[nzr] <= 1e-3 * np.abs(g_ref)[nzr] + 1e-5 * g_abs[nzr]
     host_report = {"bands": [list(b) for b in bands], "rows_per_band": 16, "texels_compared": int(big.sum()),
                    "rel_err_max": float(host_rel.max()) if host_rel.size else None,
                    "abs_err_max_over_max_grad": float(np.abs(got - g_ref).max() / scale) if scale else None,
-                   "criterion": "texels above 1e-3 of the largest gradient"}
+                   "criterion": "texels above 1e-3 of the largest gradient",
+                   "all_texels": int(nzr.sum()),
+                   "all_within_1e-3_plus_rounding": float(within.mean()) if within.size else None,
+                   "rounding": "1e-5 x the texel's sum of term magnitudes (binary32 per-sample terms)",
+                   "gpu_reduction": "binary64"}
     # every resident slot is below `used`, so g_ref covers all candidates
     picks_h, _ = fit_subvolume_texels(octree, r, g_ref, slots, 256, FIT_FD_SEED + 1)
     buf = np.zeros((FIT_SIZE, FIT_SIZE, 4), dtype=np.float64)
@@ -789,7 +800,7 @@ def run_fit(args):
     # the functional F = sum(dL/dc * c) over the bands, with dL/dc held at the
     # GPU's value: its texel gradient is exactly what the adjoint returned,
     # and its central difference is taken pixel by pixel (no cancellation)
-    fdh, anh = [], []
+    fdh, anh, magh = [], [], []
     t_fd = time.perf_counter()
     flat_vals = vals_pool.reshape(-1)
     for s_, t_, ch in picks_h:
@@ -805,18 +816,21 @@ def run_fit(args):
         num = sum(float((dl_np[v] * (a - b)).sum()) for (v, _, _), a, b in zip(bands, c1, c2))
         fdh.append(num / (up_ - dn_))
         anh.append(float(got[s_, t_, ch]))
-    fdh, anh = np.array(fdh), np.array(anh)
+        magh.append(float(g_abs[s_, t_, ch]))
+    fdh, anh, magh = np.array(fdh), np.array(anh), np.array(magh)
     relh = np.abs(fdh - anh) / np.maximum(np.abs(fdh), 1e-300)
     fd_host_report = {"texels": int(len(picks_h)), "h": h, "evaluation": "binary64 along the binary32 sample sequence",
                       "rel_err_median": float(np.median(relh)) if relh.size else None,
                       "rel_err_max": float(relh.max()) if relh.size else None,
                       "frac_within_1e-3": float((relh <= 1e-3).mean()) if relh.size else None,
-                      # binary32 accumulation of cancelling contributions: the error
+                      "frac_within_1e-3_plus_rounding": float(
+                          (np.abs(fdh - anh) <= 1e-3 * np.abs(fdh) + 1e-5 * magh).mean()) if relh.size else None,
+                      # binary32 per-sample terms that cancel: the error
                       # scaled by max(|fd|, 1e-3 * largest sampled gradient)
                       "scaled_rel_err_max": float((np.abs(fdh - anh) / np.maximum(
                           np.abs(fdh), 1e-3 * np.abs(fdh).max())).max()) if relh.size else None,
                       "seconds": round(time.perf_counter() - t_fd, 1)}
-    del traj_pool, vals_pool, got, g_ref
+    del traj_pool, vals_pool, got, g_ref, g_abs
     # ---- the fit: Adam on every pool texel, L2 image loss ----
     mine = vdist.views_of_rank(FIT_VIEWS, rank, world)
     us_mine, target_mine = [us[v] for v in mine], target[mine]

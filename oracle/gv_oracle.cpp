@@ -867,6 +867,11 @@ int oracle_fixed_path(const vv_uniforms* u, const oracle_scene* traj, const orac
 // doubles per pool texel (slot-major, brick-linear), added to.
 int oracle_backward(const vv_uniforms* u, const oracle_scene* s, const float* dl_dcolor, double* grad, int row0,
                     int row1) {
+    return oracle_backward_bound(u, s, dl_dcolor, grad, nullptr, row0, row1);
+}
+
+int oracle_backward_bound(const vv_uniforms* u, const oracle_scene* s, const float* dl_dcolor, double* grad,
+                          double* grad_abs, int row0, int row1) {
     if (!u || !s || !dl_dcolor || !grad || row0 < 0 || row1 > u->height || row0 > row1) return VV_ERR_ARG;
     Shader<float> sh;
     sh.init(u);
@@ -895,10 +900,16 @@ int oracle_backward(const vv_uniforms* u, const oracle_scene* s, const float* dl
             sh.main(x, y, c, lst);
             const float* gp = dl_dcolor + 4 * ((size_t)y * W + x);
             double g[4] = {gp[0], gp[1], gp[2], gp[3]};
+            // the same recurrence over absolute values: the magnitude that the
+            // terms summed into g and into each texel carry (a running bound
+            // for the rounding of an implementation in lower precision)
+            double ga[4] = {std::fabs(g[0]), std::fabs(g[1]), std::fabs(g[2]), std::fabs(g[3])};
             for (size_t k = tape.size(); k-- > 0;) {
                 const SampleRec& r = tape[k];
                 if (r.brick) {
                     const double d[4] = {g[0] * r.T, g[1] * r.T, g[2] * r.T, g[3] * r.T};
+                    const double da[4] = {ga[0] * std::fabs(r.T), ga[1] * std::fabs(r.T), ga[2] * std::fabs(r.T),
+                                          ga[3] * std::fabs(r.T)};
                     int i0[3], i1[3];
                     double f[3];
                     for (int a = 0; a < 3; ++a) {
@@ -917,9 +928,13 @@ int oracle_backward(const vv_uniforms* u, const oracle_scene* s, const float* dl
                         const size_t slot = ((size_t)(iz / 10) * s->slots[1] + (size_t)(iy / 10)) * s->slots[0] + (size_t)(ix / 10);
                         const size_t ti = slot * 1000 + (size_t)((iz % 10) * 100 + (iy % 10) * 10 + (ix % 10));
                         for (int ch = 0; ch < 4; ++ch) grad[4 * ti + ch] += w * d[ch];
+                        if (grad_abs)
+                            for (int ch = 0; ch < 4; ++ch) grad_abs[4 * ti + ch] += std::fabs(w) * da[ch];
                     }
                 }
                 g[3] = g[3] - (g[0] * r.src[0] + g[1] * r.src[1] + g[2] * r.src[2] + g[3] * r.src[3]);
+                ga[3] = ga[3] + (ga[0] * std::fabs(r.src[0]) + ga[1] * std::fabs(r.src[1]) +
+                                 ga[2] * std::fabs(r.src[2]) + ga[3] * std::fabs(r.src[3]));
             }
         }
     return st;

@@ -41,6 +41,13 @@ int oracle_fixed_path(const vv_uniforms* u, const oracle_scene* traj, const orac
  * given dL/d(colour) (4 floats per pixel).  Single-threaded. */
 int oracle_backward(const vv_uniforms* u, const oracle_scene* s, const float* dl_dcolor, double* grad,
                     int row0, int row1);
+/* oracle_backward, and when grad_abs is not NULL also ADDS to it the same
+ * sums over absolute values (|w| * |T| * |g| with g's alpha recurrence run
+ * on absolute values): per texel the magnitude of the terms whose sum is the
+ * gradient.  A lower-precision implementation's rounding error is bounded
+ * by a small multiple of its unit roundoff times this magnitude. */
+int oracle_backward_bound(const vv_uniforms* u, const oracle_scene* s, const float* dl_dcolor, double* grad,
+                          double* grad_abs, int row0, int row1);
 int oracle_select(const uint32_t* usage, int w, int h, uint32_t* mask);
 int oracle_compress(const uint32_t* usage, const uint32_t* mask, int w, int h, int max_push, int cap,
                     uint32_t* out, uint32_t* total);

@@ -59,6 +59,9 @@ def load() -> C.CDLL:
     lib.oracle_backward.restype = C.c_int
     lib.oracle_backward.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_void_p, C.c_void_p, C.c_int,
                                     C.c_int]
+    lib.oracle_backward_bound.restype = C.c_int
+    lib.oracle_backward_bound.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_int, C.c_int]
     lib.oracle_fixed_path.restype = C.c_int
     lib.oracle_fixed_path.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.POINTER(OracleScene), C.c_int,
                                       C.c_int, C.c_void_p, C.c_int]
@@ -138,8 +141,11 @@ def flip_pixels(u, scene: Scene, rows=None, threads: int = 0):
     return t32 != t64, c64, c32
 
 
-def backward(u, scene: Scene, dl_dcolor: np.ndarray, rows=None, grad: np.ndarray | None = None) -> np.ndarray:
-    """dL/d(texel) in float64, shape (slots, 1000, 4), of the binary32 ray cast."""
+def backward(u, scene: Scene, dl_dcolor: np.ndarray, rows=None, grad: np.ndarray | None = None,
+             grad_abs: np.ndarray | None = None) -> np.ndarray:
+    """dL/d(texel) in float64, shape (slots, 1000, 4), of the binary32 ray
+    cast; with grad_abs (same shape) also the per-texel magnitude of the
+    summed terms (see oracle_backward_bound)."""
     lib = load()
     r0, r1 = (0, u.height) if rows is None else rows
     g = np.ascontiguousarray(dl_dcolor, dtype=np.float32)
@@ -147,7 +153,8 @@ def backward(u, scene: Scene, dl_dcolor: np.ndarray, rows=None, grad: np.ndarray
     n = int(np.prod(list(scene.s.slots)))
     if grad is None:
         grad = np.zeros((n, 1000, 4), dtype=np.float64)
-    rc = lib.oracle_backward(C.byref(u), C.byref(scene.s), _p(g), _p(grad), r0, r1)
+    rc = lib.oracle_backward_bound(C.byref(u), C.byref(scene.s), _p(g), _p(grad),
+                                   _p(grad_abs) if grad_abs is not None else None, r0, r1)
     if rc != 0:
         raise RuntimeError(f"oracle_backward failed: {rc}")
     return grad

@@ -119,8 +119,11 @@ def _backward_variants(g, u, ck, per_ray, dl_t, n_slots):
 def test_backward_binary64_and_sparse_rows(fp32_scene):
     """vv_backward_ex: binary64 accumulation and the sparse gradient (rows
     claimed by touched slots) give the dense gradient; the binary64 one
-    matches the oracle's binary64 adjoint to float rounding of the
-    per-sample contributions."""
+    matches the oracle's binary64 adjoint within 1e-3 relative on every
+    texel, apart from the binary32 rounding of its per-sample terms
+    (bounded by 1e-5 times the texel's sum of term magnitudes, which the
+    oracle returns: a texel whose terms cancel to a tiny sum keeps the
+    absolute error of its large terms)."""
     from oracle import gv_oracle as go
     sc, g = fp32_scene
     n_slots = int(np.prod(sc.slots))
@@ -132,7 +135,8 @@ def test_backward_binary64_and_sparse_rows(fp32_scene):
         dl_t = torch.from_numpy(dl).cuda()
         got, rows = _backward_variants(g, u, ck, 16, dl_t, n_slots)
         assert g.ctx.device_status() == 0
-        ref = go.backward(u, sc.oracle_scene(), dl)
+        ref_abs = np.zeros((n_slots, 1000, 4), dtype=np.float64)
+        ref = go.backward(u, sc.oracle_scene(), dl, grad_abs=ref_abs)
         scale = np.abs(ref).max()
         touched = np.abs(ref).reshape(n_slots, -1).max(axis=1) > 0
         for name, v in got.items():
@@ -140,10 +144,14 @@ def test_backward_binary64_and_sparse_rows(fp32_scene):
             assert np.abs(v - ref).max() <= 1e-5 * scale, (name, np.abs(v - ref).max() / scale)
         for name, n in rows.items():
             assert n >= int(touched.sum()) and n <= n_slots
-        # binary64 accumulation: relative error 1e-5 even on texels far below the largest
-        big = np.abs(ref) > 1e-6 * scale
-        rel = np.abs(got["dense_f64"] - ref)[big] / np.abs(ref)[big]
-        assert rel.max() <= 1e-3, rel.max()
+        # binary64 accumulation: every texel, however small its gradient
+        nz = ref != 0
+        err = np.abs(got["dense_f64"] - ref)[nz]
+        assert (err <= 1e-3 * np.abs(ref)[nz] + 1e-5 * ref_abs[nz]).all()
+        cond = ref_abs[nz] / np.abs(ref)[nz]
+        # where the terms do not cancel (magnitude within 10x of the sum) the
+        # plain relative error is far below 1e-3
+        assert (err / np.abs(ref)[nz])[cond <= 10].max() <= 1e-4
 
 
 def test_sparse_rows_report_overflow(fp32_scene):
@@ -171,7 +179,9 @@ def test_gradient_matches_central_differences_of_binary64_functional(fp32_scene)
     in binary64 along the binary32 sample sequence (the control flow the
     adjoint holds fixed), at 96 random texels with a non-zero gradient, not
     only the largest.  The GPU reduces its per-sample contributions in
-    binary64 (VV_GRAD_F64).  Every texel within 1e-3 relative."""
+    binary64 (VV_GRAD_F64).  Every texel within 1e-3 relative plus the
+    binary32 rounding of its per-sample terms (1e-5 times the magnitude of
+    the terms, from the oracle's adjoint)."""
     from oracle import gv_oracle as go
     sc, g = fp32_scene
     n_slots = int(np.prod(sc.slots))
@@ -188,6 +198,10 @@ def test_gradient_matches_central_differences_of_binary64_functional(fp32_scene)
     g.ctx.synchronize()
     assert g.ctx.device_status() == 0
     an_all = grad.cpu().numpy()
+    mag = np.zeros((n_slots, 1000, 4), dtype=np.float64)
+    ref = np.zeros((n_slots, 1000, 4), dtype=np.float64)
+    for u, dl in zip(us, dls):
+        go.backward(u, sc.oracle_scene(), dl, grad=ref, grad_abs=mag)
     nz = np.argwhere(an_all != 0)
     pick = nz[rng.choice(len(nz), size=96, replace=False)]
     traj = sc.oracle_scene()
@@ -195,7 +209,7 @@ def test_gradient_matches_central_differences_of_binary64_functional(fp32_scene)
     flat = vals_pool.view(np.float32).reshape(-1)
     vals = sc.oracle_scene(pool=vals_pool)
     h = np.float32(1e-3)
-    rel = []
+    rel, ok = [], []
     for s_, t_, ch in pick:
         i = (int(s_) * 1000 + int(t_)) * 4 + int(ch)
         old = flat[i]
@@ -208,9 +222,11 @@ def test_gradient_matches_central_differences_of_binary64_functional(fp32_scene)
         flat[i] = old
         fd = (f1 - f2) / (up - dn)
         an = float(an_all[s_, t_, ch])
-        rel.append(abs(fd - an) / abs(an))
+        rel.append(abs(fd - an) / abs(fd))
+        ok.append(abs(fd - an) <= 1e-3 * abs(fd) + 1e-5 * float(mag[s_, t_, ch]))
     rel = np.array(rel)
-    assert rel.max() <= 1e-3, (rel.max(), np.median(rel))
+    assert all(ok), (rel.max(), np.median(rel))
+    assert np.median(rel) <= 1e-5, np.median(rel)
 
 
 def test_autograd_gradient_within_fp32_forward_resolution(fp32_scene):
