@@ -596,6 +596,15 @@ int vv_renderer_create(vv_ctx* ctx, vv_octree* tree, const vv_renderer_desc* d,
 void vv_renderer_destroy(vv_renderer* r);
 /* draw(): ray cast + selection mask + histopyramid + compaction on device. */
 int vv_renderer_draw(vv_renderer* r, const vv_camera* cam);
+/* The frame protocol with postDraw kept apart, as GigaVoxelsRenderer splits
+ * it: draw with `passes` VV_PASS_RAYCAST [| VV_PASS_COMPACT] (the selection
+ * mask always runs: GigaVoxelsRenderer::draw, GigaVoxelsRenderer.cpp:
+ * 1070-1088); vv_renderer_post_draw then runs the compaction of a frame
+ * drawn without it (GigaVoxelsRenderer::postDraw -> compressNodeUsageList,
+ * :1150-1186), and vv_renderer_update runs it itself if postDraw was not
+ * called.  VV_ERR_ARG without VV_PASS_RAYCAST or with unknown bits. */
+int vv_renderer_draw_passes(vv_renderer* r, const vv_camera* cam, int32_t passes);
+int vv_renderer_post_draw(vv_renderer* r);
 /* postDraw() + update(): read back the compacted page requests, run the
  * NodeUsageListProcessor / BrickPool::update policy (deterministic LRU),
  * produce and upload bricks and patch node words. */

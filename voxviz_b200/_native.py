@@ -334,6 +334,8 @@ SIGNATURES = {
     "vv_renderer_destroy": (None, [P]),
     "vv_renderer_draw": (C.c_int, [P, C.POINTER(Camera)]),
     "vv_renderer_update": (C.c_int, [P]),
+    "vv_renderer_draw_passes": (C.c_int, [P, C.POINTER(Camera), C.c_int32]),
+    "vv_renderer_post_draw": (C.c_int, [P]),
     "vv_renderer_service": (C.c_int, [P, P, P, C.c_int32]),
     "vv_renderer_set_deferred": (C.c_int, [P, C.c_int32]),
     "vv_renderer_stage_uploads": (C.c_int, [P]),

@@ -385,6 +385,16 @@ int vv_renderer_update(vv_renderer* r) {
     return r->impl->update();
 }
 
+int vv_renderer_draw_passes(vv_renderer* r, const vv_camera* cam, int32_t passes) {
+    if (!r || !cam) return VV_ERR_ARG;
+    return r->impl->draw_passes(*cam, passes);
+}
+
+int vv_renderer_post_draw(vv_renderer* r) {
+    if (!r) return VV_ERR_ARG;
+    return r->impl->post_draw();
+}
+
 int vv_renderer_service(vv_renderer* r, const uint32_t* requests, const uint32_t* count, int32_t cap) {
     if (!r) return VV_ERR_ARG;
     return r->impl->service(requests, count, cap);

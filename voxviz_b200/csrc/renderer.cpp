@@ -281,10 +281,25 @@ int GigaVoxelsRenderer::alloc_frame(int w, int h) {
     return VV_OK;
 }
 
-int GigaVoxelsRenderer::draw(const vv_camera& cam) {
+int GigaVoxelsRenderer::draw(const vv_camera& cam) { return draw_passes(cam, VV_PASS_ALL); }
+
+int GigaVoxelsRenderer::draw_passes(const vv_camera& cam, int passes) {
+    if ((passes & VV_PASS_RAYCAST) == 0 || (passes & ~VV_PASS_ALL) != 0) return VV_ERR_ARG;
     const int rc = prepare_draw(cam);
     if (rc) return rc;
-    return finish_draw(VV_PASS_ALL);
+    // the selection mask and histopyramid belong to the draw (drawVolume,
+    // GigaVoxelsRenderer.cpp:1070-1088); the compaction to postDraw (:1150-1186)
+    compact_pending_ = false;
+    const int rc2 = finish_draw(passes | VV_PASS_SELECT);
+    if (rc2) return rc2;
+    compact_pending_ = (passes & VV_PASS_COMPACT) == 0;
+    return VV_OK;
+}
+
+int GigaVoxelsRenderer::post_draw() {
+    if (!compact_pending_) return VV_OK;
+    compact_pending_ = false;
+    return finish_draw(VV_PASS_COMPACT);
 }
 
 int GigaVoxelsRenderer::prepare_draw(const vv_camera& cam) {
@@ -801,6 +816,8 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
 
 int GigaVoxelsRenderer::update() {
     if (!d_count) return VV_ERR_STATE;
+    int prc = post_draw();  // a frame drawn without compaction is compacted first
+    if (prc) return prc;
     uploaded_ = 0;
     uint32_t count = 0;
     int rc = read_count(d_count, count);

@@ -30,6 +30,11 @@ public:
     ~GigaVoxelsRenderer();
     int init();                          // Renderer::init
     int draw(const vv_camera& cam);      // Renderer::draw
+    // Renderer::draw with the chosen passes of vv_render; a frame drawn
+    // without VV_PASS_COMPACT is compacted by post_draw (Renderer::postDraw:
+    // compressNodeUsageList) or, at the latest, by update.
+    int draw_passes(const vv_camera& cam, int passes);
+    int post_draw();
     // draw() in two halves, for a ray cast made elsewhere (a batched launch
     // over several renderers): prepare_draw sets up the frame buffers and
     // uniforms, finish_draw runs the given passes of vv_render on them.
@@ -119,6 +124,7 @@ private:
     uint32_t seen_epoch_ = 0;
     vv_uniforms last_u_{};
     int cap_ = 0;
+    bool compact_pending_ = false;       // drawn without the compaction pass
     int64_t frame_ = -1;
     int32_t frame_for_compress_ = 0;
     int64_t req_count_ = 0, active_ = 0, uploaded_ = 0, uploaded_total_ = 0, evictions_ = 0, resident_ = 0;
