@@ -350,6 +350,42 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
 
 # 1,040,502 FP16 slots (8000 B each, 102x101x101): near the 102^3 slots 10-bit
 # brick pointers address, enough for the 16 views' bricks to converge
+def raycast_mode_ab(ctx, us, reps=2):
+    """The ray cast of the given frames (on the current pools) launched both
+    ways - one thread per pixel in 16x8 tiles, and persistent warps that
+    refill finished lanes with new pixels - each launch timed with CUDA
+    events (vv_render's profiling events on the context stream); both must
+    give the same colour and usage lists."""
+    import torch
+
+    import voxviz_b200 as vv
+
+    W, H = us[0].width, us[0].height
+    dev = torch.device("cuda", torch.cuda.current_device())
+    col = [torch.empty((H, W, 4), dtype=torch.float32, device=dev) for _ in range(2)]
+    use = [torch.empty((H, W, 12), dtype=torch.int32, device=dev) for _ in range(2)]
+    ctx.set_profiling(True)
+    ms = {}
+    same = True
+    for mode, name in ((False, "tiles"), (True, "refill")):
+        ctx.set_raycast_mode(mode)
+        t = []
+        for rep in range(reps + 1):
+            for u in us:
+                ctx.render(u, color=col[int(mode)].data_ptr(), usage=use[int(mode)].data_ptr(),
+                           passes=vv.VV_PASS_RAYCAST)
+                a, _ = ctx.last_times()
+                if rep:
+                    t.append(a)
+        ms[name] = float(np.mean(t))
+    ctx.set_raycast_mode(False)
+    same = bool(torch.equal(col[0], col[1]) and torch.equal(use[0], use[1]))
+    ctx.set_profiling(False)
+    return {"raycast_ms_tiles": round(ms["tiles"], 4), "raycast_ms_refill": round(ms["refill"], 4),
+            "refill_speedup": round(ms["tiles"] / ms["refill"], 3), "frames": len(us), "reps": reps,
+            "last_frame_bitexact": same}
+
+
 BATCH16_VIEWS, BATCH16_POOL_BYTES = 16, 8_324_000_000
 
 
@@ -528,6 +564,7 @@ def run_ours(args):
             roofline["issue"]["frac"] = round(roofline["issue"]["achieved_ginst_s"] /
                                               roofline["issue"]["peak_ginst_s"], 4)
     fb = fwd_bwd_leg(ctx, timed_u[-16:], min(16, args.steps), peak)
+    ab = raycast_mode_ab(ctx, timed_u)
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
@@ -552,6 +589,7 @@ def run_ours(args):
                    "host_ms_per_frame": {k[3:]: round(v / args.steps, 3) for k, v in host_ms.items()},
                    "resident": r.stats()["resident_bricks"], "pool_slots": r.stats()["pool_slots"]},
         "fwd_bwd": fb,
+        "raycast_launch_ab": ab,
         "clocks": clk, "gpu_launches": None, "setup_s": round(setup_s, 1),
     }
     # our kernels per step. draw: raycast + select + (levels-1) pyramid up +

@@ -253,6 +253,16 @@ int vv_render(vv_ctx* ctx, int32_t tree, const vv_uniforms* u,
  * (the reference kept QElapsedTimer pass timers, GigaVoxelsRenderer.cpp:858-903).
  * vv_ctx_last_times waits for the last draw and returns its two durations. */
 int vv_ctx_set_profiling(vv_ctx* ctx, int32_t on);
+/* How vv_render's ray cast (unlit, colour and usage lists) is launched; the
+ * results are the same.  VV_RAYCAST_TILES (default): one thread per pixel,
+ * 16x8-pixel CTAs.  VV_RAYCAST_REFILL: a persistent grid whose warps take
+ * 8x4-pixel tiles from a queue and run their rays one leaf segment at a
+ * time, a lane whose ray has ended taking the next pixel (ballot + popc)
+ * instead of idling until the warp's last ray ends.  No reference
+ * counterpart (one fragment per pixel in GL). */
+#define VV_RAYCAST_TILES 0
+#define VV_RAYCAST_REFILL 1
+int vv_ctx_set_raycast_mode(vv_ctx* ctx, int32_t mode);
 int vv_ctx_last_times(vv_ctx* ctx, float* raycast_ms, float* compact_ms);
 /* Footprint of one draw: the number of distinct node-pool entries and
  * brick-pool slots the ray cast of `u` reads (a counting variant of the same
@@ -418,6 +428,15 @@ typedef struct vv_octree_info {
 
 /* GigaVoxelsOctTree::build (GigaVoxelsOctTree.cpp:1656-1701) for the terrain. */
 int vv_octree_build_terrain(const vv_terrain_desc* desc, vv_octree** out);
+/* The same tree built on CUDA device `device`: the heightfield, the 2x2x2
+ * box-filter mip pyramid with round-half-up (GenerateMipMap /
+ * GetBoxFilterAverage, GigaVoxelsOctTree.cpp:809-960; the voxelizer's
+ * ComputeVoxelMipMap8, VoxelizerKernels.cu:1520) and the node
+ * classification with the border rule (Node::computeNodeType, :1490-1609;
+ * ComputeOctTreeNodeType, VoxelizerKernels.cu:2216) run as kernels; the host
+ * numbers the blocks and keeps a copy of the pyramid.  Identical to
+ * vv_octree_build_terrain.  VV_ERR_NODEV without that device. */
+int vv_octree_build_terrain_gpu(const vv_terrain_desc* desc, int32_t device, vv_octree** out);
 void vv_octree_destroy(vv_octree* tree);
 int vv_octree_get_info(const vv_octree* tree, vv_octree_info* info);
 /* Host mirror of the node pool in reference texture order, no brick resident

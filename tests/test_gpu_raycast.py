@@ -101,3 +101,25 @@ def test_miss_only_view_is_empty(cfg1):
     got = g.render(u)
     assert not got["color"].any() and not got["usage"].any()
     assert got["count"] == 0 and got["requests"].shape[0] == 0
+
+
+@pytest.mark.parametrize("fmt,view,size", [("rgba8", 3, (512, 512)), ("fp16", 5, (333, 177)),
+                                           ("rgba8", 8, (1920, 1080)), ("fp32", 9, (61, 37))])
+def test_lane_refill_ray_cast_equals_tiles(fmt, view, size):
+    """VV_RAYCAST_REFILL (persistent warps, finished lanes take new pixels)
+    gives the same colour, usage lists, mask and requests as the tiled
+    launch."""
+    sc = helpers.Scene(seed=1, depth=5, fmt=fmt)
+    g = helpers.GpuScene(sc)
+    u = sc.uniforms(sc.view(view, *size))
+    a = g.render(u)
+    g.ctx.set_raycast_mode(True)
+    try:
+        b = g.render(u)
+        b2 = g.render(u)  # the queue counter is reset per launch
+    finally:
+        g.ctx.set_raycast_mode(False)
+    for k in ("color", "usage", "mask", "requests"):
+        assert np.array_equal(a[k], b[k]), k
+        assert np.array_equal(a[k], b2[k]), k
+    assert a["status"] == b["status"] == 0

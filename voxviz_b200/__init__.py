@@ -117,11 +117,17 @@ class Octree:
 
     @classmethod
     def terrain(cls, seed: int = 1, depth: int = 5, collapse: bool = True, octaves: int = 4,
-                lacunarity: float = 2.0, gain: float = 0.5, base_cells: int = 4, threads: int = 0) -> "Octree":
+                lacunarity: float = 2.0, gain: float = 0.5, base_cells: int = 4, threads: int = 0,
+                device: int | None = None) -> "Octree":
+        """The seeded fBm terrain octree, built on the host cores or, with
+        ``device``, on that CUDA device (the same tree)."""
         d = N.TerrainDesc(seed=seed, depth=depth, octaves=octaves, lacunarity=lacunarity, gain=gain,
                           base_cells=base_cells, collapse_constant=1 if collapse else 0, threads=threads)
         h = C.c_void_p()
-        _check(lib().vv_octree_build_terrain(C.byref(d), C.byref(h)), what="octree build")
+        if device is None:
+            _check(lib().vv_octree_build_terrain(C.byref(d), C.byref(h)), what="octree build")
+        else:
+            _check(lib().vv_octree_build_terrain_gpu(C.byref(d), int(device), C.byref(h)), what="octree build (GPU)")
         return cls(h.value)
 
     @classmethod
@@ -364,6 +370,12 @@ class Context:
         t = np.ascontiguousarray(table, dtype=np.uint8)
         size = int(round(np.sqrt(t.size)))
         self._ck(lib().vv_set_jitter(self._h, _ptr(t), size), "jitter")
+
+    def set_raycast_mode(self, refill: bool) -> None:
+        """vv_ctx_set_raycast_mode: the lane-refill persistent ray cast or the
+        one-thread-per-pixel tiles (same results)."""
+        self._ck(lib().vv_ctx_set_raycast_mode(self._h, N.VV_RAYCAST_REFILL if refill else N.VV_RAYCAST_TILES),
+                 "raycast mode")
 
     def set_profiling(self, on: bool = True) -> None:
         self._ck(lib().vv_ctx_set_profiling(self._h, 1 if on else 0), "profiling")

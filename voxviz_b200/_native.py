@@ -239,6 +239,7 @@ class GradDesc(C.Structure):
 
 
 VV_GRAD_F64 = 1
+VV_RAYCAST_TILES, VV_RAYCAST_REFILL = 0, 1
 
 
 class BatchView(C.Structure):
@@ -290,6 +291,7 @@ SIGNATURES = {
     "vv_render": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.POINTER(FrameOut)]),
     "vv_compact_requests_noalloc": (C.c_int, [P, P, C.c_int32, C.c_int32, P, P, C.c_int32, C.c_int32, P]),
     "vv_ctx_set_profiling": (C.c_int, [P, C.c_int32]),
+    "vv_ctx_set_raycast_mode": (C.c_int, [P, C.c_int32]),
     "vv_ckpt_bytes": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "vv_render_forward_ckpt": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32]),
     "vv_backward": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32, P]),
@@ -305,6 +307,7 @@ SIGNATURES = {
     "vv_measure_footprint_views": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), C.c_int32, C.POINTER(C.c_int64),
                                              C.POINTER(C.c_int64)]),
     "vv_octree_build_terrain": (C.c_int, [C.POINTER(TerrainDesc), C.POINTER(P)]),
+    "vv_octree_build_terrain_gpu": (C.c_int, [C.POINTER(TerrainDesc), C.c_int32, C.POINTER(P)]),
     "vv_octree_destroy": (None, [P]),
     "vv_octree_get_info": (C.c_int, [P, C.POINTER(OctreeInfo)]),
     "vv_octree_node_words": (C.c_int, [P, P]),

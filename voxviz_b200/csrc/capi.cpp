@@ -46,6 +46,45 @@ int vv_octree_build_terrain(const vv_terrain_desc* d, vv_octree** out) {
     }
 }
 
+int vv_octree_build_terrain_gpu(const vv_terrain_desc* d, int32_t device, vv_octree** out) {
+    if (!d || !out) return VV_ERR_ARG;
+    *out = nullptr;
+    if (d->depth < 0 || d->depth > 10 || d->octaves < 1 || d->base_cells < 1) return VV_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        vv::set_thread_error("vv_octree_build_terrain_gpu: no such CUDA device");
+        return VV_ERR_NODEV;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return VV_ERR_CUDA;
+    try {
+        vv::TerrainParams p;
+        p.seed = d->seed;
+        p.depth = d->depth;
+        p.octaves = d->octaves;
+        p.lacunarity = d->lacunarity;
+        p.gain = d->gain;
+        p.base_cells = d->base_cells;
+        p.threads = d->threads;
+        std::shared_ptr<vv::TerrainVolume> vol;
+        std::vector<vv::TreeLevel> levels;
+        const std::string err = vv::gpu_build_terrain(p, d->collapse_constant != 0, vol, levels);
+        if (!err.empty()) {
+            vv::set_thread_error("vv_octree_build_terrain_gpu: " + err);
+            return VV_ERR_CUDA;
+        }
+        auto o = std::make_unique<vv_octree>();
+        o->volume = vol;
+        o->tree = vv::GigaVoxelsOctTree::from_levels(o->volume, std::move(levels), d->collapse_constant != 0);
+        *out = o.release();
+        return VV_OK;
+    } catch (const std::bad_alloc&) {
+        return VV_ERR_OOM;
+    } catch (const std::exception& e) {
+        vv::set_thread_error(std::string("vv_octree_build_terrain_gpu: ") + e.what());
+        return VV_ERR_ARG;
+    }
+}
+
 void vv_octree_destroy(vv_octree* t) { delete t; }
 
 int vv_octree_get_info(const vv_octree* t, vv_octree_info* info) {

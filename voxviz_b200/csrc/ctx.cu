@@ -183,7 +183,7 @@ int vv_ctx_destroy(vv_ctx* c) {
     if (c->bricks && !c->bricks_external) cudaFree(c->bricks);
     void* bufs[] = {c->d_status, c->d_jitter, c->d_usage, c->d_mask, c->d_counts, c->d_offsets,
                     c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words, c->d_batch, c->grads,
-                    c->cell_mask};
+                    c->cell_mask, c->d_refill_counter};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -610,7 +610,12 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
             p.grads = c->grads;
             p.grad_fmt = c->grad_fmt;
         }
-        VV_CUDA(c, launch_raycast_any(c, p));
+        if (c->raycast_mode == VV_RAYCAST_REFILL && !u->compute_lighting) {
+            if (!c->d_refill_counter) VV_CUDA(c, cudaMalloc(&c->d_refill_counter, sizeof(unsigned int)));
+            VV_CUDA(c, launch_raycast_refill(c->fmt, p, c->d_refill_counter, c->stream));
+        } else {
+            VV_CUDA(c, launch_raycast_any(c, p));
+        }
     }
     if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
     if (!(passes & (VV_PASS_SELECT | VV_PASS_COMPACT))) {
@@ -664,6 +669,13 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
     cp.max_push = out->compress_max_push > 0 ? out->compress_max_push : 4;
     VV_CUDA(c, launch_compact(cp, c->stream));
     if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
+    return VV_OK;
+}
+
+int vv_ctx_set_raycast_mode(vv_ctx* c, int32_t mode) {
+    if (!c || (mode != VV_RAYCAST_TILES && mode != VV_RAYCAST_REFILL))
+        return fail(c, VV_ERR_ARG, "unknown ray-cast mode");
+    c->raycast_mode = mode;
     return VV_OK;
 }
 

@@ -82,6 +82,10 @@ struct vv_ctx {
     size_t h_batch_cap = 0;
     void* d_batch = nullptr;
     size_t d_batch_cap = 0;
+    // ray-cast form (VV_RAYCAST_TILES / VV_RAYCAST_REFILL) and the refill
+    // form's tile counter
+    int raycast_mode = 0;
+    unsigned int* d_refill_counter = nullptr;
     // profiling
     bool profiling = false;
     bool timed = false;

@@ -41,6 +41,56 @@ __global__ void __launch_bounds__(128, 7) raycast_kernel(const __grid_constant__
                                              PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
 }
 
+// The lane-refill form (render_refill): a persistent grid of as many CTAs
+// as are resident at once, pixels handed out in 8x4 tiles from `counter`
+// (zeroed before the launch).
+template <int FMT>
+__global__ void __launch_bounds__(128, 7) raycast_refill_kernel(const __grid_constant__ RaycastParams p,
+                                                                unsigned int* counter) {
+    __shared__ uint2 path_w[kPathLevels][128];
+    __shared__ uint32_t path_p[kPathLevels][128];
+    render_refill<FMT>(p, counter, PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
+}
+
+cudaError_t launch_raycast_refill(int fmt, const RaycastParams& p, unsigned int* counter, cudaStream_t s) {
+    static int ctas[4] = {0, 0, 0, 0};  // resident CTAs on the device (per format)
+    if (fmt < 0 || fmt > 3) return cudaErrorInvalidValue;
+    cudaError_t e = cudaSuccess;
+    if (!ctas[fmt]) {
+        int dev = 0, sms = 0, per_sm = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) {
+            switch (fmt) {
+                case VV_FMT_RGBA8:
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raycast_refill_kernel<VV_FMT_RGBA8>, 128, 0);
+                    break;
+                case VV_FMT_FP16:
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raycast_refill_kernel<VV_FMT_FP16>, 128, 0);
+                    break;
+                case VV_FMT_BF16:
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raycast_refill_kernel<VV_FMT_BF16>, 128, 0);
+                    break;
+                default:
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raycast_refill_kernel<VV_FMT_FP32>, 128, 0);
+                    break;
+            }
+        }
+        if (e != cudaSuccess) return e;
+        ctas[fmt] = std::max(1, sms * per_sm);
+    }
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    dim3 block(128), grid((unsigned)ctas[fmt]);
+    switch (fmt) {
+        case VV_FMT_RGBA8: raycast_refill_kernel<VV_FMT_RGBA8><<<grid, block, 0, s>>>(p, counter); break;
+        case VV_FMT_FP16: raycast_refill_kernel<VV_FMT_FP16><<<grid, block, 0, s>>>(p, counter); break;
+        case VV_FMT_BF16: raycast_refill_kernel<VV_FMT_BF16><<<grid, block, 0, s>>>(p, counter); break;
+        default: raycast_refill_kernel<VV_FMT_FP32><<<grid, block, 0, s>>>(p, counter); break;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s) {
     dim3 block(128);
     dim3 grid((unsigned)((p.u.width + 15) / 16), (unsigned)((p.u.height + 7) / 8));

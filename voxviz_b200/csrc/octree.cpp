@@ -63,39 +63,19 @@ bool classify_node(const TerrainVolume& vol, int d, int i, int j, int k, uint32_
     return true;
 }
 
-namespace {
-struct LevelNodes {
-    std::vector<uint16_t> i, j, k;
-    std::vector<uint32_t> parent;       // local index in the previous level
-    std::vector<uint32_t> first_child;  // local index in the next level or UINT32_MAX
-    std::vector<uint32_t> cval;
-    std::vector<uint8_t> isc;
-    std::vector<uint32_t> nidx;         // global node index
-    size_t size() const { return i.size(); }
-    void push(int a, int b, int c, uint32_t p) {
-        i.push_back((uint16_t)a);
-        j.push_back((uint16_t)b);
-        k.push_back((uint16_t)c);
-        parent.push_back(p);
-    }
-};
-}  // namespace
-
 std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<const TerrainVolume> vol,
                                                             bool collapse) {
-    std::unique_ptr<GigaVoxelsOctTree> t(new GigaVoxelsOctTree());
-    t->vol_ = vol;
     const int L = vol->depth();
-    t->depth_ = L;
-    std::vector<LevelNodes> lv((size_t)L + 1);
-    lv[0].push(0, 0, 0, kNoParent);
+    std::vector<TreeLevel> lv((size_t)L + 1);
+    lv[0].i.push_back(0);
+    lv[0].j.push_back(0);
+    lv[0].k.push_back(0);
+    lv[0].parent.push_back(kNoParent);
     for (int d = 0; d <= L; ++d) {
-        LevelNodes& cur = lv[(size_t)d];
+        TreeLevel& cur = lv[(size_t)d];
         const size_t n = cur.size();
         cur.cval.assign(n, 0);
         cur.isc.assign(n, 0);
-        cur.first_child.assign(n, UINT32_MAX);
-        cur.nidx.assign(n, 0);
 #pragma omp parallel for schedule(dynamic, 256)
         for (long q = 0; q < (long)n; ++q) {
             uint32_t cv = 0;
@@ -104,30 +84,59 @@ std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<cons
             cur.cval[(size_t)q] = cv;
         }
         if (d == L) break;
-        LevelNodes& nxt = lv[(size_t)d + 1];
+        TreeLevel& nxt = lv[(size_t)d + 1];
         for (size_t q = 0; q < n; ++q) {
             if (collapse && cur.isc[q]) continue;
-            cur.first_child[q] = (uint32_t)nxt.size();
-            for (int c = 0; c < 8; ++c)
-                nxt.push(2 * cur.i[q] + (c & 1), 2 * cur.j[q] + ((c >> 1) & 1), 2 * cur.k[q] + (c >> 2),
-                         (uint32_t)q);
+            for (int c = 0; c < 8; ++c) {
+                nxt.i.push_back((uint16_t)(2 * cur.i[q] + (c & 1)));
+                nxt.j.push_back((uint16_t)(2 * cur.j[q] + ((c >> 1) & 1)));
+                nxt.k.push_back((uint16_t)(2 * cur.k[q] + (c >> 2)));
+                nxt.parent.push_back((uint32_t)q);
+            }
         }
+    }
+    return from_levels(std::move(vol), std::move(lv), collapse);
+}
+
+std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::from_levels(std::shared_ptr<const TerrainVolume> vol,
+                                                                  std::vector<TreeLevel>&& lv, bool collapse) {
+    std::unique_ptr<GigaVoxelsOctTree> t(new GigaVoxelsOctTree());
+    t->vol_ = vol;
+    const int L = vol->depth();
+    t->depth_ = L;
+    if (lv.size() != (size_t)L + 1 || lv[0].size() != 1) throw std::invalid_argument("bad tree levels");
+    // each node's first child in the next level (children come 8 per parent,
+    // in parent order)
+    std::vector<std::vector<uint32_t>> first_child(lv.size()), nidx(lv.size());
+    for (int d = 0; d <= L; ++d) {
+        const TreeLevel& cur = lv[(size_t)d];
+        if (cur.isc.size() != cur.size() || cur.cval.size() != cur.size() || cur.parent.size() != cur.size())
+            throw std::invalid_argument("bad tree level arrays");
+        first_child[(size_t)d].assign(cur.size(), UINT32_MAX);
+        nidx[(size_t)d].assign(cur.size(), 0);
+        if (d == L) break;
+        uint32_t next = 0;
+        for (size_t q = 0; q < cur.size(); ++q) {
+            if (collapse && cur.isc[q]) continue;
+            first_child[(size_t)d][q] = next;
+            next += 8;
+        }
+        if ((size_t)next != lv[(size_t)d + 1].size()) throw std::invalid_argument("tree level sizes disagree");
     }
     // Depth-first pre-order block numbering (BuildOctTreeChildren allocates a
     // child's block right before recursing into it).
     size_t blocks = 1;
     {
         std::vector<std::pair<int, uint32_t>> stack;
-        lv[0].nidx[0] = 0;
+        nidx[0][0] = 0;
         stack.push_back({0, 0u});
         while (!stack.empty()) {
             auto [d, q] = stack.back();
             stack.pop_back();
-            uint32_t fc = lv[(size_t)d].first_child[q];
+            uint32_t fc = first_child[(size_t)d][q];
             if (fc == UINT32_MAX) continue;
             size_t B = blocks++;
-            LevelNodes& nxt = lv[(size_t)d + 1];
-            for (int c = 0; c < 8; ++c) nxt.nidx[fc + (uint32_t)c] = (uint32_t)(8 * B + (size_t)c);
+            for (int c = 0; c < 8; ++c) nidx[(size_t)d + 1][fc + (uint32_t)c] = (uint32_t)(8 * B + (size_t)c);
             for (int c = 7; c >= 0; --c) stack.push_back({d + 1, fc + (uint32_t)c});
         }
     }
@@ -144,14 +153,14 @@ std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<cons
     t->word1_.assign(num_nodes, 0);
     size_t nonconst = 0;
     for (int d = 0; d <= L; ++d) {
-        const LevelNodes& cur = lv[(size_t)d];
+        const TreeLevel& cur = lv[(size_t)d];
         for (size_t q = 0; q < cur.size(); ++q) {
-            uint32_t n = cur.nidx[q];
+            uint32_t n = nidx[(size_t)d][q];
             t->level_[n] = (int8_t)d;
             t->ci_[n] = cur.i[q];
             t->cj_[n] = cur.j[q];
             t->ck_[n] = cur.k[q];
-            t->parent_[n] = d == 0 ? kNoParent : lv[(size_t)d - 1].nidx[cur.parent[q]];
+            t->parent_[n] = d == 0 ? kNoParent : nidx[(size_t)d - 1][cur.parent[q]];
             uint32_t w0 = 0, w1 = 0;
             if (cur.isc[q]) {
                 w0 |= kConstantBit;
@@ -159,7 +168,8 @@ std::unique_ptr<GigaVoxelsOctTree> GigaVoxelsOctTree::build(std::shared_ptr<cons
             } else {
                 ++nonconst;
             }
-            if (cur.first_child[q] != UINT32_MAX) w0 |= t->child_pointer(lv[(size_t)d + 1].nidx[cur.first_child[q]] / 8);
+            const uint32_t fc = first_child[(size_t)d][q];
+            if (fc != UINT32_MAX) w0 |= t->child_pointer(nidx[(size_t)d + 1][fc] / 8);
             t->word0_[n] = w0;
             t->word1_[n] = w1;
         }

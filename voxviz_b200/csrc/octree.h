@@ -27,6 +27,16 @@ constexpr uint32_t kNoParent = 0xFFFFFFFFu;
 
 inline uint32_t pack10(uint32_t x, uint32_t y, uint32_t z) { return (x << 20) | (y << 10) | z; }
 
+// The nodes of one tree level in build order: cell (i,j,k), parent (index
+// in the previous level), and the classification (constant flag and value).
+struct TreeLevel {
+    std::vector<uint16_t> i, j, k;
+    std::vector<uint32_t> parent;  // kNoParent at the root level
+    std::vector<uint8_t> isc;
+    std::vector<uint32_t> cval;
+    size_t size() const { return i.size(); }
+};
+
 class GigaVoxelsOctTree {
 public:
     // GigaVoxelsOctTree::build for a terrain volume.  collapse = true makes
@@ -35,6 +45,12 @@ public:
     // build does.
     static std::unique_ptr<GigaVoxelsOctTree> build(std::shared_ptr<const TerrainVolume> vol,
                                                     bool collapse);
+    // The same from classified levels computed elsewhere (the GPU builder):
+    // level d+1 holds the 8 children of every node of level d that has
+    // children (every node, or the non-constant ones with collapse), in the
+    // order of their parents.
+    static std::unique_ptr<GigaVoxelsOctTree> from_levels(std::shared_ptr<const TerrainVolume> vol,
+                                                          std::vector<TreeLevel>&& levels, bool collapse);
     // GigaVoxelsReader::LoadOctTreeFile (GigaVoxelsReader.cpp:541-563) from
     // the records read_gvx produced.  Node::setConstantValue
     // (GigaVoxelsOctTree.cpp:1611-1621) computes a constant node's colour
@@ -133,6 +149,12 @@ private:
     std::vector<uint32_t> word0_, word1_;
     size_t nonconst_ = 0;
 };
+
+// The terrain volume and classified tree levels of GigaVoxelsOctTree::build
+// computed on the current CUDA device (builder.cu); returns an error message,
+// empty on success.
+std::string gpu_build_terrain(const TerrainParams& p, bool collapse, std::shared_ptr<TerrainVolume>& vol_out,
+                              std::vector<TreeLevel>& levels);
 
 // Node::computeNodeType (GigaVoxelsOctTree.cpp:1490-1609) for the node at
 // level d with index (i,j,k): returns true if constant and its RGBA8 value.

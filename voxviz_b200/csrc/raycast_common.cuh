@@ -475,14 +475,23 @@ __device__ __forceinline__ void light_sample(const RaycastParams& p, F3 bpos, F3
     src.z = src.z + sh.z;
 }
 
+// Where a ray's last descent stopped (RESUME): its depth and its node's
+// cell there, packed 10:10:10.
+struct WalkResume {
+    int prev_depth = -1;
+    uint32_t prev_cell = 0u;
+};
+
+// One leaf segment of the walk (a descent and its march); false when the
+// walk has ended.  walk() runs it until then.
 template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false, bool LIT = false>
-__device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis,
-                                     PathSlots path = PathSlots{nullptr, nullptr, 0}) {
+__device__ __forceinline__ bool walk_segment(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis,
+                                             PathSlots path, WalkResume& wr) {
     bool ok = true;
-    int prev_depth = -1;       // where the last descent stopped (RESUME)
-    uint32_t prev_cell = 0u;   // its node's cell there, packed 10:10:10
-    for (;;) {
-        if (!vis.segment_begin(s)) return;
+    int& prev_depth = wr.prev_depth;
+    uint32_t& prev_cell = wr.prev_cell;
+    {
+        if (!vis.segment_begin(s)) return false;
         int skip_lo, skip_hi;
         lodb::clear_range(k.lodk, lodb::V3{s.pos.x, s.pos.y, s.pos.z}, skip_lo, skip_hi);
         uint2 node = k.root;
@@ -540,7 +549,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
         for (;;) {
             if (++s.iter > k.max_iter) {
                 vis.fail(VV_ERR_TIMEOUT);
-                return;
+                return false;
             }
             if (RESUME && depth < kPathLevels) {
                 path.w[depth * path.stride] = node;
@@ -587,7 +596,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
             node = fetch_node<COUNT>(p, s.nptr_x, s.nptr_y, s.nptr_z, ok);
             if (!ok) {
                 vis.fail(VV_ERR_BOUNDS);
-                return;
+                return false;
             }
         }
         if (k.unit_box) {
@@ -627,7 +636,7 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                     s.dst = make_float4(T * src.x + s.dst.x, T * src.y + s.dst.y, T * src.z + s.dst.z,
                                         T * src.w + s.dst.w);
                     ++s.nsamples;
-                    if (!go) return;
+                    if (!go) return false;
                 }
             }
         } else {
@@ -681,14 +690,22 @@ __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k
                     s.dst = make_float4(T * src.x + s.dst.x, T * src.y + s.dst.y, T * src.z + s.dst.z,
                                         T * src.w + s.dst.w);
                 ++s.nsamples;
-                if (!go) return;
+                if (!go) return false;
                 bpos = add(bpos, s.brick_step);
             }
         }
         vis.segment_end(s, is_const, loaded);
-        if (s.dst.w > k.astop && (is_const || loaded)) return;
+        if (s.dst.w > k.astop && (is_const || loaded)) return false;
         // restart from the root (:688-720); the node pointer keeps its value
-        if (!inside_box(s.pos, k.vmin, k.vmax)) return;
+        return inside_box(s.pos, k.vmin, k.vmax);
+    }
+}
+
+template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false, bool LIT = false>
+__device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis,
+                                     PathSlots path = PathSlots{nullptr, nullptr, 0}) {
+    WalkResume wr;
+    while (walk_segment<FMT, COUNT, V, STEPS, RESUME, LIT>(p, k, s, vis, path, wr)) {
     }
 }
 
@@ -714,16 +731,14 @@ struct UsageVisitor {
     __device__ __forceinline__ void fail(int code) { set_status(status, code); }
 };
 
-// One pixel of the forward draw: the fragment's ray walk, FragColor and the
-// three RGBA32UI usage-list layers (:490-751).
-template <int FMT, bool COUNT, int STEPS, bool RESUME = false, bool LIT = false>
-__device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int py,
-                                             PathSlots path = PathSlots{nullptr, nullptr, 0}) {
+// The set-up of pixel (px,py)'s draw: its usage-list record zeroed and the
+// visitor pointed at it, dst cleared, and the fragment's ray started; false
+// when the pixel has no fragment or its ray starts outside the volume (its
+// walk is then empty).
+__device__ __forceinline__ bool start_pixel(const RaycastParams& p, const WalkConsts& k, int px, int py,
+                                            RayState& s, UsageVisitor& vis) {
     const vv_uniforms& u = p.u;
     const size_t pix = (size_t)py * u.width + px;
-    bool ok = true;
-    const WalkConsts k = walk_consts(p, fetch_node<COUNT>(p, 0, 0, 0, ok));
-    UsageVisitor vis;
     vis.out = nullptr;
     if (p.usage) {
         uint4* o = p.usage + pix * 3;
@@ -736,14 +751,88 @@ __device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int
     vis.start_push = (px % 2) * 12 + (py % 2) * 24;
     vis.max_push = u.max_nodes_to_push;
     vis.status = p.status;
-    RayState s;
     s.dst = make_float4(0.f, 0.f, 0.f, 0.f);
     F3 pos;
-    if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s))
-        walk<FMT, COUNT, UsageVisitor, STEPS, RESUME, LIT>(p, k, s, vis, path);
+    return ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s);
+}
+
+// FragColor of pixel `pix` (:751): float4, or RGBA8 unorm.
+__device__ __forceinline__ void finish_pixel(const RaycastParams& p, size_t pix, const RayState& s) {
     if (p.color) {
         if (p.color8) ((uint32_t*)p.color)[pix] = pack_unorm8(s.dst);
         else p.color[pix] = s.dst;
+    }
+}
+
+// One pixel of the forward draw: the fragment's ray walk, FragColor and the
+// three RGBA32UI usage-list layers (:490-751).
+template <int FMT, bool COUNT, int STEPS, bool RESUME = false, bool LIT = false>
+__device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int py,
+                                             PathSlots path = PathSlots{nullptr, nullptr, 0}) {
+    bool ok = true;
+    const WalkConsts k = walk_consts(p, fetch_node<COUNT>(p, 0, 0, 0, ok));
+    UsageVisitor vis;
+    RayState s;
+    if (start_pixel(p, k, px, py, s, vis)) walk<FMT, COUNT, UsageVisitor, STEPS, RESUME, LIT>(p, k, s, vis, path);
+    finish_pixel(p, (size_t)py * p.u.width + px, s);
+}
+
+// Persistent ray cast that keeps the lanes of a warp busy: each warp takes
+// 8x4 pixel tiles from a device counter and runs its rays one leaf segment
+// at a time (walk_segment); a lane whose ray has ended takes the next pixel
+// of the warp's tile (ballot + popc rank) before the next segment, instead
+// of idling until the warp's slowest ray ends.  Same pixels, same walk, same
+// results as render_pixel.
+template <int FMT>
+__device__ __forceinline__ void render_refill(const RaycastParams& p, unsigned int* counter, PathSlots path) {
+    const vv_uniforms& u = p.u;
+    const int W = u.width, H = u.height;
+    const int tiles_x = (W + 7) >> 3;
+    const int tiles = tiles_x * ((H + 3) >> 2);
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    bool ok = true;
+    const WalkConsts k = walk_consts(p, fetch_node<false>(p, 0, 0, 0, ok));
+    int tile = 0, taken = 32;  // the warp's tile and how many of its pixels are handed out
+    bool more = true;          // tiles left
+    bool active = false;
+    size_t pix = 0;
+    RayState s;
+    UsageVisitor vis;
+    WalkResume wr;
+    for (;;) {
+        unsigned idle = __ballot_sync(0xFFFFFFFFu, !active);
+        while (idle && more) {
+            if (taken == 32) {
+                unsigned t = 0u;
+                if (lane == 0u) t = atomicAdd(counter, 1u);
+                tile = (int)__shfl_sync(0xFFFFFFFFu, t, 0);
+                taken = 0;
+                if (tile >= tiles) {
+                    more = false;
+                    break;
+                }
+            }
+            const int n = min(__popc(idle), 32 - taken);
+            const int rank = __popc(idle & below);
+            if (!active && rank < n) {
+                const int q = taken + rank;
+                const int px = (tile % tiles_x) * 8 + (q & 7), py = (tile / tiles_x) * 4 + (q >> 3);
+                if (px < W && py < H) {
+                    pix = (size_t)py * W + px;
+                    wr = WalkResume{};
+                    active = start_pixel(p, k, px, py, s, vis);
+                    if (!active) finish_pixel(p, pix, s);
+                }
+            }
+            taken += n;
+            idle = __ballot_sync(0xFFFFFFFFu, !active);
+        }
+        if (__ballot_sync(0xFFFFFFFFu, active) == 0u) return;
+        if (active && !walk_segment<FMT, false, UsageVisitor, 1, true, false>(p, k, s, vis, path, wr)) {
+            finish_pixel(p, pix, s);
+            active = false;
+        }
     }
 }
 

@@ -83,6 +83,14 @@ TerrainVolume::TerrainVolume(const TerrainParams& p) : p_(p) {
     for (int m = 1; m <= p.depth; ++m) build_level(m);
 }
 
+TerrainVolume::TerrainVolume(const TerrainParams& p, std::vector<int32_t>&& heights, std::vector<MipLevel>&& mips)
+    : p_(p), heights_(std::move(heights)), mips_(std::move(mips)) {
+    if (p.depth < 0 || p.depth > 10) throw std::invalid_argument("terrain depth must be in [0,10]");
+    dim_ = 8 << p.depth;
+    if (heights_.size() != (size_t)dim_ * dim_ || mips_.size() != (size_t)p.depth + 1)
+        throw std::invalid_argument("prebuilt terrain of the wrong size");
+}
+
 void TerrainVolume::build_heights() {
     const int n = dim_;
     heights_.resize((size_t)n * n);

@@ -46,6 +46,9 @@ struct MipLevel {
 class TerrainVolume {
 public:
     explicit TerrainVolume(const TerrainParams& p);
+    // A volume whose heights and mip pyramid were built elsewhere (the GPU
+    // builder): the same values the constructor above computes.
+    TerrainVolume(const TerrainParams& p, std::vector<int32_t>&& heights, std::vector<MipLevel>&& mips);
 
     const TerrainParams& params() const { return p_; }
     int depth() const { return p_.depth; }
