@@ -60,7 +60,18 @@ typedef enum vv_fmt {
     VV_FMT_RGBA8 = 0,   /* 4 x uint8, unorm                              */
     VV_FMT_FP16 = 1,    /* 4 x IEEE binary16                             */
     VV_FMT_BF16 = 2,    /* 4 x bfloat16                                  */
-    VV_FMT_FP32 = 3     /* 4 x float                                     */
+    VV_FMT_FP32 = 3,    /* 4 x float                                     */
+    /* S3TC block-compressed pools (GL_COMPRESSED_RGBA_S3TC_DXT5 colour and
+     * GL_COMPRESSED_RGB_S3TC_DXT1 gradient textures of the reference,
+     * GigaVoxelsRenderer.cpp:235-258): each brick's 10 z slices of 10x10
+     * texels padded to 12x12 as 4x4 blocks, 90 blocks per slot, block
+     * (z*9 + (y/4)*3 + x/4) of the slot, texel (y%4)*4 + x%4 of the block.
+     * Decoded to RGBA8 values, then filtered like RGBA8.  The expansion and
+     * interpolation rounding S3TC leaves open are fixed (voxviz_b200/csrc/
+     * dxt.h).  DXT5 for brick pools (1440 bytes per slot), DXT1 for
+     * gradient pools (720 bytes per slot, unsigned gradients). */
+    VV_FMT_DXT5 = 4,
+    VV_FMT_DXT1 = 5
 } vv_fmt;
 
 #define VV_BRICK_DIM 8          /* interior voxels per axis               */

@@ -126,6 +126,41 @@ float bf16_to_float(uint16_t h) {
     return f;
 }
 
+// S3TC decode (EXT_texture_compression_s3tc) of one texel, with the
+// expansion and rounding the library fixes: 5/6-bit channels widened by bit
+// replication, interpolated colours (2a+b+1)/3 and (a+2b+1)/3 (or (a+b+1)/2
+// and black in DXT1's three-colour mode), interpolated alphas
+// ((8-k)a0+(k-1)a1+3)/7, or ((6-k)a0+(k-1)a1+2)/5 with codes 6, 7 = 0, 255.
+// The block's bytes are read one by one (little endian).
+void s3tc_colour(const unsigned char* blk, int texel, bool force_four, int rgb[3]) {
+    const unsigned c0 = (unsigned)blk[0] | ((unsigned)blk[1] << 8), c1 = (unsigned)blk[2] | ((unsigned)blk[3] << 8);
+    const unsigned code = ((unsigned)blk[4 + texel / 4] >> (2 * (texel % 4))) & 3u;
+    const int e0[3] = {(int)(((c0 >> 11) << 3) | ((c0 >> 11) >> 2)), (int)((((c0 >> 5) & 63u) << 2) | (((c0 >> 5) & 63u) >> 4)),
+                       (int)(((c0 & 31u) << 3) | ((c0 & 31u) >> 2))};
+    const int e1[3] = {(int)(((c1 >> 11) << 3) | ((c1 >> 11) >> 2)), (int)((((c1 >> 5) & 63u) << 2) | (((c1 >> 5) & 63u) >> 4)),
+                       (int)(((c1 & 31u) << 3) | ((c1 & 31u) >> 2))};
+    for (int ch = 0; ch < 3; ++ch) {
+        int v;
+        if (code == 0) v = e0[ch];
+        else if (code == 1) v = e1[ch];
+        else if (force_four || c0 > c1) v = code == 2 ? (2 * e0[ch] + e1[ch] + 1) / 3 : (e0[ch] + 2 * e1[ch] + 1) / 3;
+        else v = code == 2 ? (e0[ch] + e1[ch] + 1) / 2 : 0;
+        rgb[ch] = v;
+    }
+}
+int s3tc_alpha(const unsigned char* blk, int texel) {
+    const int a0 = blk[0], a1 = blk[1];
+    uint64_t bits = 0;
+    for (int b = 0; b < 6; ++b) bits |= (uint64_t)blk[2 + b] << (8 * b);
+    const int k = (int)((bits >> (3 * texel)) & 7u);
+    if (k == 0) return a0;
+    if (k == 1) return a1;
+    if (a0 > a1) return ((8 - k) * a0 + (k - 1) * a1 + 3) / 7;
+    if (k == 6) return 0;
+    if (k == 7) return 255;
+    return ((6 - k) * a0 + (k - 1) * a1 + 2) / 5;
+}
+
 // The brick pool as the reference's 3D texture: texelFetch at global texel
 // (i,j,k) of a (10*slots) per-axis grid, read from the brick-linear slots.
 template <typename T>
@@ -137,6 +172,25 @@ struct BrickTexture {
         const size_t slot = ((size_t)(k / 10) * sy + (size_t)(j / 10)) * sx + (size_t)(i / 10);
         const size_t t = slot * 1000 + (size_t)((k % 10) * 100 + (j % 10) * 10 + (i % 10));
         vec4<T> v;
+        if (fmt == VV_FMT_DXT5 || fmt == VV_FMT_DXT1) {
+            // a slot's 10 slices of 3x3 blocks of 4x4 texels
+            const int x = i % 10, y = j % 10, z = k % 10;
+            const size_t blk = slot * 90 + (size_t)(z * 9 + (y / 4) * 3 + x / 4);
+            const int texel = (y % 4) * 4 + x % 4;
+            int rgb[3], a = 0;
+            if (fmt == VV_FMT_DXT5) {
+                const unsigned char* b = (const unsigned char*)data + 16 * blk;
+                a = s3tc_alpha(b, texel);
+                s3tc_colour(b + 8, texel, true, rgb);
+            } else {
+                s3tc_colour((const unsigned char*)data + 8 * blk, texel, false, rgb);
+            }
+            v.r = (T)rgb[0];
+            v.g = (T)rgb[1];
+            v.b = (T)rgb[2];
+            v.a = (T)a;
+            return v;
+        }
         switch (fmt) {
             case VV_FMT_RGBA8: {
                 uint32_t w;
@@ -264,7 +318,7 @@ struct Shader {
         vec4<T> x01 = lerp4(c001, c101, w[0]), x11 = lerp4(c011, c111, w[0]);
         vec4<T> y0 = lerp4(x00, x10, w[1]), y1 = lerp4(x01, x11, w[1]);
         vec4<T> c = lerp4(y0, y1, w[2]);
-        if (brick.fmt == VV_FMT_RGBA8) {
+        if (brick.fmt == VV_FMT_RGBA8 || brick.fmt == VV_FMT_DXT5 || brick.fmt == VV_FMT_DXT1) {
             const T k = sizeof(T) == 4 ? (T)(1.0f / 255.0f) : (T)1 / (T)255;
             c.r = c.r * k;
             c.g = c.g * k;
@@ -751,6 +805,27 @@ int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, i
 
 int oracle_max_iterations(const vv_uniforms* u) { return max_iterations(u); }
 
+int oracle_dxt_decode(const void* blocks, int fmt, long long bricks, uint32_t* rgba8) {
+    if (!blocks || !rgba8 || bricks < 0 || (fmt != VV_FMT_DXT5 && fmt != VV_FMT_DXT1)) return VV_ERR_ARG;
+    for (long long s = 0; s < bricks; ++s)
+        for (int t = 0; t < 1000; ++t) {
+            const int x = t % 10, y = (t / 10) % 10, z = t / 100;
+            const size_t blk = (size_t)s * 90 + (size_t)(z * 9 + (y / 4) * 3 + x / 4);
+            const int texel = (y % 4) * 4 + x % 4;
+            int rgb[3], a = 0;
+            if (fmt == VV_FMT_DXT5) {
+                const unsigned char* b = (const unsigned char*)blocks + 16 * blk;
+                a = s3tc_alpha(b, texel);
+                s3tc_colour(b + 8, texel, true, rgb);
+            } else {
+                s3tc_colour((const unsigned char*)blocks + 8 * blk, texel, false, rgb);
+            }
+            rgba8[(size_t)s * 1000 + (size_t)t] =
+                (uint32_t)rgb[0] | ((uint32_t)rgb[1] << 8) | ((uint32_t)rgb[2] << 16) | ((uint32_t)a << 24);
+        }
+    return VV_OK;
+}
+
 int oracle_raycast_trace(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
                          void* color, uint32_t* usage, uint64_t* trace, int threads, int32_t* status) {
     if (!u || !s || row0 < 0 || row1 > u->height || row0 > row1) return VV_ERR_ARG;
@@ -785,7 +860,7 @@ void sample64(const BrickTexture<double>& bt, const float N[3], const float bpos
         acc[2] += wt * v.b;
         acc[3] += wt * v.a;
     }
-    const double k = bt.fmt == VV_FMT_RGBA8 ? 1.0 / 255.0 : 1.0;
+    const double k = (bt.fmt == VV_FMT_RGBA8 || bt.fmt == VV_FMT_DXT5 || bt.fmt == VV_FMT_DXT1) ? 1.0 / 255.0 : 1.0;
     for (int c = 0; c < 4; ++c) out[c] = acc[c] * k;
 }
 

@@ -24,6 +24,9 @@ typedef struct oracle_scene {
 int oracle_raycast(const vv_uniforms* u, const oracle_scene* s, int precision, int row0, int row1,
                    void* color, uint32_t* usage, int threads, int32_t* status);
 int oracle_max_iterations(const vv_uniforms* u);
+/* The RGBA8 texels (1000 per brick) of `bricks` DXT5 or DXT1 pool slots
+ * (90 blocks each), decoded as the oracle's texture fetch decodes them. */
+int oracle_dxt_decode(const void* blocks, int fmt, long long bricks, uint32_t* rgba8);
 /* oracle_raycast plus `trace` (one uint64 per pixel of the full image, may
  * be NULL): a hash of each pixel's control flow (fragment, inside test, per
  * leaf segment the node, depth, flags, step count and samples composited,

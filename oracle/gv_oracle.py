@@ -54,6 +54,8 @@ def load() -> C.CDLL:
     lib.oracle_raycast_trace.restype = C.c_int
     lib.oracle_raycast_trace.argtypes = [C.POINTER(Uniforms), C.POINTER(OracleScene), C.c_int, C.c_int, C.c_int,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]
+    lib.oracle_dxt_decode.restype = C.c_int
+    lib.oracle_dxt_decode.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p]
     lib.oracle_max_iterations.restype = C.c_int
     lib.oracle_max_iterations.argtypes = [C.POINTER(Uniforms)]
     lib.oracle_backward.restype = C.c_int
@@ -193,6 +195,17 @@ def compress(usage: np.ndarray, mask: np.ndarray, max_push: int, cap: int):
     lib.oracle_compress(_p(u), _p(m), W, H, max_push, cap, _p(out), C.byref(tot))
     n = min(tot.value, cap)
     return out[:n].copy(), tot.value
+
+
+def dxt_decode(blocks: np.ndarray, fmt: int) -> np.ndarray:
+    """(bricks, 1000) uint32 RGBA8 texels of DXT5 (1440 B) or DXT1 (720 B) slots."""
+    b = np.ascontiguousarray(blocks, dtype=np.uint8)
+    n = b.shape[0]
+    out = np.zeros((n, 1000), dtype=np.uint32)
+    rc = load().oracle_dxt_decode(_p(b), int(fmt), n, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_dxt_decode failed: {rc}")
+    return out
 
 
 def max_iterations(u) -> int:

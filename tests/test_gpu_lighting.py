@@ -19,13 +19,13 @@ def lit_scene():
     g = helpers.GpuScene(sc)
     n = sc.xyz.shape[0]
     grads = {}
-    for gf in ("fp32", "rgba8"):
-        grads[gf] = np.zeros((sc.pool.shape[0], 1000 * vv.TEXEL_BYTES[vv.fmt_code(gf)]), dtype=np.uint8)
+    for gf in ("fp32", "rgba8", "dxt1"):
+        grads[gf] = np.zeros((sc.pool.shape[0], vv.BRICK_BYTES[vv.fmt_code(gf)]), dtype=np.uint8)
         grads[gf][:n] = sc.octree.produce_gradients(sc.xyz, gf)
     return sc, g, grads
 
 
-@pytest.mark.parametrize("gfmt,unsigned", [("fp32", 0), ("rgba8", 1)])
+@pytest.mark.parametrize("gfmt,unsigned", [("fp32", 0), ("rgba8", 1), ("dxt1", 1)])
 def test_lit_view_matches_oracle(lit_scene, gfmt, unsigned):
     sc, g, grads = lit_scene
     n = sc.xyz.shape[0]

@@ -15,13 +15,13 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("fmt,device_paging", [("rgba8", False), ("fp16", False), ("rgba8", True),
-                                               ("bf16", True)])
+                                               ("bf16", True), ("dxt5", True), ("dxt5", False)])
 def test_paged_camera_path_matches_oracle_and_policy(fmt, device_paging):
     depth, W, H, frames = 6, 256, 160, 12
     o = helpers.octree(seed=3, depth=depth)
     f = vv.fmt_code(fmt)
     pool_bricks = 700
-    pool_bytes = pool_bricks * 1000 * vv.TEXEL_BYTES[f]
+    pool_bytes = pool_bricks * vv.BRICK_BYTES[f]
     slots = scene.slot_grid(pool_bricks)
     ctx = vv.Context(0)
     r = vv.Renderer(ctx, o, fmt=fmt, pool_bytes=pool_bytes, preload_all=False, alpha_stop=0.99, jitter_seed=7,

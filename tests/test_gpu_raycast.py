@@ -59,7 +59,7 @@ def test_full_tree_and_camera_inside():
         assert np.array_equal(got["requests"], ref["requests"])
 
 
-@pytest.mark.parametrize("fmt", ["fp16", "bf16", "fp32"])
+@pytest.mark.parametrize("fmt", ["fp16", "bf16", "fp32", "dxt5"])
 def test_float_brick_formats_match_oracle(fmt):
     sc = helpers.Scene(seed=1, depth=5, fmt=fmt)
     g = helpers.GpuScene(sc)
@@ -104,7 +104,7 @@ def test_miss_only_view_is_empty(cfg1):
 
 
 @pytest.mark.parametrize("fmt,view,size", [("rgba8", 3, (512, 512)), ("fp16", 5, (333, 177)),
-                                           ("rgba8", 8, (1920, 1080)), ("fp32", 9, (61, 37))])
+                                           ("rgba8", 8, (1920, 1080)), ("fp32", 9, (61, 37)), ("dxt5", 4, (256, 256))])
 def test_lane_refill_ray_cast_equals_tiles(fmt, view, size):
     """VV_RAYCAST_REFILL (persistent warps, finished lanes take new pixels)
     gives the same colour, usage lists, mask and requests as the tiled

@@ -25,7 +25,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _native as N
-from ._native import (FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_FP16, VV_FMT_FP32, VV_FMT_RGBA8,  # noqa: F401
+from ._native import (BRICK_BYTES, FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_DXT1, VV_FMT_DXT5, VV_FMT_FP16, VV_FMT_FP32, VV_FMT_RGBA8,  # noqa: F401
                       VV_PASS_ALL, VV_PASS_COLOR_RGBA8, VV_PASS_COMPACT, VV_PASS_RAYCAST, VV_PASS_SELECT, Camera,
                       FrameOut,
                       NodePatch, OctreeInfo, Uniforms, VVError)
@@ -33,7 +33,7 @@ from ._native import (FMT_NAMES, TEXEL_BYTES, VV_FMT_BF16, VV_FMT_FP16, VV_FMT_F
 __all__ = ["Octree", "Context", "Renderer", "Batch", "Scene", "batch_variants", "make_camera", "look_at",
            "read_gvp", "write_gvp",
            "compute_uniforms", "make_jitter", "pixel_size", "lib", "VVError", "Uniforms", "Camera", "FMT_NAMES",
-           "TEXEL_BYTES"]
+           "TEXEL_BYTES", "BRICK_BYTES"]
 
 
 def lib() -> C.CDLL:
@@ -192,7 +192,7 @@ class Octree:
         f = fmt_code(fmt)
         xyz = np.ascontiguousarray(xyz, dtype=np.uint32).reshape(-1, 3)
         n = xyz.shape[0]
-        out = np.zeros((n, 1000 * TEXEL_BYTES[f]), dtype=np.uint8)
+        out = np.zeros((n, BRICK_BYTES[f]), dtype=np.uint8)
         _check(lib().vv_octree_produce_bricks(self._h, _ptr(xyz), n, f, _ptr(out)), what="produce bricks")
         return out
 
@@ -201,7 +201,7 @@ class Octree:
         f = fmt_code(fmt)
         xyz = np.ascontiguousarray(xyz, dtype=np.uint32).reshape(-1, 3)
         n = xyz.shape[0]
-        out = np.zeros((n, 1000 * TEXEL_BYTES[f]), dtype=np.uint8)
+        out = np.zeros((n, BRICK_BYTES[f]), dtype=np.uint8)
         _check(lib().vv_octree_produce_gradients(self._h, _ptr(xyz), n, f, _ptr(out)), what="produce gradients")
         return out
 
@@ -331,8 +331,8 @@ class Context:
     def upload_bricks(self, slot_ids: np.ndarray, texels: np.ndarray) -> None:
         s = np.ascontiguousarray(slot_ids, dtype=np.uint32)
         t = np.ascontiguousarray(texels)
-        if t.nbytes != s.size * 1000 * TEXEL_BYTES[self.fmt]:
-            raise VVError(N.VV_ERR_ARG, "texels must hold 1000 texels per slot id in the pool's format")
+        if t.nbytes != s.size * BRICK_BYTES[self.fmt]:
+            raise VVError(N.VV_ERR_ARG, "texels must hold one brick per slot id in the pool's format")
         self._ck(lib().vv_upload_bricks(self._h, _ptr(s), s.size, _ptr(t)), "brick upload")
 
     def download_bricks(self) -> np.ndarray:
@@ -340,7 +340,7 @@ class Context:
         n = sx * sy * sz
         if n == 0:
             raise VVError(N.VV_ERR_STATE, "brick pool not created")
-        out = np.zeros((n, 1000 * TEXEL_BYTES[self.fmt]), dtype=np.uint8)
+        out = np.zeros((n, BRICK_BYTES[self.fmt]), dtype=np.uint8)
         self._ck(lib().vv_brickpool_download(self._h, _ptr(out)), "brick download")
         return out
 

@@ -14,11 +14,15 @@ LIB_PATH = Path(__file__).resolve().parent / "libvoxviz_b200.so"
 VV_OK, VV_ERR_ARG, VV_ERR_OOM, VV_ERR_CUDA, VV_ERR_TIMEOUT, VV_ERR_BOUNDS, VV_ERR_STATE, VV_ERR_NODEV, VV_ERR_IO = range(9)
 VV_GVX_CONSTANT_COLORS, VV_GVX_SKIP_GRADIENTS = 1, 2
 VV_SCENE_HOST_ONLY, VV_SCENE_SYNCHRONOUS, VV_SCENE_BATCHED = 1, 2, 4
-VV_FMT_RGBA8, VV_FMT_FP16, VV_FMT_BF16, VV_FMT_FP32 = range(4)
+VV_FMT_RGBA8, VV_FMT_FP16, VV_FMT_BF16, VV_FMT_FP32, VV_FMT_DXT5, VV_FMT_DXT1 = range(6)
 VV_PASS_RAYCAST, VV_PASS_SELECT, VV_PASS_COMPACT, VV_PASS_ALL = 1, 2, 4, 7
 VV_PASS_COLOR_RGBA8 = 8
-FMT_NAMES = {"rgba8": VV_FMT_RGBA8, "fp16": VV_FMT_FP16, "bf16": VV_FMT_BF16, "fp32": VV_FMT_FP32}
+FMT_NAMES = {"rgba8": VV_FMT_RGBA8, "fp16": VV_FMT_FP16, "bf16": VV_FMT_BF16, "fp32": VV_FMT_FP32,
+             "dxt5": VV_FMT_DXT5, "dxt1": VV_FMT_DXT1}
 TEXEL_BYTES = {VV_FMT_RGBA8: 4, VV_FMT_FP16: 8, VV_FMT_BF16: 8, VV_FMT_FP32: 16}
+# bytes of one stored brick (pool slot): 1000 texels, or 90 S3TC blocks
+BRICK_BYTES = {VV_FMT_RGBA8: 4000, VV_FMT_FP16: 8000, VV_FMT_BF16: 8000, VV_FMT_FP32: 16000, VV_FMT_DXT5: 1440,
+               VV_FMT_DXT1: 720}
 
 f3 = C.c_float * 3
 i3 = C.c_int32 * 3

@@ -136,8 +136,8 @@ int vv_octree_node_info(const vv_octree* t, uint32_t x, uint32_t y, uint32_t z, 
 
 int vv_octree_produce_bricks(const vv_octree* t, const uint32_t* xyz, int32_t n, int32_t fmt, void* out) {
     if (!t || n < 0 || (n > 0 && (!xyz || !out))) return VV_ERR_ARG;
-    const size_t tb = vv::texel_bytes(fmt);
-    if (!tb) return VV_ERR_ARG;
+    const size_t bb = vv::brick_bytes(fmt);
+    if (!bb || fmt == VV_FMT_DXT1) return VV_ERR_ARG;
     for (int32_t i = 0; i < n; ++i) {
         const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
         if (idx == vv::kNoParent || t->tree->level(idx) < 0) return VV_ERR_ARG;
@@ -146,16 +146,16 @@ int vv_octree_produce_bricks(const vv_octree* t, const uint32_t* xyz, int32_t n,
 #pragma omp parallel for schedule(dynamic, 16)
     for (int32_t i = 0; i < n; ++i) {
         const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
-        t->tree->produce_brick(idx, fmt, o + (size_t)i * VV_BRICK_TEXELS * tb);
+        t->tree->produce_brick(idx, fmt, o + (size_t)i * bb);
     }
     return VV_OK;
 }
 
 int vv_octree_produce_gradients(const vv_octree* t, const uint32_t* xyz, int32_t n, int32_t fmt, void* out) {
     if (!t || n < 0 || (n > 0 && (!xyz || !out))) return VV_ERR_ARG;
-    if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return VV_ERR_ARG;
+    if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8 && fmt != VV_FMT_DXT1) return VV_ERR_ARG;
     if (t->tree->file_backed() ? !t->tree->file_has_normals() : t->tree->depth() > 6) return VV_ERR_ARG;
-    const size_t tb = vv::texel_bytes(fmt);
+    const size_t tb = vv::brick_bytes(fmt);
     for (int32_t i = 0; i < n; ++i) {
         const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
         if (idx == vv::kNoParent || t->tree->level(idx) < 0) return VV_ERR_ARG;
@@ -168,7 +168,7 @@ int vv_octree_produce_gradients(const vv_octree* t, const uint32_t* xyz, int32_t
 #pragma omp parallel for schedule(dynamic, 16)
     for (int32_t i = 1; i < n; ++i) {
         const uint32_t idx = t->tree->index_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
-        t->tree->produce_gradient_brick(idx, fmt, o + (size_t)i * VV_BRICK_TEXELS * tb);
+        t->tree->produce_gradient_brick(idx, fmt, o + (size_t)i * tb);
     }
     return VV_OK;
 }
@@ -320,7 +320,7 @@ int vv_scene_create(vv_ctx* ctx, const char* gvp_path, const vv_scene_desc* d, v
         vv::set_thread_error("vv_scene_create: a context is required unless VV_SCENE_HOST_ONLY");
         return VV_ERR_ARG;
     }
-    if (!(d->flags & VV_SCENE_HOST_ONLY) && !vv::texel_bytes(d->fmt)) return VV_ERR_ARG;
+    if (!(d->flags & VV_SCENE_HOST_ONLY) && (!vv::brick_bytes(d->fmt) || d->fmt == VV_FMT_DXT1)) return VV_ERR_ARG;
     try {
         vv::GvpFile f;
         std::string err;

@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "../../include/voxviz_b200.h"
+#include "dxt.h"
 
 namespace vv {
 
@@ -25,6 +26,13 @@ constexpr int kCellsPerAxis = 9;
 template <int FMT>
 __device__ __forceinline__ bool texel_is_zero(const void* pool, size_t i) {
     if (FMT == VV_FMT_RGBA8) return ((const uint32_t*)pool)[i] == 0u;
+    if (FMT == VV_FMT_DXT5) {  // the decoded texel
+        const size_t slot = i / 1000u;
+        const int r = (int)(i - slot * 1000u), z = r / 100, y = (r / 10) % 10, x = r % 10;
+        const uint4 v = ((const uint4*)pool)[slot * dxt::kBlocksPerSlot + (size_t)dxt::block_of(x, y, z)];
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        return dxt::decode_dxt5(w, dxt::texel_of(x, y)) == 0u;
+    }
     if (FMT == VV_FMT_FP32) {
         const uint4 v = ((const uint4*)pool)[i];
         return (v.x | v.y | v.z | v.w) == 0u;

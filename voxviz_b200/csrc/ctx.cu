@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "dxt.h"
 #include "cellmask.cuh"
 #include "kernels.cuh"
 
@@ -32,12 +33,16 @@ int cuda_fail(vv_ctx* c, cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail(c, e_, #expr); \
     } while (0)
 
-size_t fmt_texel_bytes(int fmt) {
+// Bytes of one stored brick (slot) of a pool in `fmt`; 0 for a format the
+// brick pool (grad false) or the gradient pool (grad true) cannot hold.
+size_t fmt_brick_bytes(int fmt, bool grad) {
     switch (fmt) {
-        case VV_FMT_RGBA8: return 4;
-        case VV_FMT_FP16: return 8;
-        case VV_FMT_BF16: return 8;
-        case VV_FMT_FP32: return 16;
+        case VV_FMT_RGBA8: return 4u * VV_BRICK_TEXELS;
+        case VV_FMT_FP16: return grad ? 0u : 8u * VV_BRICK_TEXELS;
+        case VV_FMT_BF16: return grad ? 0u : 8u * VV_BRICK_TEXELS;
+        case VV_FMT_FP32: return 16u * VV_BRICK_TEXELS;
+        case VV_FMT_DXT5: return grad ? 0u : (size_t)dxt::kDxt5SlotBytes;
+        case VV_FMT_DXT1: return grad ? (size_t)dxt::kDxt1SlotBytes : 0u;
         default: return 0;
     }
 }
@@ -286,8 +291,8 @@ int vv_brickpool_create(vv_ctx* c, int32_t sx, int32_t sy, int32_t sz, int32_t f
     if (!c) return VV_ERR_ARG;
     if (sx <= 0 || sy <= 0 || sz <= 0 || sx * 10 > 1023 || sy * 10 > 1023 || sz * 10 > 1023)
         return fail(c, VV_ERR_ARG, "brick pool slots per axis must be in [1,102]");
-    const size_t tb = fmt_texel_bytes(fmt);
-    if (!tb) return fail(c, VV_ERR_ARG, "unknown brick format");
+    const size_t bb = fmt_brick_bytes(fmt, false);
+    if (!bb) return fail(c, VV_ERR_ARG, "unknown brick format");
     cudaSetDevice(c->device);
     if (c->bricks) {
         VV_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -300,7 +305,7 @@ int vv_brickpool_create(vv_ctx* c, int32_t sx, int32_t sy, int32_t sz, int32_t f
     }
     c->bricks_external = false;
     const long long total = (long long)sx * sy * sz;
-    const size_t bytes = (size_t)total * VV_BRICK_TEXELS * tb;
+    const size_t bytes = (size_t)total * bb;
     cudaError_t e = cudaMalloc(&c->bricks, bytes);
     if (e != cudaSuccess) {
         c->bricks = nullptr;
@@ -312,7 +317,7 @@ int vv_brickpool_create(vv_ctx* c, int32_t sx, int32_t sy, int32_t sz, int32_t f
     c->slots[2] = sz;
     c->total_slots = total;
     c->fmt = fmt;
-    c->brick_bytes = VV_BRICK_TEXELS * tb;
+    c->brick_bytes = bb;
     c->pool_bytes = bytes;
     return rebuild_cell_masks(c);  // of the zeroed pool
 }
@@ -368,7 +373,7 @@ int vv_upload_bricks(vv_ctx* c, const uint32_t* slots, int32_t n, const void* te
 
 int vv_gradpool_create(vv_ctx* c, int32_t fmt) {
     if (!c) return VV_ERR_ARG;
-    if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return fail(c, VV_ERR_ARG, "gradient pool format: FP32 or RGBA8");
+    if (!fmt_brick_bytes(fmt, true)) return fail(c, VV_ERR_ARG, "gradient pool format: FP32, RGBA8 or DXT1");
     if (!c->bricks) return fail(c, VV_ERR_STATE, "create the brick pool first");
     cudaSetDevice(c->device);
     if (c->grads) {
@@ -376,8 +381,8 @@ int vv_gradpool_create(vv_ctx* c, int32_t fmt) {
         cudaFree(c->grads);
         c->grads = nullptr;
     }
-    const size_t tb = fmt_texel_bytes(fmt);
-    const size_t bytes = (size_t)c->total_slots * VV_BRICK_TEXELS * tb;
+    const size_t gb = fmt_brick_bytes(fmt, true);
+    const size_t bytes = (size_t)c->total_slots * gb;
     cudaError_t e = cudaMalloc(&c->grads, bytes);
     if (e != cudaSuccess) {
         c->grads = nullptr;
@@ -385,7 +390,7 @@ int vv_gradpool_create(vv_ctx* c, int32_t fmt) {
     }
     VV_CUDA(c, cudaMemsetAsync(c->grads, 0, bytes, c->stream));
     c->grad_fmt = fmt;
-    c->grad_brick_bytes = VV_BRICK_TEXELS * tb;
+    c->grad_brick_bytes = gb;
     c->grad_pool_bytes = bytes;
     return VV_OK;
 }
@@ -430,8 +435,8 @@ int vv_brickpool_attach(vv_ctx* c, void* texels, int32_t sx, int32_t sy, int32_t
     if (!c || !texels) return fail(c, VV_ERR_ARG, "bad attach arguments");
     if (sx <= 0 || sy <= 0 || sz <= 0 || sx * 10 > 1023 || sy * 10 > 1023 || sz * 10 > 1023)
         return fail(c, VV_ERR_ARG, "brick pool slots per axis must be in [1,102]");
-    const size_t tb = fmt_texel_bytes(fmt);
-    if (!tb) return fail(c, VV_ERR_ARG, "unknown brick format");
+    const size_t bb = fmt_brick_bytes(fmt, false);
+    if (!bb) return fail(c, VV_ERR_ARG, "unknown brick format");
     if (((uintptr_t)texels & 15u) != 0) return fail(c, VV_ERR_ARG, "attached pool must be 16-byte aligned");
     cudaSetDevice(c->device);
     // Launches already queued hold the old pointer by value; only an owned
@@ -447,8 +452,8 @@ int vv_brickpool_attach(vv_ctx* c, void* texels, int32_t sx, int32_t sy, int32_t
     c->slots[2] = sz;
     c->total_slots = (long long)sx * sy * sz;
     c->fmt = fmt;
-    c->brick_bytes = VV_BRICK_TEXELS * tb;
-    c->pool_bytes = (size_t)c->total_slots * VV_BRICK_TEXELS * tb;
+    c->brick_bytes = bb;
+    c->pool_bytes = (size_t)c->total_slots * bb;
     // the caller writes this memory: no empty-cell skipping until
     // vv_brickpool_update_cell_masks
     return alloc_cell_masks(c);
@@ -470,6 +475,7 @@ static int diff_params(vv_ctx* c, int32_t tree, const vv_uniforms* u, RaycastPar
         if (u->brick_pool_dimension[a] != (float)(c->slots[a] * 10))
             return fail(c, VV_ERR_ARG, "brick_pool_dimension does not match the brick pool");
     if (u->compute_lighting) return fail(c, VV_ERR_ARG, "the adjoint covers the unlit ray cast only");
+    if (c->fmt == VV_FMT_DXT5) return fail(c, VV_ERR_ARG, "the adjoint needs an uncompressed brick pool");
     std::memset(&p, 0, sizeof(p));
     p.u = *u;
     set_divisors(p);

@@ -53,8 +53,8 @@ __global__ void __launch_bounds__(128, 7) raycast_refill_kernel(const __grid_con
 }
 
 cudaError_t launch_raycast_refill(int fmt, const RaycastParams& p, unsigned int* counter, cudaStream_t s) {
-    static int ctas[4] = {0, 0, 0, 0};  // resident CTAs on the device (per format)
-    if (fmt < 0 || fmt > 3) return cudaErrorInvalidValue;
+    static int ctas[5] = {0, 0, 0, 0, 0};  // resident CTAs on the device (per format)
+    if (fmt < 0 || fmt > VV_FMT_DXT5) return cudaErrorInvalidValue;
     cudaError_t e = cudaSuccess;
     if (!ctas[fmt]) {
         int dev = 0, sms = 0, per_sm = 0;
@@ -71,6 +71,9 @@ cudaError_t launch_raycast_refill(int fmt, const RaycastParams& p, unsigned int*
                 case VV_FMT_BF16:
                     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raycast_refill_kernel<VV_FMT_BF16>, 128, 0);
                     break;
+                case VV_FMT_DXT5:
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raycast_refill_kernel<VV_FMT_DXT5>, 128, 0);
+                    break;
                 default:
                     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raycast_refill_kernel<VV_FMT_FP32>, 128, 0);
                     break;
@@ -86,6 +89,7 @@ cudaError_t launch_raycast_refill(int fmt, const RaycastParams& p, unsigned int*
         case VV_FMT_RGBA8: raycast_refill_kernel<VV_FMT_RGBA8><<<grid, block, 0, s>>>(p, counter); break;
         case VV_FMT_FP16: raycast_refill_kernel<VV_FMT_FP16><<<grid, block, 0, s>>>(p, counter); break;
         case VV_FMT_BF16: raycast_refill_kernel<VV_FMT_BF16><<<grid, block, 0, s>>>(p, counter); break;
+        case VV_FMT_DXT5: raycast_refill_kernel<VV_FMT_DXT5><<<grid, block, 0, s>>>(p, counter); break;
         default: raycast_refill_kernel<VV_FMT_FP32><<<grid, block, 0, s>>>(p, counter); break;
     }
     return cudaGetLastError();
@@ -105,6 +109,7 @@ cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s) {
         case VV_FMT_FP16: VV_LAUNCH(VV_FMT_FP16) break;
         case VV_FMT_BF16: VV_LAUNCH(VV_FMT_BF16) break;
         case VV_FMT_FP32: VV_LAUNCH(VV_FMT_FP32) break;
+        case VV_FMT_DXT5: VV_LAUNCH(VV_FMT_DXT5) break;
         default: return cudaErrorInvalidValue;
     }
 #undef VV_LAUNCH
@@ -425,6 +430,7 @@ cudaError_t launch_cell_masks(const uint32_t* slots, long long n, const void* po
         case VV_FMT_FP16: cell_mask_kernel<VV_FMT_FP16><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
         case VV_FMT_BF16: cell_mask_kernel<VV_FMT_BF16><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
         case VV_FMT_FP32: cell_mask_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
+        case VV_FMT_DXT5: cell_mask_kernel<VV_FMT_DXT5><<<grid, 256, 0, s>>>(slots, pool, total_slots, masks); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -1,6 +1,8 @@
 // octree.cpp - terrain octree builder, node-pool layout and brick production.
 #include "octree.h"
 
+#include "dxt.h"
+
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -451,6 +453,22 @@ size_t texel_bytes(int fmt) {
     }
 }
 
+size_t brick_bytes(int fmt) {
+    if (fmt == VV_FMT_DXT5) return (size_t)dxt::kDxt5SlotBytes;
+    if (fmt == VV_FMT_DXT1) return (size_t)dxt::kDxt1SlotBytes;
+    return VV_BRICK_TEXELS * texel_bytes(fmt);
+}
+
+// The 90 blocks of a brick (10^3 RGBA8 texels) in DXT5 or DXT1.
+static void encode_brick_dxt(const uint32_t* rgba, int fmt, void* out) {
+    for (int b = 0; b < dxt::kBlocksPerSlot; ++b) {
+        uint32_t px[16], valid;
+        dxt::gather_block(rgba, b, px, valid);
+        if (fmt == VV_FMT_DXT5) dxt::encode_dxt5(px, valid, (uint32_t*)out + 4 * b);
+        else dxt::encode_dxt1(px, valid, (uint32_t*)out + 2 * b);
+    }
+}
+
 uint16_t float_to_half_rn(float f) {
     uint32_t x;
     std::memcpy(&x, &f, 4);
@@ -508,12 +526,22 @@ void convert_texel(uint32_t v, int fmt, void* dst) {
 void GigaVoxelsOctTree::produce_brick(uint32_t n, int fmt, void* out) const {
     uint32_t tmp[VV_BRICK_TEXELS];
     produce_brick_rgba8(n, tmp);
+    if (fmt == VV_FMT_DXT5) {
+        encode_brick_dxt(tmp, fmt, out);
+        return;
+    }
     const size_t tb = texel_bytes(fmt);
     unsigned char* o = (unsigned char*)out;
     for (int t = 0; t < VV_BRICK_TEXELS; ++t) convert_texel(tmp[t], fmt, o + (size_t)t * tb);
 }
 
 bool GigaVoxelsOctTree::produce_gradient_brick(uint32_t n, int fmt, void* out) const {
+    if (fmt == VV_FMT_DXT1) {  // the unsigned RGBA8 gradients, block-compressed
+        uint32_t tmp[VV_BRICK_TEXELS];
+        if (!produce_gradient_brick(n, VV_FMT_RGBA8, tmp)) return false;
+        encode_brick_dxt(tmp, fmt, out);
+        return true;
+    }
     if (fmt != VV_FMT_FP32 && fmt != VV_FMT_RGBA8) return false;
     if (file_) {
         // the file's unsigned bytes (GradientsAreUnsigned is set for every

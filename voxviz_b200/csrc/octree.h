@@ -163,6 +163,9 @@ bool classify_node(const TerrainVolume& vol, int d, int i, int j, int k, uint32_
 // Store one normalized value v/255 (v in [0,255]) as the given format.
 void convert_texel(uint32_t rgba8, int fmt, void* dst);
 size_t texel_bytes(int fmt);
+// Bytes of one stored brick in fmt (1000 texels, or 90 blocks for DXT5 /
+// DXT1); 0 for an unknown format.
+size_t brick_bytes(int fmt);
 uint16_t float_to_half_rn(float f);
 uint16_t float_to_bf16_rn(float f);
 

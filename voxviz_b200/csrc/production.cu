@@ -7,6 +7,7 @@
 
 #include "../../include/voxviz_b200.h"
 #include "cellmask.cuh"
+#include "dxt.h"
 #include "production.h"
 #include "terrain.h"
 
@@ -79,12 +80,24 @@ __device__ __forceinline__ void store_texel(void* pool, size_t i, uint32_t v) {
     }
 }
 
+// A DXT5 pool slot from the brick's RGBA8 texels in shared memory (all
+// threads of the CTA, after a barrier): one 16-byte block per thread.
+__device__ __forceinline__ void encode_dxt5_slot(const uint32_t* rgba, void* pool, size_t slot) {
+    for (int b = threadIdx.x; b < dxt::kBlocksPerSlot; b += blockDim.x) {
+        uint32_t px[16], valid, w[4];
+        dxt::gather_block(rgba, b, px, valid);
+        dxt::encode_dxt5(px, valid, w);
+        ((uint4*)pool)[slot * dxt::kBlocksPerSlot + (size_t)b] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
 // One CTA per brick.  Texel (bx,by,bz) of node (d; i,j,k) is the mip-level
 // (L-d) voxel (8i-1+bx, 8j-1+by, 8k-1+bz), transparent black outside the level.
 template <int FMT>
 __device__ __forceinline__ void produce_one(const DeviceTerrainView& t, const uint4 job, void* __restrict__ pool,
                                             uint32_t* __restrict__ masks, long long total_slots, int* status) {
     __shared__ uint8_t zero[VV_BRICK_TEXELS];  // texel all-zero flags for the slot's cell mask
+    __shared__ uint32_t rgba[FMT == VV_FMT_DXT5 ? VV_BRICK_TEXELS : 1];  // the brick before compression
     if ((long long)job.x >= total_slots || (int)job.y > t.depth) {
         if (threadIdx.x == 0 && status) atomicCAS(status, 0, VV_ERR_BOUNDS);
         return;
@@ -107,14 +120,19 @@ __device__ __forceinline__ void produce_one(const DeviceTerrainView& t, const ui
                 if (z < s + r) v = L.data[L.off[c] + (uint32_t)(z - s)];
             }
         }
-        store_texel<FMT>(pool, base + (size_t)q, v);
-        zero[q] = v == 0u ? 1 : 0;  // RGBA8 zero stores as zero in every format
+        if constexpr (FMT == VV_FMT_DXT5) rgba[q] = v;
+        else store_texel<FMT>(pool, base + (size_t)q, v);
+        zero[q] = v == 0u ? 1 : 0;  // RGBA8 zero stores (and DXT-decodes) as zero in every format
+    }
+    if constexpr (FMT == VV_FMT_DXT5) {
+        __syncthreads();
+        encode_dxt5_slot(rgba, pool, (size_t)job.x);
     }
     if (masks) {  // the same for the whole CTA
         __syncthreads();
         write_cell_mask(zero, masks + (size_t)job.x * kCellMaskWords);
-        __syncthreads();  // zero[] serves the CTA's next job
     }
+    __syncthreads();  // zero[] and rgba[] serve the CTA's next job
 }
 
 template <int FMT>
@@ -152,6 +170,7 @@ template <int FMT>
 __device__ __forceinline__ void copy_one(const DeviceBrickStoreView& st, const uint4 job, void* __restrict__ pool,
                                          uint32_t* __restrict__ masks, long long total_slots, int* status) {
     __shared__ uint8_t zero[VV_BRICK_TEXELS];
+    __shared__ uint32_t rgba[FMT == VV_FMT_DXT5 ? VV_BRICK_TEXELS : 1];
     if ((long long)job.x >= total_slots || job.y >= st.bricks) {
         if (threadIdx.x == 0 && status) atomicCAS(status, 0, VV_ERR_BOUNDS);
         return;
@@ -172,8 +191,13 @@ __device__ __forceinline__ void copy_one(const DeviceBrickStoreView& st, const u
     } else {
         for (int q = threadIdx.x; q < VV_BRICK_TEXELS; q += blockDim.x) {
             const uint32_t v = __ldg(src + q);
-            store_texel<FMT>(pool, base + (size_t)q, v);
+            if constexpr (FMT == VV_FMT_DXT5) rgba[q] = v;
+            else store_texel<FMT>(pool, base + (size_t)q, v);
             zero[q] = v == 0u;
+        }
+        if constexpr (FMT == VV_FMT_DXT5) {
+            __syncthreads();
+            encode_dxt5_slot(rgba, pool, (size_t)job.x);
         }
     }
     if (masks) {
@@ -607,6 +631,7 @@ cudaError_t launch_produce_bricks(const DeviceTerrainView& t, const uint4* jobs,
         case VV_FMT_FP16: produce_kernel<VV_FMT_FP16><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
         case VV_FMT_BF16: produce_kernel<VV_FMT_BF16><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
         case VV_FMT_FP32: produce_kernel<VV_FMT_FP32><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_DXT5: produce_kernel<VV_FMT_DXT5><<<n, 256, 0, s>>>(t, jobs, pool, masks, total_slots, status); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -632,6 +657,9 @@ cudaError_t launch_produce_staged(const DeviceTerrainView& t, const uint4* jobs,
             break;
         case VV_FMT_FP32:
             produce_staged_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, masks, total_slots, status);
+            break;
+        case VV_FMT_DXT5:
+            produce_staged_kernel<VV_FMT_DXT5><<<grid, 256, 0, s>>>(t, jobs, count, max_jobs, pool, masks, total_slots, status);
             break;
         default: return cudaErrorInvalidValue;
     }
@@ -666,6 +694,7 @@ cudaError_t launch_copy_bricks(const DeviceBrickStoreView& st, const uint4* jobs
         case VV_FMT_FP16: copy_kernel<VV_FMT_FP16><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
         case VV_FMT_BF16: copy_kernel<VV_FMT_BF16><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
         case VV_FMT_FP32: copy_kernel<VV_FMT_FP32><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
+        case VV_FMT_DXT5: copy_kernel<VV_FMT_DXT5><<<n, 256, 0, s>>>(st, jobs, pool, masks, total_slots, status); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -691,6 +720,9 @@ cudaError_t launch_copy_staged(const DeviceBrickStoreView& st, const uint4* jobs
             break;
         case VV_FMT_FP32:
             copy_staged_kernel<VV_FMT_FP32><<<grid, 256, 0, s>>>(st, jobs, count, max_jobs, pool, masks, total_slots, status);
+            break;
+        case VV_FMT_DXT5:
+            copy_staged_kernel<VV_FMT_DXT5><<<grid, 256, 0, s>>>(st, jobs, count, max_jobs, pool, masks, total_slots, status);
             break;
         default: return cudaErrorInvalidValue;
     }

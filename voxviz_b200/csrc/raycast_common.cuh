@@ -13,6 +13,7 @@
 #include <cuda_fp16.h>
 
 #include "cellmask.cuh"
+#include "dxt.h"
 #include "fixed_div.h"
 #include "kernels.cuh"
 #include "lod_bound.h"
@@ -99,6 +100,42 @@ struct Texel<VV_FMT_FP32> {
     static constexpr float kScale = 1.0f;
     __device__ __forceinline__ static float4 load(const void* pool, uint32_t i) {
         return __ldg((const float4*)pool + i);
+    }
+};
+
+// Block-compressed pools (dxt.h): texel i = slot * 1000 + (z*10 + y)*10 + x
+// decoded from its 4x4 block of slice z, as RGBA8 values.
+__device__ __forceinline__ void dxt_address(uint32_t i, uint32_t& block, int& t) {
+    const uint32_t slot = i / 1000u, r = i - slot * 1000u;
+    const uint32_t z = r / 100u, yx = r - z * 100u, y = yx / 10u, x = yx - y * 10u;
+    block = slot * (uint32_t)dxt::kBlocksPerSlot + (uint32_t)dxt::block_of((int)x, (int)y, (int)z);
+    t = dxt::texel_of((int)x, (int)y);
+}
+template <>
+struct Texel<VV_FMT_DXT5> {
+    static constexpr float kScale = 1.0f / 255.0f;
+    __device__ __forceinline__ static float4 load(const void* pool, uint32_t i) {
+        uint32_t b;
+        int t;
+        dxt_address(i, b, t);
+        const uint4 v = __ldg((const uint4*)pool + b);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        const uint32_t c = dxt::decode_dxt5(w, t);
+        return make_float4(byte_as_float(c, 0x7440u), byte_as_float(c, 0x7441u), byte_as_float(c, 0x7442u),
+                           byte_as_float(c, 0x7443u));
+    }
+};
+template <>
+struct Texel<VV_FMT_DXT1> {
+    static constexpr float kScale = 1.0f / 255.0f;
+    __device__ __forceinline__ static float4 load(const void* pool, uint32_t i) {
+        uint32_t b;
+        int t;
+        dxt_address(i, b, t);
+        const uint2 v = __ldg((const uint2*)pool + b);
+        const uint32_t w[2] = {v.x, v.y};
+        const uint32_t c = dxt::decode_dxt1(w, t);
+        return make_float4(byte_as_float(c, 0x7440u), byte_as_float(c, 0x7441u), byte_as_float(c, 0x7442u), 0.0f);
     }
 };
 
@@ -454,8 +491,9 @@ __device__ __forceinline__ float pow100(float x) {
 // shading (:293-312) with k_Ambient 0.05, k_Diffuse = k_Specular = 1,
 // k_Shininess 100, added to src.rgb when the gradient normalizes (:370-384).
 __device__ __forceinline__ void light_sample(const RaycastParams& p, F3 bpos, F3 dir, F3 light_dir, float4& src) {
-    F3 n = p.grad_fmt == VV_FMT_RGBA8 ? sample_gradient<VV_FMT_RGBA8>(p, bpos)
-                                      : sample_gradient<VV_FMT_FP32>(p, bpos);
+    F3 n = p.grad_fmt == VV_FMT_RGBA8  ? sample_gradient<VV_FMT_RGBA8>(p, bpos)
+           : p.grad_fmt == VV_FMT_DXT1 ? sample_gradient<VV_FMT_DXT1>(p, bpos)
+                                       : sample_gradient<VV_FMT_FP32>(p, bpos);
     if (p.u.gradients_unsigned) n = sub(muls(n, 2.0f), f3(1.0f, 1.0f, 1.0f));  // LookupGradient :318-322
     n = normalize3(n);
     if (isnan(n.x) || isnan(n.y) || isnan(n.z)) return;  // homogeneous region: no lighting

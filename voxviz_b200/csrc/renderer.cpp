@@ -164,11 +164,11 @@ GigaVoxelsRenderer::~GigaVoxelsRenderer() {
 }
 
 int GigaVoxelsRenderer::init() {
-    const size_t tb = texel_bytes(d_.fmt);
-    if (!tb) return VV_ERR_ARG;
-    texel_bytes_ = tb;
+    const size_t bb = brick_bytes(d_.fmt);
+    if (!bb || d_.fmt == VV_FMT_DXT1) return VV_ERR_ARG;
+    brick_bytes_ = bb;
     size_t want;
-    if (d_.pool_bytes > 0) want = (size_t)d_.pool_bytes / (VV_BRICK_TEXELS * tb);
+    if (d_.pool_bytes > 0) want = (size_t)d_.pool_bytes / bb;
     else want = tree_->nonconst_count() + 1;
     if (want < 1) want = 1;
     // BrickPool::init slot grid (GigaVoxelsBrickPool.cpp:75-87)
@@ -540,7 +540,7 @@ int GigaVoxelsRenderer::flush_uploads() {
         return rc;
     }
     if (n) {
-        const size_t bb = VV_BRICK_TEXELS * texel_bytes_;
+        const size_t bb = brick_bytes_;
         const size_t bytes = n * bb;
         if (h_stage_cap_ < bytes) {
             // pinned memory is slow to allocate: grow geometrically, at least 4096 bricks

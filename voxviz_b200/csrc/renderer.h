@@ -100,7 +100,7 @@ private:
     vv_renderer_desc d_;
     int slots_[3] = {0, 0, 0};
     uint32_t total_slots_ = 0;
-    size_t texel_bytes_ = 4;
+    size_t brick_bytes_ = 4000;          // one stored brick in the pool's format
     SlotOrderBuffers order_;
     uint32_t head_ = 0;                  // position of the LRU front in order_.order[order_.cur]
     uint32_t epoch_ = 1;                 // mark of the next partition's touches

@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-from . import TEXEL_BYTES, Octree, fmt_code, look_at, make_camera
+from . import BRICK_BYTES, Octree, fmt_code, look_at, make_camera
 
 RESIDENT = np.uint32(0x80000000)
 CONSTANT = np.uint32(0x40000000)
@@ -64,7 +64,7 @@ def resident_scene(octree: Octree, fmt="rgba8", slots=None):
     ptr = ((px << 20) | (py << 10) | pz).astype(np.uint32)
     words[xyz[:, 2], xyz[:, 1], xyz[:, 0], 0] |= RESIDENT
     words[xyz[:, 2], xyz[:, 1], xyz[:, 0], 1] = ptr
-    pool = np.zeros((sx * sy * sz, 1000 * TEXEL_BYTES[f]), dtype=np.uint8)
+    pool = np.zeros((sx * sy * sz, BRICK_BYTES[f]), dtype=np.uint8)
     if count:
         pool[:count] = octree.produce_bricks(xyz, f)
     return words, pool, (sx, sy, sz), xyz
