@@ -1118,9 +1118,10 @@ def run_batched(args):
 
 
 def run_precision(args):
-    """The 256^3 scene in RGBA8 / FP16 / BF16 / FP32 brick pools, 64 seeded
-    512x512 views: Mrays/s, HBM GB/s and per-pixel error against the FP64
-    oracle (on the same stored bricks, and on the FP32 bricks)."""
+    """The 256^3 scene in RGBA8 / FP16 / BF16 / FP32 brick pools (and the
+    block-compressed DXT5 pool), 64 seeded 512x512 views: Mrays/s, HBM GB/s
+    and per-pixel error against the FP64 oracle (on the same stored bricks,
+    and on the FP32 bricks)."""
     import torch
 
     import voxviz_b200 as vv
@@ -1137,7 +1138,7 @@ def run_precision(args):
     threads = go.cpu_count()
     ref32 = None
     rows = {}
-    order = ["fp32", "rgba8", "fp16", "bf16"]
+    order = ["fp32", "rgba8", "fp16", "bf16", "dxt5"]
     for fmt in order:
         f = vv.fmt_code(fmt)
         words, pool, slots, xyz = scene.resident_scene(octree, f)
@@ -1158,7 +1159,7 @@ def run_precision(args):
             a, _ = ctx.last_times()
             nodes, bricks = ctx.footprint(u)
             ms.append(a)
-            gbs.append((8 * nodes + 1000 * vv.TEXEL_BYTES[f] * bricks + 512 * 512 * 16) / (a / 1e3) / 1e9)
+            gbs.append((8 * nodes + vv.BRICK_BYTES[f] * bricks + 512 * 512 * 16) / (a / 1e3) / 1e9)
             imgs.append(color.cpu().numpy().copy())
         status = ctx.device_status(clear=True)
         sc = go.Scene(words, pool, slots, f, jit)
@@ -1179,7 +1180,7 @@ def run_precision(args):
                      "pixels_over_1_255_vs_fp64": float((px_own > 1.0 / 255.0).mean()),
                      "err_vs_fp64_same_sample_sequence": {"max": float(e_fix.max()),
                                                           "rms": float(np.sqrt((e_fix ** 2).mean()))},
-                     "status": status, "brick_bytes": 1000 * vv.TEXEL_BYTES[f]}
+                     "status": status, "brick_bytes": vv.BRICK_BYTES[f]}
         ctx.close()
     # the lighting path (GigaVoxels.frag with ComputeLighting): RGBA8 bricks,
     # FP32 gradient bricks, against the FP64 oracle's lit shader
