@@ -63,6 +63,8 @@ def parse():
                         "views of 4 terrains in one persistent launch; profile-raycast / profile-adjoint: a few "
                         "frames of the paged terrain (one renderer, a few GB) for ncu captures")
     p.add_argument("--fit-steps", type=int, default=200)
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the config 3/4/5 legs of the default (paged) run")
     p.add_argument("--dump-reference-state", default=None, help=argparse.SUPPRESS)
     return p.parse_args()
 
@@ -611,10 +613,26 @@ def run_ours(args):
         out["parity"], u_chk, words, pool = parity_frame(r, ctx, chk, jit)
         slots = tuple(int(v) // 10 for v in u_chk.brick_pool_dimension)
         out["cpu_baseline"] = cpu_baseline([u_chk] + timed_u[-12:], words, pool, slots, 0, jit, args.cpu_seconds)
-    if rank == 0:
-        print(json.dumps(out), flush=True)
     r.close()
     ctx.close()
+    if world == 1 and not args.no_configs:
+        # configs 3, 4 and 5 of the workload family in the same run: the
+        # brick formats against the FP64 oracle, the batched launch of 64
+        # views of 4 terrains, and the differentiable fit (each summarised;
+        # `--workload precision|batched|fit` prints them in full)
+        sub = argparse.Namespace(**vars(args))
+        sub.emit = False
+        for key, fn in (("config3_precision", run_precision), ("config4_batched", run_batched),
+                        ("config5_fit", run_fit)):
+            t0 = time.perf_counter()
+            try:
+                out[key] = summarise_config(key, fn(sub))
+            except Exception as e:  # a failed leg is reported, the headline stands
+                out[key] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            out[key]["wall_s"] = round(time.perf_counter() - t0, 1)
+            torch.cuda.empty_cache()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     vdist.shutdown()
 
 
@@ -938,12 +956,14 @@ def run_fit(args):
                    else "single GPU"},
         "n_gpus": world, "clocks": clk, "setup_s": round(setup_s, 1),
     }
-    if rank == 0:
+    if rank == 0 and getattr(args, "emit", True):
         print(json.dumps(out), flush=True)
     r.close()
     ctx.close()
     vdist.barrier()
-    vdist.shutdown()
+    if getattr(args, "emit", True):
+        vdist.shutdown()
+    return out
 
 
 BATCH_DEPTHS, BATCH_VIEWS, BATCH_SIDE = (7, 8, 9, 10), 64, (256, 2048)
@@ -1111,10 +1131,12 @@ def run_batched(args):
                               for (p, u_), t in zip(passes, trees)], "data": "synthetic"},
         "setup_s": round(setup_s, 1),
     }
-    print(json.dumps(out), flush=True)
+    if getattr(args, "emit", True):
+        print(json.dumps(out), flush=True)
     for t in trees:
         t["r"].close()
         t["ctx"].close()
+    return out
 
 
 def run_precision(args):
@@ -1222,7 +1244,24 @@ def run_precision(args):
            "config": {"workload": "fBm terrain 256^3 (depth 5), 64 seeded 512x512 views, FP32 compositing",
                       "peak_gbs": peak, "peak_source": peak_kind, "data": "synthetic"},
            "formats": rows, "oracle_threads": threads}
-    print(json.dumps(out), flush=True)
+    if getattr(args, "emit", True):
+        print(json.dumps(out), flush=True)
+    return out
+
+
+def summarise_config(key, d):
+    """The figures of a config run that the headline line carries."""
+    if key == "config3_precision":
+        return {"formats": {f: {k: v[k] for k in ("mrays_s", "hbm_gbs_algorithmic", "frac_of_peak",
+                                                  "err_vs_fp64_same_bricks", "pixels_over_1_255_vs_fp64",
+                                                  "err_vs_fp64_same_sample_sequence") if k in v}
+                            for f, v in d["formats"].items()}, "config": d["config"]}
+    if key == "config4_batched":
+        return {k: d[k] for k in ("value", "unit", "per_view_mrays_s", "ms", "bitexact_vs_per_view",
+                                  "graph_requests_equal_eager", "uploads_per_paged_frame", "autotune", "config")}
+    return {k: d[k] for k in ("value", "unit", "fwd_mrays_s", "plain_raycast_mrays_s", "ms", "adam_steps", "loss",
+                              "grad_check_fd_gpu_fp32", "grad_check_fd_fixed_path_fp64",
+                              "grad_check_fp64_host_adjoint", "status", "config")}
 
 
 def run_profile(args):
