@@ -316,6 +316,9 @@ int vv_backward(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl
  * contributions that found no row.  Row order depends on timing; the map
  * tells which slot each row holds. */
 #define VV_GRAD_F64 1
+/* Lanes of a warp that add to the same texel at once are summed with
+ * __match_any_sync and shuffles first, one atomic per texel and warp. */
+#define VV_GRAD_WARP_SUM 2
 typedef struct vv_grad_desc {
     void* grad;
     int32_t flags;

@@ -110,9 +110,11 @@ __device__ __forceinline__ int grad_row(const GradTarget& gt, uint32_t slot, int
 // texel are summed by shuffles first and the sum goes out in one atomic
 // (coherent rays often sample the same brick cells at once).
 __device__ __forceinline__ void add_texel(const GradTarget& gt, int row, uint32_t t, float4 d) {
-    const uint64_t key = ((uint64_t)(uint32_t)row << 10) | t;
-    const unsigned active = __activemask();
-    const unsigned peers = __match_any_sync(active, key);
+    unsigned peers = 1u << (threadIdx.x & 31);
+    if (gt.warp_sum) {
+        const uint64_t key = ((uint64_t)(uint32_t)row << 10) | t;
+        peers = __match_any_sync(__activemask(), key);
+    }
     const int leader = __ffs(peers) - 1;
     const int lane = threadIdx.x & 31;
     if (__popc(peers) > 1) {

@@ -518,7 +518,7 @@ int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* d
     int rc = diff_params(c, tree, u, p);
     if (rc) return rc;
     if (!ckpt || per_ray <= 0 || !dl_dcolor || !g || !g->grad) return fail(c, VV_ERR_ARG, "bad backward buffers");
-    if ((g->flags & ~VV_GRAD_F64) != 0) return fail(c, VV_ERR_ARG, "unknown gradient flags");
+    if ((g->flags & ~(VV_GRAD_F64 | VV_GRAD_WARP_SUM)) != 0) return fail(c, VV_ERR_ARG, "unknown gradient flags");
     const uintptr_t align = (g->flags & VV_GRAD_F64) ? 32u : 16u;
     if (((uintptr_t)g->grad & (align - 1)) != 0 || ((uintptr_t)dl_dcolor & 15u) != 0)
         return fail(c, VV_ERR_ARG, "gradient buffers must be aligned to a texel (16 bytes, 32 for binary64)");
@@ -528,6 +528,7 @@ int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* d
     GradTarget gt;
     gt.grad = g->grad;
     gt.f64 = (g->flags & VV_GRAD_F64) ? 1 : 0;
+    gt.warp_sum = (g->flags & VV_GRAD_WARP_SUM) ? 1 : 0;
     gt.slot_map = g->slot_map;
     gt.rows_used = g->rows_used;
     gt.rows_cap = g->slot_map ? g->rows_cap : 0;

@@ -71,6 +71,7 @@ cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int
 struct GradTarget {
     void* grad;
     int f64;
+    int warp_sum;  // sum the lanes that add to the same texel before the atomic
     int* slot_map;
     int* rows_used;
     int rows_cap;
