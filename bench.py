@@ -288,8 +288,10 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
     row of 1000 float4 per brick slot the frame touches, claimed by the
     first sample that reaches the slot (vv_backward_ex with a slot map; the
     rows to zero per frame are bounded by the frame's footprint, counted
-    before the timed loop).  Device-timed with CUDA events on the stream both
-    run on; the backward's roofline counts its algorithmic bytes."""
+    before the timed loop); lanes adding to the same texel are summed in the
+    warp first (VV_GRAD_WARP_SUM: coherent rays hit the same cells; the A/B
+    without it is reported).  Device-timed with CUDA events on the stream
+    both run on; the backward's roofline counts its algorithmic bytes."""
     import torch
 
     import voxviz_b200 as vv
@@ -308,11 +310,11 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
     used = torch.zeros(1, dtype=torch.int32, device=dev)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     fwd_ms, bwd_ms, alg_f, alg_b = [], [], [], []
-    ws_ms = []  # the same backward with warp sums before the atomics (A/B)
+    plain_ms = []  # the same backward without warp sums before the atomics (A/B)
     for i in range(reps + 2 + min(reps, 8)):
         k = i % len(us)
         u = us[k]
-        ws = i >= reps + 2
+        ws = i < reps + 2
         ev[0].record()
         ctx.forward_ckpt(u, color.data_ptr(), ck.data_ptr(), per_ray)
         ev[1].record()
@@ -324,8 +326,8 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
                         rows_used=used.data_ptr(), rows_cap=feet[k][1], warp_sum=ws)
         ev[2].record()
         torch.cuda.synchronize()
-        if ws:
-            ws_ms.append(ev[1].elapsed_time(ev[2]))
+        if not ws:
+            plain_ms.append(ev[1].elapsed_time(ev[2]))
         elif i >= 2:
             fwd_ms.append(ev[0].elapsed_time(ev[1]))
             bwd_ms.append(ev[1].elapsed_time(ev[2]))
@@ -345,7 +347,7 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
             "fwd_ms": round(f, 3), "bwd_ms": round(b, 3), "frames": len(us), "reps": reps, "per_ray_ckpts": per_ray,
             "ckpt_bytes": nb, "grad_rows_max": cap, "grad_bytes_max": int(cap * 16000),
             "dense_grad_bytes_avoided": int(n_slots * 16000), "status": status,
-            "bwd_ms_with_warp_sums": round(float(np.mean(ws_ms)), 3) if ws_ms else None,
+            "bwd_ms_without_warp_sums": round(float(np.mean(plain_ms)), 3) if plain_ms else None,
             "roofline": {"forward_ckpt": {"bound": "hbm", "achieved": round(gb_f, 1), "peak": peak, "unit": "GB/s",
                                           "frac": round(gb_f / peak, 4)},
                          "backward": {"bound": "hbm", "achieved": round(gb_b, 1), "peak": peak, "unit": "GB/s",
@@ -901,10 +903,10 @@ def run_fit(args):
     richardson = []
     for q in np.nonzero(~okh)[0]:
         f2 = fd_at(idx[q], h / 2)
-        r = (4.0 * f2 - fdh[q]) / 3.0
-        richardson.append({"fd_h": float(fdh[q]), "fd_h_2": float(f2), "richardson": float(r),
+        rx = (4.0 * f2 - fdh[q]) / 3.0
+        richardson.append({"fd_h": float(fdh[q]), "fd_h_2": float(f2), "richardson": float(rx),
                            "gradient": float(anh[q]), "rel_err_h": float(relh[q]),
-                           "rel_err_richardson": float(abs(r - anh[q]) / max(abs(r), 1e-300)),
+                           "rel_err_richardson": float(abs(rx - anh[q]) / max(abs(rx), 1e-300)),
                            "channel": int(idx[q] % 4)})
     fd_host_report = {"texels": int(len(picks_h)), "h": h, "evaluation": "binary64 along the binary32 sample sequence",
                       "rel_err_median": float(np.median(relh)) if relh.size else None,
