@@ -360,38 +360,40 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
 # 1,040,502 FP16 slots (8000 B each, 102x101x101): near the 102^3 slots 10-bit
 # brick pointers address, enough for the 16 views' bricks to converge
 def raycast_mode_ab(ctx, us, reps=2):
-    """The ray cast of the given frames (on the current pools) launched both
-    ways - one thread per pixel in 16x8 tiles, and persistent warps that
-    refill finished lanes with new pixels - each launch timed with CUDA
-    events (vv_render's profiling events on the context stream); both must
-    give the same colour and usage lists."""
+    """The ray cast of the given frames (on the current pools) launched three
+    ways - one thread per pixel in 16x8 tiles; persistent warps that refill
+    finished lanes with new pixels; the tiles with each warp's shared brick
+    slot staged in shared memory by cp.async.bulk - each launch timed with
+    CUDA events (vv_render's profiling events on the context stream); all
+    must give the same colour and usage lists."""
     import torch
 
     import voxviz_b200 as vv
 
     W, H = us[0].width, us[0].height
     dev = torch.device("cuda", torch.cuda.current_device())
-    col = [torch.empty((H, W, 4), dtype=torch.float32, device=dev) for _ in range(2)]
-    use = [torch.empty((H, W, 12), dtype=torch.int32, device=dev) for _ in range(2)]
+    names = ("tiles", "refill", "staged")
+    col = {n: torch.empty((H, W, 4), dtype=torch.float32, device=dev) for n in names}
+    use = {n: torch.empty((H, W, 12), dtype=torch.int32, device=dev) for n in names}
     ctx.set_profiling(True)
     ms = {}
-    same = True
-    for mode, name in ((False, "tiles"), (True, "refill")):
-        ctx.set_raycast_mode(mode)
+    for name in names:
+        ctx.set_raycast_mode(name)
         t = []
         for rep in range(reps + 1):
             for u in us:
-                ctx.render(u, color=col[int(mode)].data_ptr(), usage=use[int(mode)].data_ptr(),
-                           passes=vv.VV_PASS_RAYCAST)
+                ctx.render(u, color=col[name].data_ptr(), usage=use[name].data_ptr(), passes=vv.VV_PASS_RAYCAST)
                 a, _ = ctx.last_times()
                 if rep:
                     t.append(a)
         ms[name] = float(np.mean(t))
-    ctx.set_raycast_mode(False)
-    same = bool(torch.equal(col[0], col[1]) and torch.equal(use[0], use[1]))
+    ctx.set_raycast_mode("tiles")
+    same = all(bool(torch.equal(col["tiles"], col[n]) and torch.equal(use["tiles"], use[n])) for n in names[1:])
     ctx.set_profiling(False)
     return {"raycast_ms_tiles": round(ms["tiles"], 4), "raycast_ms_refill": round(ms["refill"], 4),
-            "refill_speedup": round(ms["tiles"] / ms["refill"], 3), "frames": len(us), "reps": reps,
+            "raycast_ms_staged": round(ms["staged"], 4),
+            "refill_speedup": round(ms["tiles"] / ms["refill"], 3),
+            "staged_speedup": round(ms["tiles"] / ms["staged"], 3), "frames": len(us), "reps": reps,
             "last_frame_bitexact": same}
 
 

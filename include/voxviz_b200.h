@@ -269,10 +269,15 @@ int vv_ctx_set_profiling(vv_ctx* ctx, int32_t on);
  * 16x8-pixel CTAs.  VV_RAYCAST_REFILL: a persistent grid whose warps take
  * 8x4-pixel tiles from a queue and run their rays one leaf segment at a
  * time, a lane whose ray has ended taking the next pixel (ballot + popc)
- * instead of idling until the warp's last ray ends.  No reference
- * counterpart (one fragment per pixel in GL). */
+ * instead of idling until the warp's last ray ends.  VV_RAYCAST_STAGED
+ * (RGBA8 pools only, else VV_ERR_ARG): the tiles launch, each warp copying
+ * the brick slot that most of its lanes enter together into shared memory
+ * (one cp.async.bulk of 4000 bytes) and those lanes sampling it there.  No
+ * reference counterpart (one fragment per pixel in GL, bricks sampled
+ * through the texture cache). */
 #define VV_RAYCAST_TILES 0
 #define VV_RAYCAST_REFILL 1
+#define VV_RAYCAST_STAGED 2
 int vv_ctx_set_raycast_mode(vv_ctx* ctx, int32_t mode);
 int vv_ctx_last_times(vv_ctx* ctx, float* raycast_ms, float* compact_ms);
 /* Footprint of one draw: the number of distinct node-pool entries and

@@ -103,6 +103,31 @@ def test_miss_only_view_is_empty(cfg1):
     assert got["count"] == 0 and got["requests"].shape[0] == 0
 
 
+@pytest.mark.parametrize("view,size,depth", [(3, (512, 512), 5), (8, (1920, 1080), 5), (6, (333, 177), 6),
+                                             (2, (61, 37), 4)])
+def test_brick_staging_ray_cast_equals_tiles(view, size, depth):
+    """VV_RAYCAST_STAGED (each warp's shared brick slot copied to shared
+    memory by cp.async.bulk) gives the same colour, usage lists, mask and
+    requests as the tiled launch; non-RGBA8 pools refuse the mode."""
+    sc = helpers.Scene(seed=1, depth=depth, fmt="rgba8")
+    g = helpers.GpuScene(sc)
+    u = sc.uniforms(sc.view(view, *size))
+    a = g.render(u)
+    g.ctx.set_raycast_mode("staged")
+    try:
+        b = g.render(u)
+        b2 = g.render(u)
+    finally:
+        g.ctx.set_raycast_mode("tiles")
+    for k in ("color", "usage", "mask", "requests"):
+        assert np.array_equal(a[k], b[k]), k
+        assert np.array_equal(a[k], b2[k]), k
+    assert a["status"] == b["status"] == b2["status"] == 0
+    h = helpers.GpuScene(helpers.Scene(seed=1, depth=4, fmt="fp16"))
+    with pytest.raises(vv.VVError):
+        h.ctx.set_raycast_mode("staged")
+
+
 @pytest.mark.parametrize("fmt,view,size", [("rgba8", 3, (512, 512)), ("fp16", 5, (333, 177)),
                                            ("rgba8", 8, (1920, 1080)), ("fp32", 9, (61, 37)), ("dxt5", 4, (256, 256))])
 def test_lane_refill_ray_cast_equals_tiles(fmt, view, size):

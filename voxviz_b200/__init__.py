@@ -371,11 +371,21 @@ class Context:
         size = int(round(np.sqrt(t.size)))
         self._ck(lib().vv_set_jitter(self._h, _ptr(t), size), "jitter")
 
-    def set_raycast_mode(self, refill: bool) -> None:
-        """vv_ctx_set_raycast_mode: the lane-refill persistent ray cast or the
-        one-thread-per-pixel tiles (same results)."""
-        self._ck(lib().vv_ctx_set_raycast_mode(self._h, N.VV_RAYCAST_REFILL if refill else N.VV_RAYCAST_TILES),
-                 "raycast mode")
+    def set_raycast_mode(self, mode) -> None:
+        """vv_ctx_set_raycast_mode: "tiles" (default, one thread per pixel),
+        "refill" (lane-refill persistent warps) or "staged" (the tiles with
+        each warp's shared brick slot copied to shared memory; RGBA8 pools).
+        All give the same results.  True / False mean "refill" / "tiles"."""
+        modes = {"tiles": N.VV_RAYCAST_TILES, "refill": N.VV_RAYCAST_REFILL, "staged": N.VV_RAYCAST_STAGED}
+        if isinstance(mode, bool):
+            m = N.VV_RAYCAST_REFILL if mode else N.VV_RAYCAST_TILES
+        elif isinstance(mode, str):
+            if mode not in modes:
+                raise ValueError(f"unknown ray-cast mode {mode!r}")
+            m = modes[mode]
+        else:
+            m = int(mode)
+        self._ck(lib().vv_ctx_set_raycast_mode(self._h, m), "raycast mode")
 
     def set_profiling(self, on: bool = True) -> None:
         self._ck(lib().vv_ctx_set_profiling(self._h, 1 if on else 0), "profiling")

@@ -243,7 +243,7 @@ class GradDesc(C.Structure):
 
 
 VV_GRAD_F64, VV_GRAD_WARP_SUM = 1, 2
-VV_RAYCAST_TILES, VV_RAYCAST_REFILL = 0, 1
+VV_RAYCAST_TILES, VV_RAYCAST_REFILL, VV_RAYCAST_STAGED = 0, 1, 2
 
 
 class BatchView(C.Structure):

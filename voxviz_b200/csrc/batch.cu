@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(TW * TH, 896 / (TW * TH))
         const int px = s_tx * TW + wx, py = s_ty * TH + wy;
         if (px < sp.u.width && py < sp.u.height)
             render_pixel<FMT, false, STEPS, true>(sp, px, py,
-                                                  PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], TW * TH});
+                                                  PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], TW * TH, nullptr});
         // every thread is done with s_* before thread 0 takes the next tile
         __syncthreads();
     }

@@ -620,6 +620,8 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         if (c->raycast_mode == VV_RAYCAST_REFILL && !u->compute_lighting) {
             if (!c->d_refill_counter) VV_CUDA(c, cudaMalloc(&c->d_refill_counter, sizeof(unsigned int)));
             VV_CUDA(c, launch_raycast_refill(c->fmt, p, c->d_refill_counter, c->stream));
+        } else if (c->raycast_mode == VV_RAYCAST_STAGED && !u->compute_lighting && c->fmt == VV_FMT_RGBA8) {
+            VV_CUDA(c, launch_raycast_staged(c->fmt, p, c->stream));
         } else {
             VV_CUDA(c, launch_raycast_any(c, p));
         }
@@ -680,8 +682,10 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
 }
 
 int vv_ctx_set_raycast_mode(vv_ctx* c, int32_t mode) {
-    if (!c || (mode != VV_RAYCAST_TILES && mode != VV_RAYCAST_REFILL))
+    if (!c || (mode != VV_RAYCAST_TILES && mode != VV_RAYCAST_REFILL && mode != VV_RAYCAST_STAGED))
         return fail(c, VV_ERR_ARG, "unknown ray-cast mode");
+    if (mode == VV_RAYCAST_STAGED && c->fmt != VV_FMT_RGBA8)
+        return fail(c, VV_ERR_ARG, "brick staging needs an RGBA8 brick pool");
     c->raycast_mode = mode;
     return VV_OK;
 }

@@ -38,7 +38,32 @@ __global__ void __launch_bounds__(128, 7) raycast_kernel(const __grid_constant__
     __shared__ uint2 path_w[kPathLevels][128];
     __shared__ uint32_t path_p[kPathLevels][128];
     render_pixel<FMT, COUNT, 1, !COUNT, LIT>(p, px, py,
-                                             PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
+                                             PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128, nullptr});
+}
+
+// The brick-staging form (RGBA8 pools): the pixels and walk of raycast_kernel,
+// each warp with one slot copy in shared memory (StageBuf).  33 KB of shared
+// memory per CTA allow 6 resident CTAs, hence the register cap of 6.
+__global__ void __launch_bounds__(128, 6) raycast_staged_kernel(const __grid_constant__ RaycastParams p) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ StageBuf stage[4];
+    if (lane == 0) stage_init(&stage[warp]);
+    __syncwarp();
+    const int px = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
+    const int py = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+    if (px >= p.u.width || py >= p.u.height) return;
+    __shared__ uint2 path_w[kPathLevels][128];
+    __shared__ uint32_t path_p[kPathLevels][128];
+    render_pixel<VV_FMT_RGBA8, false, 1, true, false, true>(
+        p, px, py, PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128, &stage[warp]});
+}
+
+cudaError_t launch_raycast_staged(int fmt, const RaycastParams& p, cudaStream_t s) {
+    if (fmt != VV_FMT_RGBA8) return cudaErrorInvalidValue;
+    dim3 block(128);
+    dim3 grid((unsigned)((p.u.width + 15) / 16), (unsigned)((p.u.height + 7) / 8));
+    raycast_staged_kernel<<<grid, block, 0, s>>>(p);
+    return cudaGetLastError();
 }
 
 // The lane-refill form (render_refill): a persistent grid of as many CTAs
@@ -49,7 +74,7 @@ __global__ void __launch_bounds__(128, 7) raycast_refill_kernel(const __grid_con
                                                                 unsigned int* counter) {
     __shared__ uint2 path_w[kPathLevels][128];
     __shared__ uint32_t path_p[kPathLevels][128];
-    render_refill<FMT>(p, counter, PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
+    render_refill<FMT>(p, counter, PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128, nullptr});
 }
 
 cudaError_t launch_raycast_refill(int fmt, const RaycastParams& p, unsigned int* counter, cudaStream_t s) {

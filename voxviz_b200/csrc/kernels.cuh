@@ -61,6 +61,7 @@ struct CompactParams {
 cudaError_t launch_raycast(int fmt, const RaycastParams& p, cudaStream_t s);
 // The persistent lane-refill ray cast (same results; plain unlit draws only).
 cudaError_t launch_raycast_refill(int fmt, const RaycastParams& p, unsigned int* counter, cudaStream_t s);
+cudaError_t launch_raycast_staged(int fmt, const RaycastParams& p, cudaStream_t s);
 // Differentiable forward (colour + per-ray checkpoints) and its adjoint.
 size_t ckpt_bytes(int w, int h, int per_ray);
 cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int per_ray, cudaStream_t s);

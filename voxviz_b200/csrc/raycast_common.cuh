@@ -69,11 +69,13 @@ __device__ __forceinline__ float byte_as_float(uint32_t v, uint32_t sel) {
 template <>
 struct Texel<VV_FMT_RGBA8> {
     static constexpr float kScale = 1.0f / 255.0f;
-    __device__ __forceinline__ static float4 load(const void* pool, uint32_t i) {
-        const uint32_t v = __ldg((const uint32_t*)pool + i);
+    __device__ __forceinline__ static float4 unpack(uint32_t v) {
         // selectors: result bytes (low to high) = byte k of v, 0, 0, 0x4B
         return make_float4(byte_as_float(v, 0x7440u), byte_as_float(v, 0x7441u), byte_as_float(v, 0x7442u),
                            byte_as_float(v, 0x7443u));
+    }
+    __device__ __forceinline__ static float4 load(const void* pool, uint32_t i) {
+        return unpack(__ldg((const uint32_t*)pool + i));
     }
 };
 template <>
@@ -215,10 +217,12 @@ __device__ __forceinline__ float4 sample_brick(const RaycastParams& p, F3 uvw) {
 // sample_brick, only the texel addressing is shorter) or, when the slot's
 // cell mask `cmask` (or nullptr) marks the taps' cell all zero, kEmptyCell
 // (out = 0, exactly what the taps give); kOutside (and nothing) otherwise.
+// With STAGED and `stex` (the slot's RGBA8 texels in shared memory) the taps
+// are read from there.
 enum { kOutside = 0, kInSlot = 1, kEmptyCell = 2 };
-template <int FMT>
+template <int FMT, bool STAGED = false>
 __device__ __forceinline__ int sample_in_slot(const RaycastParams& p, F3 uvw, const int base[3], uint32_t slot_texel0,
-                                              const uint32_t* cmask, float4& out) {
+                                              const uint32_t* cmask, float4& out, const uint32_t* stex = nullptr) {
     const float* N = p.u.brick_pool_dimension;
     const float ta[3] = {uvw.x * N[0] - 0.5f, uvw.y * N[1] - 0.5f, uvw.z * N[2] - 0.5f};
     // the first tap per axis, floor(t) as an integer in one conversion (the
@@ -237,12 +241,31 @@ __device__ __forceinline__ int sample_in_slot(const RaycastParams& p, F3 uvw, co
     float f[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) f[a] = ta[a] - floorf(ta[a]);
-    const uint32_t i000 = slot_texel0 + (uint32_t)((l[2] * 10 + l[1]) * 10 + l[0]);
+    const uint32_t l000 = (uint32_t)((l[2] * 10 + l[1]) * 10 + l[0]);
+    const uint32_t i000 = slot_texel0 + l000;
     const void* pool = p.bricks;
-    const float4 v000 = Texel<FMT>::load(pool, i000), v100 = Texel<FMT>::load(pool, i000 + 1u);
-    const float4 v010 = Texel<FMT>::load(pool, i000 + 10u), v110 = Texel<FMT>::load(pool, i000 + 11u);
-    const float4 v001 = Texel<FMT>::load(pool, i000 + 100u), v101 = Texel<FMT>::load(pool, i000 + 101u);
-    const float4 v011 = Texel<FMT>::load(pool, i000 + 110u), v111 = Texel<FMT>::load(pool, i000 + 111u);
+    float4 v000, v100, v010, v110, v001, v101, v011, v111;
+    if (STAGED && stex) {
+        static_assert(!STAGED || FMT == VV_FMT_RGBA8, "staging holds RGBA8 slots");
+        const uint32_t* t = stex + l000;
+        v000 = Texel<VV_FMT_RGBA8>::unpack(t[0]);
+        v100 = Texel<VV_FMT_RGBA8>::unpack(t[1]);
+        v010 = Texel<VV_FMT_RGBA8>::unpack(t[10]);
+        v110 = Texel<VV_FMT_RGBA8>::unpack(t[11]);
+        v001 = Texel<VV_FMT_RGBA8>::unpack(t[100]);
+        v101 = Texel<VV_FMT_RGBA8>::unpack(t[101]);
+        v011 = Texel<VV_FMT_RGBA8>::unpack(t[110]);
+        v111 = Texel<VV_FMT_RGBA8>::unpack(t[111]);
+    } else {
+        v000 = Texel<FMT>::load(pool, i000);
+        v100 = Texel<FMT>::load(pool, i000 + 1u);
+        v010 = Texel<FMT>::load(pool, i000 + 10u);
+        v110 = Texel<FMT>::load(pool, i000 + 11u);
+        v001 = Texel<FMT>::load(pool, i000 + 100u);
+        v101 = Texel<FMT>::load(pool, i000 + 101u);
+        v011 = Texel<FMT>::load(pool, i000 + 110u);
+        v111 = Texel<FMT>::load(pool, i000 + 111u);
+    }
     const float4 c0 = lerp4(lerp4(v000, v100, f[0]), lerp4(v010, v110, f[0]), f[1]);
     const float4 c1 = lerp4(lerp4(v001, v101, f[0]), lerp4(v011, v111, f[0]), f[1]);
     float4 c = lerp4(c0, c1, f[2]);
@@ -442,11 +465,124 @@ __device__ __forceinline__ bool ray_start(const RaycastParams& p, const WalkCons
 // it skips would take exactly the recorded path (same nodes, same words,
 // every stop condition false), so the walk is unchanged.
 constexpr int kPathLevels = 11;  // levels 0..10
+struct StageBuf;
 struct PathSlots {
     uint2* w;
     uint32_t* p;
     int stride;
+    StageBuf* stage;  // the warp's staged brick (VV_RAYCAST_STAGED), else nullptr
 };
+
+// ---- brick staging (VV_RAYCAST_STAGED, RGBA8 pools) ------------------------
+//
+// Each warp owns one 10^3-texel RGBA8 slot copy in shared memory.  When the
+// lanes that reach a brick segment together share a slot (__match_any_sync),
+// the largest such group copies that slot's 4000 bytes with one
+// cp.async.bulk (global -> this CTA's shared memory, no multicast) and
+// samples it from shared memory; other lanes read the pool as usual.
+//   state = tag << 32 | mask: tag = the slot the buffer holds (kNoSlot while
+//   a copy is in flight), mask = the lanes reading it.  A group joins a
+//   buffer that holds its slot, or refills an unread one; both by one
+//   atomicCAS of its leader, so a copy never overwrites texels being read.
+// The only wait is the copy's own mbarrier (bounded: on timeout the status
+// is set, the buffer stays claimed and the lanes read the pool).
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+constexpr int kStageMinLanes = 4;  // smallest group worth a copy
+struct __align__(16) StageBuf {
+    uint32_t texels[1000];
+    unsigned long long state;
+    unsigned long long bar;
+    uint32_t phase;  // completed copies (the mbarrier's phase parity)
+};
+
+// Lane 0 of the warp, before any lane returns.
+__device__ __forceinline__ void stage_init(StageBuf* sb) {
+    sb->state = (unsigned long long)kNoSlot << 32;
+    sb->phase = 0u;
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&sb->bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Called by the converged lanes entering a brick segment; `slot` is the
+// lane's slot or kNoSlot.  True: the lane reads its slot from sb->texels
+// until stage_release.
+__device__ __forceinline__ bool stage_acquire(StageBuf* sb, const void* pool, uint32_t slot, int* status) {
+    const unsigned am = __activemask();
+    const unsigned peers = __match_any_sync(am, slot);
+    const int lane = (int)(threadIdx.x & 31u);
+    const int leader = __ffs(peers) - 1;
+    // 1: joined a buffer holding the slot, 2: claimed it for a copy
+    int act = 0;
+    if (lane == leader && slot != kNoSlot) {
+        unsigned long long st = *(volatile unsigned long long*)&sb->state;
+        for (int tries = 0; tries < 4; ++tries) {
+            unsigned long long want;
+            int a;
+            if ((uint32_t)(st >> 32) == slot) {
+                want = st | peers;
+                a = 1;
+            } else if ((uint32_t)st == 0u && __popc(peers) >= kStageMinLanes) {
+                want = ((unsigned long long)kNoSlot << 32) | peers;
+                a = 2;
+            } else {
+                break;
+            }
+            const unsigned long long old = atomicCAS(&sb->state, st, want);
+            if (old == st) {
+                act = a;
+                break;
+            }
+            st = old;
+        }
+        __threadfence_block();
+    }
+    act = __shfl_sync(peers, act, leader);
+    if (act == 2) {
+        const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&sb->bar);
+        const uint32_t parity = sb->phase & 1u;
+        if (lane == leader) {
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sb->texels);
+            const uint32_t* src = (const uint32_t*)pool + (size_t)slot * 1000u;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 4000;" ::"r"(bar) : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 4000, [%2];" ::"r"(dst),
+                "l"(src), "r"(bar)
+                : "memory");
+        }
+        uint32_t done = 0u;
+        for (int i = 0; i < (1 << 20) && !done; ++i) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(bar), "r"(parity)
+                : "memory");
+        }
+        done = __all_sync(peers, done != 0u);
+        if (!done) {
+            set_status(status, VV_ERR_TIMEOUT);
+            return false;
+        }
+        __syncwarp(peers);
+        if (lane == leader) {
+            sb->phase = sb->phase + 1u;
+            __threadfence_block();
+            atomicExch(&sb->state, ((unsigned long long)slot << 32) | peers);
+        }
+        __syncwarp(peers);
+        return true;
+    }
+    return act == 1;
+}
+
+// The lane stops reading the staged slot.
+__device__ __forceinline__ void stage_release(StageBuf* sb) {
+    __threadfence_block();
+    atomicAnd(&sb->state, ~(1ull << (threadIdx.x & 31u)));
+}
 
 // ---- lighting (GigaVoxels.frag with ComputeLighting) ----------------------
 
@@ -522,7 +658,7 @@ struct WalkResume {
 
 // One leaf segment of the walk (a descent and its march); false when the
 // walk has ended.  walk() runs it until then.
-template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false, bool LIT = false>
+template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false, bool LIT = false, bool STAGED = false>
 __device__ __forceinline__ bool walk_segment(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis,
                                              PathSlots path, WalkResume& wr) {
     bool ok = true;
@@ -695,7 +831,7 @@ __device__ __forceinline__ bool walk_segment(const RaycastParams& p, const WalkC
             // taps inside this brick's slot skip the general texel addressing
             int base[3] = {(int)((cur_bw >> 20) & 0x3FFu) - 1, (int)((cur_bw >> 10) & 0x3FFu) - 1,
                            (int)(cur_bw & 0x3FFu) - 1};
-            uint32_t slot_texel0 = 0u;
+            uint32_t slot_texel0 = 0u, slot_id = kNoSlot;
             const uint32_t* cmask = nullptr;  // the slot's empty-cell mask (not in footprint counts)
             if (base[0] >= 0 && base[1] >= 0 && base[2] >= 0 && base[0] % 10 == 0 && base[1] % 10 == 0 &&
                 base[2] % 10 == 0 && base[0] < p.slots[0] * 10 && base[1] < p.slots[1] * 10 &&
@@ -703,10 +839,13 @@ __device__ __forceinline__ bool walk_segment(const RaycastParams& p, const WalkC
                 const uint32_t slot = ((uint32_t)base[2] / 10u * (uint32_t)p.slots[1] + (uint32_t)base[1] / 10u) *
                                           (uint32_t)p.slots[0] + (uint32_t)base[0] / 10u;
                 slot_texel0 = slot * 1000u;
+                slot_id = slot;
                 if (!COUNT && p.cell_mask) cmask = p.cell_mask + (size_t)slot * kCellMaskWords;
             } else {
                 base[0] = base[1] = base[2] = -100000;
             }
+            const bool staged = STAGED && stage_acquire(path.stage, p.bricks, slot_id, p.status);
+            const uint32_t* stex = staged ? path.stage->texels : nullptr;
 #pragma unroll(STEPS)
             for (int i = 0; i < n; ++i) {
                 s.pos = add(s.pos, wstep);
@@ -716,7 +855,7 @@ __device__ __forceinline__ bool walk_segment(const RaycastParams& p, const WalkC
                     break;
                 }
                 float4 src;
-                const int in = COUNT ? kOutside : sample_in_slot<FMT>(p, bpos, base, slot_texel0, cmask, src);
+                const int in = COUNT ? kOutside : sample_in_slot<FMT, STAGED>(p, bpos, base, slot_texel0, cmask, src, stex);
                 if (in == kOutside) src = sample_brick<FMT, COUNT>(p, bpos);
                 src.w = 1.0f - (1.0f - src.w);
                 // shading adds rgb times finite factors: nothing to a zero sample
@@ -728,9 +867,13 @@ __device__ __forceinline__ bool walk_segment(const RaycastParams& p, const WalkC
                     s.dst = make_float4(T * src.x + s.dst.x, T * src.y + s.dst.y, T * src.z + s.dst.z,
                                         T * src.w + s.dst.w);
                 ++s.nsamples;
-                if (!go) return false;
+                if (!go) {
+                    if (staged) stage_release(path.stage);
+                    return false;
+                }
                 bpos = add(bpos, s.brick_step);
             }
+            if (staged) stage_release(path.stage);
         }
         vis.segment_end(s, is_const, loaded);
         if (s.dst.w > k.astop && (is_const || loaded)) return false;
@@ -739,11 +882,11 @@ __device__ __forceinline__ bool walk_segment(const RaycastParams& p, const WalkC
     }
 }
 
-template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false, bool LIT = false>
+template <int FMT, bool COUNT, class V, int STEPS = 1, bool RESUME = false, bool LIT = false, bool STAGED = false>
 __device__ __forceinline__ void walk(const RaycastParams& p, const WalkConsts& k, RayState& s, V& vis,
-                                     PathSlots path = PathSlots{nullptr, nullptr, 0}) {
+                                     PathSlots path = PathSlots{nullptr, nullptr, 0, nullptr}) {
     WalkResume wr;
-    while (walk_segment<FMT, COUNT, V, STEPS, RESUME, LIT>(p, k, s, vis, path, wr)) {
+    while (walk_segment<FMT, COUNT, V, STEPS, RESUME, LIT, STAGED>(p, k, s, vis, path, wr)) {
     }
 }
 
@@ -804,14 +947,15 @@ __device__ __forceinline__ void finish_pixel(const RaycastParams& p, size_t pix,
 
 // One pixel of the forward draw: the fragment's ray walk, FragColor and the
 // three RGBA32UI usage-list layers (:490-751).
-template <int FMT, bool COUNT, int STEPS, bool RESUME = false, bool LIT = false>
+template <int FMT, bool COUNT, int STEPS, bool RESUME = false, bool LIT = false, bool STAGED = false>
 __device__ __forceinline__ void render_pixel(const RaycastParams& p, int px, int py,
-                                             PathSlots path = PathSlots{nullptr, nullptr, 0}) {
+                                             PathSlots path = PathSlots{nullptr, nullptr, 0, nullptr}) {
     bool ok = true;
     const WalkConsts k = walk_consts(p, fetch_node<COUNT>(p, 0, 0, 0, ok));
     UsageVisitor vis;
     RayState s;
-    if (start_pixel(p, k, px, py, s, vis)) walk<FMT, COUNT, UsageVisitor, STEPS, RESUME, LIT>(p, k, s, vis, path);
+    if (start_pixel(p, k, px, py, s, vis))
+        walk<FMT, COUNT, UsageVisitor, STEPS, RESUME, LIT, STAGED>(p, k, s, vis, path);
     finish_pixel(p, (size_t)py * p.u.width + px, s);
 }
 
