@@ -282,16 +282,25 @@ def parity_frame(r, ctx, cam, jitter):
     return out, u, words, pool
 
 
+# the adjoint's atomics: the timed form and the A/B forms (vv_backward_ex flags)
+BWD_MAIN = {"spread": True, "warp_sum": False}
+BWD_AB = {"warp_sums": {"spread": False, "warp_sum": True}, "plain": {"spread": False, "warp_sum": False},
+          "spread_and_warp_sums": {"spread": True, "warp_sum": True}}
+
+
 def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
     """Checkpointing forward + adjoint of the L2 loss sum(colour^2) over the
     given frames on the current pools.  The texel gradient is sparse: one
     row of 1000 float4 per brick slot the frame touches, claimed by the
     first sample that reaches the slot (vv_backward_ex with a slot map; the
     rows to zero per frame are bounded by the frame's footprint, counted
-    before the timed loop); lanes adding to the same texel are summed in the
-    warp first (VV_GRAD_WARP_SUM: coherent rays hit the same cells; the A/B
-    without it is reported).  Device-timed with CUDA events on the stream
-    both run on; the backward's roofline counts its algorithmic bytes."""
+    before the timed loop).  The timed form spreads the atomics over two
+    copies of the rows (VV_GRAD_SPREAD: fewer concurrent atomics on one
+    address; the copies are added on the stream, inside the timing); the
+    A/B forms (warp sums of the lanes in one cell, VV_GRAD_WARP_SUM; plain
+    atomics; both) are timed on the same frames.  Device-timed with CUDA
+    events on the stream both run on; the backward's roofline counts its
+    algorithmic bytes."""
     import torch
 
     import voxviz_b200 as vv
@@ -310,11 +319,22 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
     used = torch.zeros(1, dtype=torch.int32, device=dev)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     fwd_ms, bwd_ms, alg_f, alg_b = [], [], [], []
-    plain_ms = []  # the same backward without warp sums before the atomics (A/B)
-    for i in range(reps + 2 + min(reps, 8)):
+    ab_ms = {name: [] for name in BWD_AB}
+    n_ab = min(reps, 8)
+    # size the context's copies of the rows for the largest frame (untimed)
+    kmax = int(np.argmax([b for _, b in feet]))
+    ctx.forward_ckpt(us[kmax], color.data_ptr(), ck.data_ptr(), per_ray)
+    smap.fill_(-1)
+    used.zero_()
+    rows.zero_()
+    ctx.backward_ex(us[kmax], color.data_ptr(), ck.data_ptr(), per_ray, rows.data_ptr(), slot_map=smap.data_ptr(),
+                    rows_used=used.data_ptr(), rows_cap=cap, spread=True)
+    torch.cuda.synchronize()
+    runs = [(None, i) for i in range(reps + 2)] + [(name, i) for name in BWD_AB for i in range(n_ab + 1)]
+    for mode, i in runs:
         k = i % len(us)
         u = us[k]
-        ws = i < reps + 2
+        flags = BWD_MAIN if mode is None else BWD_AB[mode]
         ev[0].record()
         ctx.forward_ckpt(u, color.data_ptr(), ck.data_ptr(), per_ray)
         ev[1].record()
@@ -323,11 +343,12 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
         used.zero_()
         rows[: feet[k][1]].zero_()
         ctx.backward_ex(u, dl.data_ptr(), ck.data_ptr(), per_ray, rows.data_ptr(), slot_map=smap.data_ptr(),
-                        rows_used=used.data_ptr(), rows_cap=feet[k][1], warp_sum=ws)
+                        rows_used=used.data_ptr(), rows_cap=feet[k][1], **flags)
         ev[2].record()
         torch.cuda.synchronize()
-        if not ws:
-            plain_ms.append(ev[1].elapsed_time(ev[2]))
+        if mode is not None:
+            if i >= 1:
+                ab_ms[mode].append(ev[1].elapsed_time(ev[2]))
         elif i >= 2:
             fwd_ms.append(ev[0].elapsed_time(ev[1]))
             bwd_ms.append(ev[1].elapsed_time(ev[2]))
@@ -347,7 +368,8 @@ def fwd_bwd_leg(ctx, us, reps, peak, per_ray=16):
             "fwd_ms": round(f, 3), "bwd_ms": round(b, 3), "frames": len(us), "reps": reps, "per_ray_ckpts": per_ray,
             "ckpt_bytes": nb, "grad_rows_max": cap, "grad_bytes_max": int(cap * 16000),
             "dense_grad_bytes_avoided": int(n_slots * 16000), "status": status,
-            "bwd_ms_without_warp_sums": round(float(np.mean(plain_ms)), 3) if plain_ms else None,
+            "bwd_form": BWD_MAIN,
+            "bwd_ms_ab": {name: round(float(np.mean(v)), 3) for name, v in ab_ms.items() if v},
             "roofline": {"forward_ckpt": {"bound": "hbm", "achieved": round(gb_f, 1), "peak": peak, "unit": "GB/s",
                                           "frac": round(gb_f / peak, 4)},
                          "backward": {"bound": "hbm", "achieved": round(gb_b, 1), "peak": peak, "unit": "GB/s",
@@ -565,14 +587,18 @@ def run_ours(args):
                                                  "W*H*(16 colour + 48 usage); mean over 8 of the timed frames"},
                 "traffic_source": prof.get("source") if prof else None}
     if prof:
-        # the bound the kernel actually meets: instruction issue
+        # the bound the kernel actually meets: instruction issue, from the
+        # captured launch's own instruction count and duration (its frame
+        # is not one of the timed frames, so the timed mean is not used)
+        n_inst, dur = prof.get("warp_instructions_per_launch"), prof.get("duration_ms_under_ncu")
         roofline["issue"] = {"issue_slots_busy_frac": prof.get("issue_slots_busy_frac"),
-                             "warp_instructions_per_launch": prof.get("warp_instructions_per_launch"),
-                             "achieved_ginst_s": round(prof["warp_instructions_per_launch"] / (ray_mean / 1e3) / 1e9,
-                                                       1) if prof.get("warp_instructions_per_launch") else None,
+                             "warp_instructions_per_launch": n_inst,
+                             "captured_launch_ms": dur,
+                             "achieved_ginst_s": round(n_inst / (dur / 1e3) / 1e9, 1) if n_inst and dur else None,
                              "peak_ginst_s": round(148 * 4 * (clk.get("sm_mhz") or 1965.0) / 1e3, 1),
-                             "note": "peak = 148 SMs x 4 schedulers x 1 warp instruction per clock at the "
-                                     "median SM clock of the timed region"}
+                             "note": "one ncu-captured launch (profiles/raycast_paged_1080p.md); peak = 148 SMs x 4 "
+                                     "schedulers x 1 warp instruction per clock at the median SM clock of the timed "
+                                     "region"}
         if roofline["issue"]["achieved_ginst_s"]:
             roofline["issue"]["frac"] = round(roofline["issue"]["achieved_ginst_s"] /
                                               roofline["issue"]["peak_ginst_s"], 4)

@@ -321,9 +321,19 @@ int vv_backward(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl
  * contributions that found no row.  Row order depends on timing; the map
  * tells which slot each row holds. */
 #define VV_GRAD_F64 1
-/* Lanes of a warp that add to the same texel at once are summed with
- * __match_any_sync and shuffles first, one atomic per texel and warp. */
+/* Lanes of a warp whose samples lie in the same brick cell (the same 8
+ * texels) are summed with __match_any_sync and shuffles first, one atomic
+ * per texel and cell group. */
 #define VV_GRAD_WARP_SUM 2
+/* Spread the atomics of a sparse binary32 gradient (needs a slot map; not
+ * with VV_GRAD_F64, else VV_ERR_ARG) over VV_GRAD_SPREAD_COPIES copies of
+ * the rows: the warps of a CTA add to different copies (fewer concurrent
+ * atomics on one address), the extra copies live in context memory
+ * ((copies - 1) * rows_cap * 16000 bytes, kept between calls) and are added
+ * into `grad` on the stream after the adjoint.  Same gradient up to the
+ * order of the float additions. */
+#define VV_GRAD_SPREAD 4
+#define VV_GRAD_SPREAD_COPIES 4
 typedef struct vv_grad_desc {
     void* grad;
     int32_t flags;

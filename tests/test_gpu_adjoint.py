@@ -84,10 +84,11 @@ def test_backward_matches_fp64_oracle(fp32_scene, per_ray):
 
 
 def _backward_variants(g, u, ck, per_ray, dl_t, n_slots):
-    """The adjoint of one view four ways: dense float, dense binary64, and
-    sparse rows (slot map) in float and in binary64; the sparse ones are
-    scattered back to slots.  Returns {name: (slots, 1000, 4) float64} and
-    the rows each sparse call claimed."""
+    """The adjoint of one view several ways: dense float, dense binary64,
+    and sparse rows (slot map) in float and in binary64, in float with cell
+    warp sums, with the atomics spread over copies of the rows, and with
+    both; the sparse ones are scattered back to slots.  Returns {name:
+    (slots, 1000, 4) float64} and the rows each sparse call claimed."""
     dev = torch.device("cuda", 0)
     out, rows = {}, {}
     dense = torch.zeros((n_slots, 1000, 4), dtype=torch.float32, device=dev)
@@ -96,13 +97,15 @@ def _backward_variants(g, u, ck, per_ray, dl_t, n_slots):
     d64 = torch.zeros((n_slots, 1000, 4), dtype=torch.float64, device=dev)
     g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), per_ray, d64.data_ptr(), f64=True)
     out["dense_f64"] = d64
-    for f64 in (False, True):
+    forms = {"rows_f32": {}, "rows_f64": {"f64": True}, "rows_f32_warp_sum": {"warp_sum": True},
+             "rows_f32_spread": {"spread": True}, "rows_f32_spread_warp_sum": {"spread": True, "warp_sum": True}}
+    for name, kw in forms.items():
         cap = n_slots
-        rowbuf = torch.zeros((cap, 1000, 4), dtype=torch.float64 if f64 else torch.float32, device=dev)
+        rowbuf = torch.zeros((cap, 1000, 4), dtype=torch.float64 if kw.get("f64") else torch.float32, device=dev)
         smap = torch.full((n_slots,), -1, dtype=torch.int32, device=dev)
         used = torch.zeros(1, dtype=torch.int32, device=dev)
-        g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), per_ray, rowbuf.data_ptr(), f64=f64,
-                          slot_map=smap.data_ptr(), rows_used=used.data_ptr(), rows_cap=cap)
+        g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), per_ray, rowbuf.data_ptr(),
+                          slot_map=smap.data_ptr(), rows_used=used.data_ptr(), rows_cap=cap, **kw)
         torch.cuda.synchronize()
         n = int(used.item())
         m = smap.cpu().numpy()
@@ -110,8 +113,8 @@ def _backward_variants(g, u, ck, per_ray, dl_t, n_slots):
         full = torch.zeros((n_slots, 1000, 4), dtype=torch.float64, device=dev)
         sl = torch.from_numpy(np.nonzero(m >= 0)[0]).to(dev)
         full[sl] = rowbuf[smap[sl].long()].double()
-        out["rows_f64" if f64 else "rows_f32"] = full
-        rows["rows_f64" if f64 else "rows_f32"] = n
+        out[name] = full
+        rows[name] = n
     torch.cuda.synchronize()
     return {k: v.cpu().numpy() for k, v in out.items()}, rows
 
@@ -152,6 +155,55 @@ def test_backward_binary64_and_sparse_rows(fp32_scene):
         # where the terms do not cancel (magnitude within 10x of the sum) the
         # plain relative error is far below 1e-3
         assert (err / np.abs(ref)[nz])[cond <= 10].max() <= 1e-4
+
+
+def test_spread_copies_stay_zero_between_calls(fp32_scene):
+    """VV_GRAD_SPREAD: the context's extra copies of the rows are added
+    into the caller's rows and left zero, so repeated calls - with other row
+    capacities, after an overflow, and after a call without spreading - give
+    the same gradient as plain atomics; it needs a slot map and binary32
+    rows."""
+    sc, g = fp32_scene
+    u = sc.uniforms(sc.view(8, 160, 120))
+    _, ck = _ckpt_color(g, u, 16)
+    rng = np.random.default_rng(3)
+    dl_t = torch.from_numpy(rng.standard_normal((120, 160, 4)).astype(np.float32)).cuda()
+    n_slots = int(np.prod(sc.slots))
+    dev = torch.device("cuda", 0)
+
+    def run(cap, **kw):
+        rowbuf = torch.zeros((cap, 1000, 4), dtype=torch.float32, device=dev)
+        smap = torch.full((n_slots,), -1, dtype=torch.int32, device=dev)
+        used = torch.zeros(1, dtype=torch.int32, device=dev)
+        g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), 16, rowbuf.data_ptr(), slot_map=smap.data_ptr(),
+                          rows_used=used.data_ptr(), rows_cap=cap, **kw)
+        torch.cuda.synchronize()
+        m = smap.cpu().numpy()
+        full = np.zeros((n_slots, 1000, 4), dtype=np.float64)
+        sl = np.nonzero(m >= 0)[0]
+        full[sl] = rowbuf.cpu().numpy()[m[sl]]
+        return full
+
+    ref = run(n_slots)
+    scale = np.abs(ref).max()
+    touched = int((np.abs(ref).reshape(n_slots, -1).max(axis=1) > 0).sum())
+    for cap in (n_slots, touched + 3, n_slots // 2 + touched, touched):
+        got = run(cap, spread=True)
+        assert g.ctx.device_status() == 0
+        assert np.array_equal(got != 0, ref != 0)
+        assert np.abs(got - ref).max() <= 1e-5 * scale
+    # an overflowing call drops contributions but leaves the copies clean
+    run(2, spread=True)
+    from voxviz_b200 import _native as N
+    assert g.ctx.device_status(clear=True) == N.VV_ERR_OOM
+    got = run(n_slots, spread=True, warp_sum=True)
+    assert g.ctx.device_status() == 0
+    assert np.abs(got - ref).max() <= 1e-5 * scale
+    with pytest.raises(vv.VVError):
+        run(n_slots, spread=True, f64=True)
+    with pytest.raises(vv.VVError):
+        g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), 16,
+                          torch.zeros((n_slots, 1000, 4), device=dev).data_ptr(), spread=True)
 
 
 def test_sparse_rows_report_overflow(fp32_scene):

@@ -53,19 +53,25 @@ struct CkptVisitor {
     __device__ __forceinline__ void fail(int code) { set_status(status, code); }
 };
 
+// The samples of one piece, compactly: T (the transmittance before the
+// sample, negated for a constant-node sample: T > 0 or +0 for brick samples),
+// the sample's alpha, r = dot(dL/dc.rgb, src.rgb) (dL/dc.rgb is constant
+// along the ray) and the brick position.  24 bytes a sample.
 struct ReplayVisitor {
     int first, last, n;
-    float4 src[kPiece];
+    float gx, gy, gz;  // dL/dc.rgb
     float T[kPiece];
+    float a[kPiece];
+    float r[kPiece];
     F3 bpos[kPiece];
-    bool brick[kPiece];
     __device__ __forceinline__ bool segment_begin(const RayState& s) { return s.nsamples < last; }
     __device__ __forceinline__ bool sample(int kind, const float4& v, F3 b, float t, int index) {
         if (index >= first && n < kPiece) {
-            src[n] = v;
-            T[n] = t;
+            T[n] = kind == kSampleBrick ? t : -t;
+            a[n] = v.w;
+            // the first three products of the g.a update, in its order
+            r[n] = gx * v.x + gy * v.y + gz * v.z;
             bpos[n] = b;
-            brick[n] = kind == kSampleBrick;
             ++n;
         }
         return index + 1 < last;
@@ -106,51 +112,97 @@ __device__ __forceinline__ int grad_row(const GradTarget& gt, uint32_t slot, int
     return -1;
 }
 
-// gradient += d at texel `i` of row `row`: lanes of a warp adding to the same
-// texel are summed by shuffles first and the sum goes out in one atomic
-// (coherent rays often sample the same brick cells at once).
-__device__ __forceinline__ void add_texel(const GradTarget& gt, int row, uint32_t t, float4 d) {
-    unsigned peers = 1u << (threadIdx.x & 31);
-    if (gt.warp_sum) {
-        const uint64_t key = ((uint64_t)(uint32_t)row << 10) | t;
-        peers = __match_any_sync(__activemask(), key);
-    }
-    const int leader = __ffs(peers) - 1;
-    const int lane = threadIdx.x & 31;
-    if (__popc(peers) > 1) {
-        // sum over the peers in lane order (a fixed order for a fixed set)
-        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (unsigned m = peers; m; m &= m - 1) {
-            const int src = __ffs(m) - 1;
-            s.x += __shfl_sync(peers, d.x, src);
-            s.y += __shfl_sync(peers, d.y, src);
-            s.z += __shfl_sync(peers, d.z, src);
-            s.w += __shfl_sync(peers, d.w, src);
-        }
-        d = s;
-    }
-    if (lane != leader) return;
-    const size_t i = (size_t)row * 1000u + t;
-    if (gt.f64) {
+// gradient element i += v (binary32 rows: one vector reduction, red.v4.f32,
+// which returns nothing - atomicAdd(float4*) returns the old value and so
+// holds four registers until the L2 answers - into the warp's copy of the
+// rows; binary64 rows: four double atomics).
+template <bool F64>
+__device__ __forceinline__ void texel_atomic(const GradTarget& gt, size_t i, float4 v) {
+    if (F64) {
         double* g = (double*)gt.grad + 4 * i;
-        atomicAdd(g + 0, (double)d.x);
-        atomicAdd(g + 1, (double)d.y);
-        atomicAdd(g + 2, (double)d.z);
-        atomicAdd(g + 3, (double)d.w);
+        atomicAdd(g + 0, (double)v.x);
+        atomicAdd(g + 1, (double)v.y);
+        atomicAdd(g + 2, (double)v.z);
+        atomicAdd(g + 3, (double)v.w);
     } else {
-        atomicAdd((float4*)gt.grad + i, d);
+        float4* g = (float4*)gt.grad + i;
+        const unsigned c = (threadIdx.x >> 5) & (unsigned)(gt.copies - 1);
+        if (c) g = gt.spread + (size_t)(c - 1u) * (size_t)gt.rows_cap * 1000u + i;
+        asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(g), "f"(v.x), "f"(v.y), "f"(v.z),
+                     "f"(v.w)
+                     : "memory");
     }
 }
 
 // dL/d texel += w_j * d for the 8 taps of the sample at uvw (the addressing
-// of sample_brick, clamps included: clamped taps share a texel).
-__device__ __forceinline__ void scatter_texels(const RaycastParams& p, F3 uvw, float4 d, const GradTarget& gt) {
+// of sample_brick, clamps included: clamped taps share a texel).  The slot
+// map is read once per slot change: (c_slot, c_row) is the thread's last
+// slot and its row.  Taps in one slot (the usual case): WSUM groups the
+// lanes whose samples lie in the same cell (one __match_any_sync a sample:
+// the same 8 texels), sums each tap over the group by shuffles in lane order
+// and lets the group's first lane issue the atomics; without WSUM each lane
+// starts its 8 taps at a different one (fewer lanes of one instruction on
+// one texel).
+template <bool F64, bool WSUM>
+__device__ __forceinline__ void scatter_texels(const RaycastParams& p, F3 uvw, float4 d, const GradTarget& gt,
+                                               uint32_t& c_slot, int& c_row) {
     const float* N = p.u.brick_pool_dimension;
     const Axis ax = axis_taps(uvw.x, N[0], p.slots[0] * 10);
     const Axis ay = axis_taps(uvw.y, N[1], p.slots[1] * 10);
     const Axis az = axis_taps(uvw.z, N[2], p.slots[2] * 10);
     const uint32_t SX = (uint32_t)p.slots[0], SY = (uint32_t)p.slots[1];
+    const int lane = (int)(threadIdx.x & 31u);
+    if (ax.s0 == ax.s1 && ay.s0 == ay.s1 && az.s0 == az.s1) {
+        const uint32_t slot = ((uint32_t)az.s0 * SY + (uint32_t)ay.s0) * SX + (uint32_t)ax.s0;
+        if (slot != c_slot) {
+            c_row = grad_row(gt, slot, p.status);
+            c_slot = slot;
+        }
+        if (c_row < 0) return;
+        const uint32_t t0 = (uint32_t)((az.l0 * 10 + ay.l0) * 10 + ax.l0);
+        const uint32_t dx = (uint32_t)(ax.l1 - ax.l0), dy = (uint32_t)(10 * (ay.l1 - ay.l0)),
+                       dz = (uint32_t)(100 * (az.l1 - az.l0));
+        const size_t base = (size_t)c_row * 1000u + t0;
+        if (WSUM) {
+            const uint64_t key = ((uint64_t)(uint32_t)c_row << 16) | (t0 << 3) | (dx << 2) | ((dy ? 1u : 0u) << 1) |
+                                 (dz ? 1u : 0u);
+            const unsigned peers = __match_any_sync(__activemask(), key);
+            const bool group = __popc(peers) > 1;
+            const bool lead = lane == __ffs(peers) - 1;
 #pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int bx = t & 1, by = (t >> 1) & 1, bz = t >> 2;
+                const float w = (bx ? ax.f : 1.0f - ax.f) * (by ? ay.f : 1.0f - ay.f) * (bz ? az.f : 1.0f - az.f);
+                float4 v = make_float4(w * d.x, w * d.y, w * d.z, w * d.w);
+                if (group) {
+                    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (unsigned m = peers; m; m &= m - 1) {
+                        const int src = __ffs(m) - 1;
+                        s.x += __shfl_sync(peers, v.x, src);
+                        s.y += __shfl_sync(peers, v.y, src);
+                        s.z += __shfl_sync(peers, v.z, src);
+                        s.w += __shfl_sync(peers, v.w, src);
+                    }
+                    v = s;
+                }
+                if (lead && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))
+                    texel_atomic<F64>(gt, base + (bx ? dx : 0u) + (by ? dy : 0u) + (bz ? dz : 0u), v);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int t = (q + lane) & 7;
+                const int bx = t & 1, by = (t >> 1) & 1, bz = t >> 2;
+                const float w = (bx ? ax.f : 1.0f - ax.f) * (by ? ay.f : 1.0f - ay.f) * (bz ? az.f : 1.0f - az.f);
+                if (w == 0.0f) continue;
+                texel_atomic<F64>(gt, base + (bx ? dx : 0u) + (by ? dy : 0u) + (bz ? dz : 0u),
+                                  make_float4(w * d.x, w * d.y, w * d.z, w * d.w));
+            }
+        }
+        return;
+    }
+    // taps in two or more slots
+#pragma unroll 1
     for (int t = 0; t < 8; ++t) {
         const int bx = t & 1, by = (t >> 1) & 1, bz = t >> 2;
         const float w = (bx ? ax.f : 1.0f - ax.f) * (by ? ay.f : 1.0f - ay.f) * (bz ? az.f : 1.0f - az.f);
@@ -159,9 +211,13 @@ __device__ __forceinline__ void scatter_texels(const RaycastParams& p, F3 uvw, f
         const int sy = by ? ay.s1 : ay.s0, ly = by ? ay.l1 : ay.l0;
         const int sz = bz ? az.s1 : az.s0, lz = bz ? az.l1 : az.l0;
         const uint32_t slot = ((uint32_t)sz * SY + (uint32_t)sy) * SX + (uint32_t)sx;
-        const int row = grad_row(gt, slot, p.status);
-        if (row < 0) continue;
-        add_texel(gt, row, (uint32_t)((lz * 10 + ly) * 10 + lx), make_float4(w * d.x, w * d.y, w * d.z, w * d.w));
+        if (slot != c_slot) {
+            c_row = grad_row(gt, slot, p.status);
+            c_slot = slot;
+        }
+        if (c_row < 0) continue;
+        texel_atomic<F64>(gt, (size_t)c_row * 1000u + (uint32_t)((lz * 10 + ly) * 10 + lx),
+                          make_float4(w * d.x, w * d.y, w * d.z, w * d.w));
     }
 }
 
@@ -169,6 +225,14 @@ __device__ __forceinline__ void pixel_of(int& px, int& py) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     px = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
     py = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+}
+// The adjoint's pixels: a CTA covers the same 16x8 pixels, each warp every
+// second pixel of them in x and y, so that a warp's lanes sample fewer
+// common texels at once (fewer lanes of one atomic on one address).
+__device__ __forceinline__ void pixel_of_strided(int& px, int& py) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    px = blockIdx.x * 16 + 2 * (lane & 7) + (warp & 1);
+    py = blockIdx.y * 8 + 2 * (lane >> 3) + (warp >> 1);
 }
 
 }  // namespace
@@ -199,19 +263,20 @@ __global__ void __launch_bounds__(128, 7) forward_ckpt_kernel(const __grid_const
     __shared__ uint32_t path_p[kPathLevels][128];
     if (ray_origin(u, k, px, py, pos) && ray_start(p, k, px, py, pos, s))
         walk<FMT, false, CkptVisitor, 1, true>(p, k, s, vis,
-                                               PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
+                                               PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128, nullptr});
     if (p.color) p.color[pix] = s.dst;
     hdr[pix] = make_int2(vis.count, s.nsamples);
 }
 
-// 7 resident CTAs per SM (72 registers, a few bytes spilled): 3 % faster
-// than 5 on the paged 1080p adjoint leg, 0.5 % faster than 6
-template <int FMT>
+// 7 resident CTAs per SM (72 registers): the occupancy that measured
+// fastest for the walk.  F64: binary64 gradient rows; WSUM: the lanes of a
+// cell summed before the atomics (scatter_texels).
+template <int FMT, bool F64, bool WSUM>
 __global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
                                                        const Ckpt* ckpt, int per_ray, const float4* dl_dcolor,
                                                        const GradTarget gt) {
     int px, py;
-    pixel_of(px, py);
+    pixel_of_strided(px, py);
     const vv_uniforms& u = p.u;
     if (px >= u.width || py >= u.height) return;
     const size_t pix = (size_t)py * u.width + px;
@@ -229,7 +294,12 @@ __global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant_
     const Ckpt* ck = ckpt + pix * (size_t)per_ray;
     __shared__ uint2 path_w[kPathLevels][128];
     __shared__ uint32_t path_p[kPathLevels][128];
+    uint32_t c_slot = 0xFFFFFFFFu;  // the last slot scattered into and its gradient row
+    int c_row = -1;
     ReplayVisitor rv;
+    rv.gx = g.x;
+    rv.gy = g.y;
+    rv.gz = g.z;
     for (int c = C - 1; c >= 0; --c) {
         const Ckpt cc = ck[c];
         const int a = (int)cc.c.x, b = c + 1 < C ? (int)ck[c + 1].c.x : total;
@@ -245,16 +315,59 @@ __global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant_
             rv.first = a + m * kPiece;
             rv.last = min(b, rv.first + kPiece);
             rv.n = 0;
-            walk<FMT, false, ReplayVisitor, 1, true>(p, k, s, rv,
-                                                     PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128});
+            walk<FMT, false, ReplayVisitor, 1, true>(
+                p, k, s, rv, PathSlots{&path_w[0][threadIdx.x], &path_p[0][threadIdx.x], 128, nullptr});
             for (int j = rv.n - 1; j >= 0; --j) {
-                const float t = rv.T[j];
-                const float4 sv = rv.src[j];
-                if (rv.brick[j]) scatter_texels(p, rv.bpos[j], make_float4(g.x * t, g.y * t, g.z * t, g.w * t), gt);
-                g.w = g.w - (g.x * sv.x + g.y * sv.y + g.z * sv.z + g.w * sv.w);
+                const float tj = rv.T[j];
+                const float t = fabsf(tj);
+                if (!(__float_as_uint(tj) >> 31))
+                    scatter_texels<F64, WSUM>(p, rv.bpos[j], make_float4(g.x * t, g.y * t, g.z * t, g.w * t), gt,
+                                              c_slot, c_row);
+                // g.a -= dot(g, src), the products summed in the order x, y, z, w
+                g.w = g.w - (rv.r[j] + g.w * rv.a[j]);
             }
         }
     }
+}
+
+// grad[e] += copy_k[e] for the extra copies k of the rows in use, each copy
+// element zeroed after it is read (the copies are all zero between calls).
+// All loads of an element are issued before its stores (streaming: the
+// copies are not read again soon).
+template <int EXTRA>
+__global__ void spread_reduce_kernel(float4* __restrict__ grad, float4* __restrict__ spread,
+                                     const int* __restrict__ rows_used, int rows_cap) {
+    const size_t n = (size_t)min(*rows_used, rows_cap) * 1000u;
+    const size_t stride = (size_t)rows_cap * 1000u;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        float4 v[EXTRA];
+#pragma unroll
+        for (int k = 0; k < EXTRA; ++k) v[k] = __ldcs(spread + (size_t)k * stride + e);
+        float4 s = grad[e];
+#pragma unroll
+        for (int k = 0; k < EXTRA; ++k) s = make_float4(s.x + v[k].x, s.y + v[k].y, s.z + v[k].z, s.w + v[k].w);
+        grad[e] = s;
+#pragma unroll
+        for (int k = 0; k < EXTRA; ++k) __stcs(spread + (size_t)k * stride + e, zero);
+    }
+}
+
+cudaError_t launch_spread_reduce(const GradTarget& grad, cudaStream_t s) {
+    if (grad.copies <= 1) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const dim3 blocks((unsigned)(sms * 16)), threads(256);
+    switch (grad.copies) {
+        case 2: spread_reduce_kernel<1><<<blocks, threads, 0, s>>>((float4*)grad.grad, grad.spread, grad.rows_used,
+                                                                   grad.rows_cap); break;
+        case 4: spread_reduce_kernel<3><<<blocks, threads, 0, s>>>((float4*)grad.grad, grad.spread, grad.rows_used,
+                                                                   grad.rows_cap); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 size_t ckpt_bytes(int w, int h, int per_ray) {
@@ -282,13 +395,23 @@ cudaError_t launch_backward(int fmt, const RaycastParams& p, const void* ckpt, i
     const int2* hdr = (const int2*)ckpt;
     const Ckpt* ck = (const Ckpt*)((const char*)ckpt + (size_t)W * H * sizeof(int2));
     dim3 block(128), grid((unsigned)((W + 15) / 16), (unsigned)((H + 7) / 8));
+#define VV_BWD(F)                                                                                    \
+    if (grad.f64 && grad.warp_sum)                                                                   \
+        backward_kernel<F, true, true><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad);   \
+    else if (grad.f64)                                                                               \
+        backward_kernel<F, true, false><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad);  \
+    else if (grad.warp_sum)                                                                          \
+        backward_kernel<F, false, true><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad);  \
+    else                                                                                             \
+        backward_kernel<F, false, false><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad);
     switch (fmt) {
-        case VV_FMT_RGBA8: backward_kernel<VV_FMT_RGBA8><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
-        case VV_FMT_FP16: backward_kernel<VV_FMT_FP16><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
-        case VV_FMT_BF16: backward_kernel<VV_FMT_BF16><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
-        case VV_FMT_FP32: backward_kernel<VV_FMT_FP32><<<grid, block, 0, s>>>(p, hdr, ck, per_ray, dl_dcolor, grad); break;
+        case VV_FMT_RGBA8: VV_BWD(VV_FMT_RGBA8) break;
+        case VV_FMT_FP16: VV_BWD(VV_FMT_FP16) break;
+        case VV_FMT_BF16: VV_BWD(VV_FMT_BF16) break;
+        case VV_FMT_FP32: VV_BWD(VV_FMT_FP32) break;
         default: return cudaErrorInvalidValue;
     }
+#undef VV_BWD
     return cudaGetLastError();
 }
 

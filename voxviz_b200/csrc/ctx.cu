@@ -188,7 +188,7 @@ int vv_ctx_destroy(vv_ctx* c) {
     if (c->bricks && !c->bricks_external) cudaFree(c->bricks);
     void* bufs[] = {c->d_status, c->d_jitter, c->d_usage, c->d_mask, c->d_counts, c->d_offsets,
                     c->d_up_slots, c->d_up_bricks, c->d_patches, c->d_grid_words, c->d_batch, c->grads,
-                    c->cell_mask, c->d_refill_counter};
+                    c->cell_mask, c->d_refill_counter, c->d_spread};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -518,7 +518,11 @@ int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* d
     int rc = diff_params(c, tree, u, p);
     if (rc) return rc;
     if (!ckpt || per_ray <= 0 || !dl_dcolor || !g || !g->grad) return fail(c, VV_ERR_ARG, "bad backward buffers");
-    if ((g->flags & ~(VV_GRAD_F64 | VV_GRAD_WARP_SUM)) != 0) return fail(c, VV_ERR_ARG, "unknown gradient flags");
+    if ((g->flags & ~(VV_GRAD_F64 | VV_GRAD_WARP_SUM | VV_GRAD_SPREAD)) != 0)
+        return fail(c, VV_ERR_ARG, "unknown gradient flags");
+    const bool spread = (g->flags & VV_GRAD_SPREAD) != 0;
+    if (spread && (!g->slot_map || (g->flags & VV_GRAD_F64)))
+        return fail(c, VV_ERR_ARG, "VV_GRAD_SPREAD needs a slot map and binary32 rows");
     const uintptr_t align = (g->flags & VV_GRAD_F64) ? 32u : 16u;
     if (((uintptr_t)g->grad & (align - 1)) != 0 || ((uintptr_t)dl_dcolor & 15u) != 0)
         return fail(c, VV_ERR_ARG, "gradient buffers must be aligned to a texel (16 bytes, 32 for binary64)");
@@ -532,7 +536,30 @@ int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* d
     gt.slot_map = g->slot_map;
     gt.rows_used = g->rows_used;
     gt.rows_cap = g->slot_map ? g->rows_cap : 0;
+    gt.copies = 1;
+    gt.spread = nullptr;
+    if (spread) {
+        const size_t need = (size_t)(VV_GRAD_SPREAD_COPIES - 1) * (size_t)g->rows_cap * 1000u;
+        if (c->spread_elems < need) {
+            // grown by half again at least, so that row capacities that vary
+            // from call to call settle after a few calls
+            const size_t want = std::max(need, c->spread_elems + c->spread_elems / 2);
+            if (c->d_spread) cudaFree(c->d_spread);
+            c->d_spread = nullptr;
+            c->spread_elems = 0;
+            if (cudaMalloc((void**)&c->d_spread, want * sizeof(float4)) != cudaSuccess) {
+                c->d_spread = nullptr;
+                return fail(c, VV_ERR_OOM, "cudaMalloc gradient copies");
+            }
+            // zero once: the reduction re-zeroes what the adjoint wrote
+            VV_CUDA(c, cudaMemsetAsync(c->d_spread, 0, want * sizeof(float4), c->stream));
+            c->spread_elems = want;
+        }
+        gt.copies = VV_GRAD_SPREAD_COPIES;
+        gt.spread = c->d_spread;
+    }
     VV_CUDA(c, launch_backward(c->fmt, p, ckpt, per_ray, (const float4*)dl_dcolor, gt, c->stream));
+    VV_CUDA(c, launch_spread_reduce(gt, c->stream));
     return VV_OK;
 }
 

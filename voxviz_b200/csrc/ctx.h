@@ -82,6 +82,10 @@ struct vv_ctx {
     size_t h_batch_cap = 0;
     void* d_batch = nullptr;
     size_t d_batch_cap = 0;
+    // extra copies of a sparse gradient's rows (VV_GRAD_SPREAD), all zero
+    // between calls
+    float4* d_spread = nullptr;
+    size_t spread_elems = 0;
     // ray-cast form (VV_RAYCAST_TILES / VV_RAYCAST_REFILL) and the refill
     // form's tile counter
     int raycast_mode = 0;

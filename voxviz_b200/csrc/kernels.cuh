@@ -68,7 +68,10 @@ cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int
 // Where the adjoint adds dL/d(texel): `grad` holds 4 floats (or, with f64,
 // 4 doubles) per texel, 1000 texels per row; row = brick-pool slot (dense,
 // slot_map NULL) or the row the slot map assigns (claimed on first touch
-// from rows_used, at most rows_cap rows).
+// from rows_used, at most rows_cap rows).  With copies > 1 (binary32 sparse
+// rows) warp w of a CTA adds to copy w % copies: copy 0 is `grad`, copy
+// k > 0 starts at spread + (k - 1) * rows_cap * 1000 (all zero before the
+// launch; launch_spread_reduce adds them into `grad` and zeroes them).
 struct GradTarget {
     void* grad;
     int f64;
@@ -76,9 +79,12 @@ struct GradTarget {
     int* slot_map;
     int* rows_used;
     int rows_cap;
+    int copies;      // 1, 2 or 4
+    float4* spread;  // copies 1..copies-1
 };
 cudaError_t launch_backward(int fmt, const RaycastParams& p, const void* ckpt, int per_ray, const float4* dl_dcolor,
                             const GradTarget& grad, cudaStream_t s);
+cudaError_t launch_spread_reduce(const GradTarget& grad, cudaStream_t s);
 cudaError_t launch_select(const uint4* usage, uint32_t* mask, uint32_t* level0, int w, int h,
                           cudaStream_t s);
 cudaError_t launch_compact(const CompactParams& p, cudaStream_t s);
