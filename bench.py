@@ -984,6 +984,22 @@ def run_fit(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_ms = vdist.max_over_ranks(t0.elapsed_time(t1), "cuda")
+    # A/B: the same backward with the atomics spread over four copies of the
+    # gradient (VV_GRAD_SPREAD, one reduction over the pool after the views)
+    spread_bwd_ms = []
+    for step in range(4 + 2):
+        c = diff.render(param, ctx, slots, us_mine, spread=True)
+        loss = ((c - target_mine) ** 2).sum() / target.numel()
+        param.grad = None
+        ev[1].record()
+        loss.backward()
+        vdist.sum_gradients(param.grad)
+        ev[2].record()
+        torch.cuda.synchronize()
+        if step >= 2:
+            spread_bwd_ms.append(ev[1].elapsed_time(ev[2]))
+    param.grad = None
+    b_spread = vdist.max_over_ranks(float(np.mean(spread_bwd_ms)), "cuda")
     status |= diff.check_status(ctx)
     if losses:
         lt = torch.stack(losses)
@@ -1000,7 +1016,10 @@ def run_fit(args):
         "fwd_mrays_s": round(rays / (f / 1e3) / 1e6, 2), "higher_is_better": True,
         "plain_raycast_mrays_s": round(rays / (plain_ms / 1e3) / 1e6, 2),
         "ms": {"fwd": round(f, 3), "bwd": round(b, 3), "adam": round(a, 3),
-               "step_total_mean": round(total_ms / max(1, args.fit_steps), 3)},
+               "step_total_mean": round(total_ms / max(1, args.fit_steps), 3),
+               "bwd_with_spread": round(b_spread, 3)},
+        "bwd_form": "dense binary32 gradient, plain atomics (A/B: spread over 4 copies, reduced over the pool once "
+                    "per step)",
         "adam_steps": args.fit_steps, "lr": FIT_LR,
         "loss": {"first": losses[0] if losses else None, "last": losses[-1] if losses else None,
                  "at": {str(k): losses[k] for k in (0, 10, 50, 100, 199) if k < len(losses)}},
@@ -1129,6 +1148,8 @@ def run_batched(args):
     # first-seen order over the views, one LRU pass), not one per view
     views_of = [[k for k, (t, _) in enumerate(views) if t is tt] for tt in trees]
 
+    service_parts = {"ms_readback": 0.0, "ms_visit": 0.0, "ms_policy": 0.0, "requests": 0}
+
     def service_all():
         counts = torch.cat([cnt for _, _, cnt in req]).cpu().tolist()
         for t, ks in zip(trees, views_of):
@@ -1137,6 +1158,10 @@ def run_batched(args):
             total = torch.tensor([cat.shape[0]], dtype=torch.int32, device=dev)
             t["r"].service(cat.data_ptr(), total.data_ptr(), max(1, int(cat.shape[0])))
             t["r"].stage_uploads()
+            st = t["r"].stats()
+            for key in ("ms_readback", "ms_visit", "ms_policy"):
+                service_parts[key] += st[key]
+            service_parts["requests"] += int(cat.shape[0])
 
     graph = torch.cuda.CUDAGraph()
     side = torch.cuda.Stream()
@@ -1156,13 +1181,21 @@ def run_batched(args):
     t0 = time.perf_counter()
     paged_frames = 4
     total_before = sum(t["r"].stats()["bricks_uploaded_total"] for t in trees)
+    frame_parts = []
     for _ in range(paged_frames):
+        for key in service_parts:
+            service_parts[key] = 0
+        ta = time.perf_counter()
         graph.replay()
         torch.cuda.synchronize()
+        tb = time.perf_counter()
         service_all()
+        tc = time.perf_counter()
         total_now = sum(t["r"].stats()["bricks_uploaded_total"] for t in trees)
         uploads.append(int(total_now - total_before))
         total_before = total_now
+        frame_parts.append({"ms_graph": round((tb - ta) * 1e3, 2), "ms_service": round((tc - tb) * 1e3, 2),
+                            **{k: round(v, 2) if k != "requests" else v for k, v in service_parts.items()}})
     torch.cuda.synchronize()
     ms_frame_paged = (time.perf_counter() - t0) / paged_frames * 1e3
     for t in trees:
@@ -1178,6 +1211,7 @@ def run_batched(args):
                "frame_graph_with_staged_uploads": round(ms_frame_graph, 3),
                "frame_graph_plus_host_service": round(ms_frame_paged, 3)},
         "uploads_per_paged_frame": uploads,
+        "paged_frame_parts": frame_parts,
         "autotune": tune, "bitexact_vs_per_view": exact,
         "graph_requests_equal_eager": counts_graph == counts_eager,
         "kernel_launches_per_frame": launches_frame, "status": status,
@@ -1316,8 +1350,10 @@ def summarise_config(key, d):
                             for f, v in d["formats"].items()}, "config": d["config"]}
     if key == "config4_batched":
         return {k: d[k] for k in ("value", "unit", "per_view_mrays_s", "ms", "bitexact_vs_per_view",
-                                  "graph_requests_equal_eager", "uploads_per_paged_frame", "autotune", "config")}
-    return {k: d[k] for k in ("value", "unit", "fwd_mrays_s", "plain_raycast_mrays_s", "ms", "adam_steps", "loss",
+                                  "graph_requests_equal_eager", "uploads_per_paged_frame", "paged_frame_parts",
+                                  "autotune", "config")}
+    return {k: d[k] for k in ("value", "unit", "fwd_mrays_s", "plain_raycast_mrays_s", "ms", "bwd_form", "adam_steps",
+                              "loss",
                               "grad_check_fd_gpu_fp32", "grad_check_fd_fixed_path_fp64",
                               "grad_check_fp64_host_adjoint", "status", "config")}
 

@@ -325,14 +325,19 @@ int vv_backward(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl
  * texels) are summed with __match_any_sync and shuffles first, one atomic
  * per texel and cell group. */
 #define VV_GRAD_WARP_SUM 2
-/* Spread the atomics of a sparse binary32 gradient (needs a slot map; not
- * with VV_GRAD_F64, else VV_ERR_ARG) over VV_GRAD_SPREAD_COPIES copies of
- * the rows: the warps of a CTA add to different copies (fewer concurrent
- * atomics on one address), the extra copies live in context memory
- * ((copies - 1) * rows_cap * 16000 bytes, kept between calls) and are added
- * into `grad` on the stream after the adjoint.  Same gradient up to the
- * order of the float additions. */
+/* Spread the atomics of a binary32 gradient (not with VV_GRAD_F64, else
+ * VV_ERR_ARG) over VV_GRAD_SPREAD_COPIES copies of the rows: the warps of a
+ * CTA add to different copies (fewer concurrent atomics on one address).
+ * The extra copies live in context memory ((copies - 1) * rows * 16000
+ * bytes, rows = rows_cap with a slot map, else the pool's slots; kept
+ * between calls) and are added into `grad` on the stream after the adjoint
+ * (the rows in use with a slot map, every slot without).  Same gradient up
+ * to the order of the float additions.  With VV_GRAD_SPREAD_KEEP as well
+ * the sums stay in the copies; the next call with VV_GRAD_SPREAD and
+ * without KEEP adds them into its `grad` - the calls in between must use
+ * the same `grad`, slot map and row count (e.g. the views of one step). */
 #define VV_GRAD_SPREAD 4
+#define VV_GRAD_SPREAD_KEEP 8
 #define VV_GRAD_SPREAD_COPIES 4
 typedef struct vv_grad_desc {
     void* grad;

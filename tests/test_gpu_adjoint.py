@@ -202,8 +202,42 @@ def test_spread_copies_stay_zero_between_calls(fp32_scene):
     with pytest.raises(vv.VVError):
         run(n_slots, spread=True, f64=True)
     with pytest.raises(vv.VVError):
-        g.ctx.backward_ex(u, dl_t.data_ptr(), ck.data_ptr(), 16,
-                          torch.zeros((n_slots, 1000, 4), device=dev).data_ptr(), spread=True)
+        run(n_slots, keep=True)
+
+
+def test_spread_dense_rows_and_kept_sums(fp32_scene):
+    """VV_GRAD_SPREAD on dense rows (one row per pool slot), and
+    VV_GRAD_SPREAD_KEEP: two views whose copies are reduced once give the
+    sum of the two views' plain gradients."""
+    sc, g = fp32_scene
+    n_slots = int(np.prod(sc.slots))
+    dev = torch.device("cuda", 0)
+    views = []
+    for seed, (w, h) in ((5, (96, 64)), (8, (160, 120))):
+        u = sc.uniforms(sc.view(seed, w, h))
+        _, ck = _ckpt_color(g, u, 16)
+        rng = np.random.default_rng(seed)
+        views.append((u, ck, torch.from_numpy(rng.standard_normal((h, w, 4)).astype(np.float32)).cuda()))
+    ref = torch.zeros((n_slots, 1000, 4), dtype=torch.float32, device=dev)
+    for u, ck, dl in views:
+        g.ctx.backward(u, dl.data_ptr(), ck.data_ptr(), 16, ref.data_ptr())
+    one = torch.zeros_like(ref)
+    u, ck, dl = views[0]
+    g.ctx.backward_ex(u, dl.data_ptr(), ck.data_ptr(), 16, one.data_ptr(), spread=True)
+    two = torch.zeros_like(ref)
+    for k, (u, ck, dl) in enumerate(views):
+        g.ctx.backward_ex(u, dl.data_ptr(), ck.data_ptr(), 16, two.data_ptr(), spread=True, keep=k == 0)
+    torch.cuda.synchronize()
+    assert g.ctx.device_status() == 0
+    ref_one = torch.zeros_like(ref)
+    u0, ck0, dl0 = views[0]
+    g.ctx.backward(u0, dl0.data_ptr(), ck0.data_ptr(), 16, ref_one.data_ptr())
+    r1, o1, r2, o2 = (x.cpu().numpy().astype(np.float64) for x in (ref_one, one, ref, two))
+    for r, o in ((r1, o1), (r2, o2)):
+        scale = np.abs(r).max()
+        assert scale > 0
+        assert np.array_equal(r != 0, o != 0)
+        assert np.abs(o - r).max() <= 1e-5 * scale
 
 
 def test_sparse_rows_report_overflow(fp32_scene):

@@ -445,13 +445,14 @@ class Context:
 
     def backward_ex(self, u: Uniforms, dl_dcolor: int, ckpt: int, per_ray: int, grad: int, f64: bool = False,
                     slot_map: int = 0, rows_used: int = 0, rows_cap: int = 0, tree: int = 0,
-                    warp_sum: bool = False, spread: bool = False) -> None:
+                    warp_sum: bool = False, spread: bool = False, keep: bool = False) -> None:
         """vv_backward_ex: binary64 accumulation, a sparse gradient (rows
         claimed per touched slot through `slot_map`), warp sums before the
-        atomics and/or the atomics spread over copies of the rows (sparse
-        binary32 rows only)."""
+        atomics and/or the atomics spread over copies of the rows (binary32
+        rows; with `keep` the copies' sums wait for the next spread call
+        without it)."""
         flags = ((N.VV_GRAD_F64 if f64 else 0) | (N.VV_GRAD_WARP_SUM if warp_sum else 0) |
-                 (N.VV_GRAD_SPREAD if spread else 0))
+                 (N.VV_GRAD_SPREAD if spread else 0) | (N.VV_GRAD_SPREAD_KEEP if keep else 0))
         g = N.GradDesc(grad=grad, flags=flags, rows_cap=rows_cap, slot_map=slot_map or None,
                        rows_used=rows_used or None)
         self._ck(lib().vv_backward_ex(self._h, tree, C.byref(u), C.c_void_p(dl_dcolor), C.c_void_p(ckpt), per_ray,

@@ -242,7 +242,7 @@ class GradDesc(C.Structure):
                 ("rows_used", C.c_void_p)]
 
 
-VV_GRAD_F64, VV_GRAD_WARP_SUM, VV_GRAD_SPREAD = 1, 2, 4
+VV_GRAD_F64, VV_GRAD_WARP_SUM, VV_GRAD_SPREAD, VV_GRAD_SPREAD_KEEP = 1, 2, 4, 8
 VV_RAYCAST_TILES, VV_RAYCAST_REFILL, VV_RAYCAST_STAGED = 0, 1, 2
 
 

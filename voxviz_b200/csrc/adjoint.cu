@@ -127,7 +127,7 @@ __device__ __forceinline__ void texel_atomic(const GradTarget& gt, size_t i, flo
     } else {
         float4* g = (float4*)gt.grad + i;
         const unsigned c = (threadIdx.x >> 5) & (unsigned)(gt.copies - 1);
-        if (c) g = gt.spread + (size_t)(c - 1u) * (size_t)gt.rows_cap * 1000u + i;
+        if (c) g = gt.spread + (size_t)(c - 1u) * (size_t)gt.spread_rows * 1000u + i;
         asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(g), "f"(v.x), "f"(v.y), "f"(v.z),
                      "f"(v.w)
                      : "memory");
@@ -330,15 +330,15 @@ __global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant_
     }
 }
 
-// grad[e] += copy_k[e] for the extra copies k of the rows in use, each copy
-// element zeroed after it is read (the copies are all zero between calls).
-// All loads of an element are issued before its stores (streaming: the
-// copies are not read again soon).
+// grad[e] += copy_k[e] for the extra copies k of the rows in use (all rows
+// without a row counter), each copy element zeroed after it is read (the
+// copies are all zero between reductions).  All loads of an element are
+// issued before its stores (streaming: the copies are not read again soon).
 template <int EXTRA>
 __global__ void spread_reduce_kernel(float4* __restrict__ grad, float4* __restrict__ spread,
-                                     const int* __restrict__ rows_used, int rows_cap) {
-    const size_t n = (size_t)min(*rows_used, rows_cap) * 1000u;
-    const size_t stride = (size_t)rows_cap * 1000u;
+                                     const int* __restrict__ rows_used, int rows) {
+    const size_t n = (size_t)(rows_used ? min(*rows_used, rows) : rows) * 1000u;
+    const size_t stride = (size_t)rows * 1000u;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         float4 v[EXTRA];
@@ -362,9 +362,9 @@ cudaError_t launch_spread_reduce(const GradTarget& grad, cudaStream_t s) {
     const dim3 blocks((unsigned)(sms * 16)), threads(256);
     switch (grad.copies) {
         case 2: spread_reduce_kernel<1><<<blocks, threads, 0, s>>>((float4*)grad.grad, grad.spread, grad.rows_used,
-                                                                   grad.rows_cap); break;
+                                                                   grad.spread_rows); break;
         case 4: spread_reduce_kernel<3><<<blocks, threads, 0, s>>>((float4*)grad.grad, grad.spread, grad.rows_used,
-                                                                   grad.rows_cap); break;
+                                                                   grad.spread_rows); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -518,11 +518,12 @@ int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* d
     int rc = diff_params(c, tree, u, p);
     if (rc) return rc;
     if (!ckpt || per_ray <= 0 || !dl_dcolor || !g || !g->grad) return fail(c, VV_ERR_ARG, "bad backward buffers");
-    if ((g->flags & ~(VV_GRAD_F64 | VV_GRAD_WARP_SUM | VV_GRAD_SPREAD)) != 0)
+    if ((g->flags & ~(VV_GRAD_F64 | VV_GRAD_WARP_SUM | VV_GRAD_SPREAD | VV_GRAD_SPREAD_KEEP)) != 0)
         return fail(c, VV_ERR_ARG, "unknown gradient flags");
     const bool spread = (g->flags & VV_GRAD_SPREAD) != 0;
-    if (spread && (!g->slot_map || (g->flags & VV_GRAD_F64)))
-        return fail(c, VV_ERR_ARG, "VV_GRAD_SPREAD needs a slot map and binary32 rows");
+    const bool keep = (g->flags & VV_GRAD_SPREAD_KEEP) != 0;
+    if ((spread && (g->flags & VV_GRAD_F64)) || (keep && !spread))
+        return fail(c, VV_ERR_ARG, "VV_GRAD_SPREAD needs binary32 rows; VV_GRAD_SPREAD_KEEP needs VV_GRAD_SPREAD");
     const uintptr_t align = (g->flags & VV_GRAD_F64) ? 32u : 16u;
     if (((uintptr_t)g->grad & (align - 1)) != 0 || ((uintptr_t)dl_dcolor & 15u) != 0)
         return fail(c, VV_ERR_ARG, "gradient buffers must be aligned to a texel (16 bytes, 32 for binary64)");
@@ -538,8 +539,13 @@ int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* d
     gt.rows_cap = g->slot_map ? g->rows_cap : 0;
     gt.copies = 1;
     gt.spread = nullptr;
+    gt.spread_rows = 0;
     if (spread) {
-        const size_t need = (size_t)(VV_GRAD_SPREAD_COPIES - 1) * (size_t)g->rows_cap * 1000u;
+        const long long rows = g->slot_map ? (long long)g->rows_cap : c->total_slots;
+        if (rows <= 0 || rows > INT32_MAX) return fail(c, VV_ERR_ARG, "no rows to spread over");
+        if (c->spread_rows_kept && c->spread_rows_kept != rows)
+            return fail(c, VV_ERR_ARG, "kept gradient copies have another row count");
+        const size_t need = (size_t)(VV_GRAD_SPREAD_COPIES - 1) * (size_t)rows * 1000u;
         if (c->spread_elems < need) {
             // grown by half again at least, so that row capacities that vary
             // from call to call settle after a few calls
@@ -557,9 +563,15 @@ int vv_backward_ex(vv_ctx* c, int32_t tree, const vv_uniforms* u, const float* d
         }
         gt.copies = VV_GRAD_SPREAD_COPIES;
         gt.spread = c->d_spread;
+        gt.spread_rows = (int)rows;
     }
     VV_CUDA(c, launch_backward(c->fmt, p, ckpt, per_ray, (const float4*)dl_dcolor, gt, c->stream));
-    VV_CUDA(c, launch_spread_reduce(gt, c->stream));
+    if (keep) {
+        c->spread_rows_kept = gt.spread_rows;
+    } else {
+        c->spread_rows_kept = 0;
+        VV_CUDA(c, launch_spread_reduce(gt, c->stream));
+    }
     return VV_OK;
 }
 

@@ -86,6 +86,7 @@ struct vv_ctx {
     // between calls
     float4* d_spread = nullptr;
     size_t spread_elems = 0;
+    long long spread_rows_kept = 0;  // rows per copy of sums kept by VV_GRAD_SPREAD_KEEP, else 0
     // ray-cast form (VV_RAYCAST_TILES / VV_RAYCAST_REFILL) and the refill
     // form's tile counter
     int raycast_mode = 0;

@@ -68,10 +68,11 @@ cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int
 // Where the adjoint adds dL/d(texel): `grad` holds 4 floats (or, with f64,
 // 4 doubles) per texel, 1000 texels per row; row = brick-pool slot (dense,
 // slot_map NULL) or the row the slot map assigns (claimed on first touch
-// from rows_used, at most rows_cap rows).  With copies > 1 (binary32 sparse
-// rows) warp w of a CTA adds to copy w % copies: copy 0 is `grad`, copy
-// k > 0 starts at spread + (k - 1) * rows_cap * 1000 (all zero before the
-// launch; launch_spread_reduce adds them into `grad` and zeroes them).
+// from rows_used, at most rows_cap rows).  With copies > 1 (binary32 rows)
+// warp w of a CTA adds to copy w % copies: copy 0 is `grad`, copy k > 0
+// starts at spread + (k - 1) * spread_rows * 1000 (spread_rows = rows_cap,
+// or the pool's slots for dense rows; all zero before the first launch;
+// launch_spread_reduce adds the rows in use into `grad` and zeroes them).
 struct GradTarget {
     void* grad;
     int f64;
@@ -79,8 +80,9 @@ struct GradTarget {
     int* slot_map;
     int* rows_used;
     int rows_cap;
-    int copies;      // 1, 2 or 4
-    float4* spread;  // copies 1..copies-1
+    int copies;       // 1, 2 or 4
+    float4* spread;   // copies 1..copies-1
+    int spread_rows;  // rows per copy
 };
 cudaError_t launch_backward(int fmt, const RaycastParams& p, const void* ckpt, int per_ray, const float4* dl_dcolor,
                             const GradTarget& grad, cudaStream_t s);

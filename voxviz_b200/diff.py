@@ -5,8 +5,12 @@ per texel, brick-linear 10x10x10 slots, the layout of ``vv_brickpool_*``)
 attached to a :class:`~voxviz_b200.Context` as caller-owned memory.  The
 forward runs the checkpointing ray cast of every view
 (``vv_render_forward_ckpt``: the same colour as ``vv_render``, bit for bit);
-the backward runs the adjoint (``vv_backward``), which adds dL/d(texel) into
-a zeroed tensor of the pool's shape.  The forward's control flow (descent,
+the backward runs the adjoint (``vv_backward_ex``), which adds dL/d(texel)
+into a zeroed tensor of the pool's shape; with ``spread`` the views' atomics
+go to four copies of the gradient in context memory (three times the pool's
+size; fewer concurrent atomics on one texel), added into the tensor once
+after the last view - a pass over the whole pool, which on dense pools of
+many slots costs more than the contention it removes (the default is off).  The forward's control flow (descent,
 step counts, early termination) is held fixed, as for any reverse-mode
 derivative of the shader (GigaVoxelsNoLighting.frag:280,354 composite
 ``dst += (1 - dst.a) * src``).
@@ -70,7 +74,8 @@ class RayCast(torch.autograd.Function):
     """colour (V, H, W, 4) float32 = ray cast of every view over ``pool``."""
 
     @staticmethod
-    def forward(fctx, pool: torch.Tensor, ctx: Context, slots, uniforms: Sequence[Uniforms], per_ray: int):
+    def forward(fctx, pool: torch.Tensor, ctx: Context, slots, uniforms: Sequence[Uniforms], per_ray: int,
+                spread: bool = False):
         attach_pool(ctx, pool, slots)
         _bind_stream(ctx, pool.device)
         H, W = uniforms[0].height, uniforms[0].width
@@ -86,6 +91,7 @@ class RayCast(torch.autograd.Function):
         fctx.slots = slots
         fctx.uniforms = list(uniforms)
         fctx.per_ray = per_ray
+        fctx.spread = spread
         fctx.save_for_backward(pool, ckpt)
         return color
 
@@ -97,15 +103,17 @@ class RayCast(torch.autograd.Function):
         _bind_stream(ctx, pool.device)
         g = grad_color.contiguous().to(torch.float32)
         grad = torch.zeros_like(pool)
+        last = len(fctx.uniforms) - 1
         for v, u in enumerate(fctx.uniforms):
-            ctx.backward(u, g[v].data_ptr(), ckpt[v].data_ptr(), fctx.per_ray, grad.data_ptr())
-        return grad, None, None, None, None
+            ctx.backward_ex(u, g[v].data_ptr(), ckpt[v].data_ptr(), fctx.per_ray, grad.data_ptr(),
+                            spread=fctx.spread, keep=fctx.spread and v < last)
+        return grad, None, None, None, None, None
 
 
 def render(pool: torch.Tensor, ctx: Context, slots, uniforms: Sequence[Uniforms],
-           per_ray: int = DEFAULT_PER_RAY) -> torch.Tensor:
+           per_ray: int = DEFAULT_PER_RAY, spread: bool = False) -> torch.Tensor:
     """Differentiable colour of every view; ``pool`` may require grad."""
-    return RayCast.apply(pool, ctx, slots, list(uniforms), per_ray)
+    return RayCast.apply(pool, ctx, slots, list(uniforms), per_ray, spread)
 
 
 def check_status(ctx: Context) -> int:
