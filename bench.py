@@ -103,11 +103,21 @@ class ClockSampler:
         self.p = None
 
     def start(self):
+        """Start sampling every 25 ms and return once the first sample is
+        written, so that the sampler is running when the timed region
+        starts (nvidia-smi takes a while to come up)."""
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "25"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return
+        t_end = time.perf_counter() + 5.0
+        while time.perf_counter() < t_end and self.p.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if self.p is None:
@@ -1179,10 +1189,15 @@ def run_batched(args):
     # whole frames: graph replay, then the host service of all 64 views
     uploads = []
     t0 = time.perf_counter()
-    paged_frames = 4
+    # 3 warm-up frames (the first services after the switch to
+    # one service per terrain size their buffers), then 4 timed frames
+    warm_frames, paged_frames = 3, 4
     total_before = sum(t["r"].stats()["bricks_uploaded_total"] for t in trees)
     frame_parts = []
-    for _ in range(paged_frames):
+    for fi in range(warm_frames + paged_frames):
+        if fi == warm_frames:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
         for key in service_parts:
             service_parts[key] = 0
         ta = time.perf_counter()
@@ -1194,7 +1209,8 @@ def run_batched(args):
         total_now = sum(t["r"].stats()["bricks_uploaded_total"] for t in trees)
         uploads.append(int(total_now - total_before))
         total_before = total_now
-        frame_parts.append({"ms_graph": round((tb - ta) * 1e3, 2), "ms_service": round((tc - tb) * 1e3, 2),
+        frame_parts.append({"warmup": fi < warm_frames,
+                            "ms_graph": round((tb - ta) * 1e3, 2), "ms_service": round((tc - tb) * 1e3, 2),
                             **{k: round(v, 2) if k != "requests" else v for k, v in service_parts.items()}})
     torch.cuda.synchronize()
     ms_frame_paged = (time.perf_counter() - t0) / paged_frames * 1e3

@@ -158,7 +158,7 @@ GigaVoxelsRenderer::~GigaVoxelsRenderer() {
         if (b) cudaFree(b);
     slot_order_free(order_);
     if (ev_flush_) cudaEventDestroy(ev_flush_);
-    void* hbufs[] = {h_def_jobs_, h_def_patches_, h_def_counts_, h_fjobs_, h_fpatch_};
+    void* hbufs[] = {h_def_jobs_, h_def_patches_, (void*)h_def_counts_, h_fjobs_, h_fpatch_};
     for (void* b : hbufs)
         if (b) cudaFreeHost(b);
 }
@@ -715,7 +715,8 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
     // change is pending on the host), the distinct nodes are classified on
     // the device, whose LRU order takes their touches and the root's; the
     // host reads back only the upload candidates and the order's front.
-    const bool classified = !deferred_ && touched_.empty();
+    // (deferred uploads: once the device has applied the last staging)
+    const bool classified = touched_.empty() && (!deferred_ || h_def_counts_[3] == h_def_counts_[2]);
     uint32_t root_slot = 0xFFFFFFFFu;
     if (classified) {
         int rc = flush_touches();  // earlier host touches come first
@@ -902,12 +903,12 @@ int GigaVoxelsRenderer::set_deferred(bool on) {
         if (cudaHostAlloc((void**)&h_def_jobs_, (size_t)def_job_cap_ * sizeof(uint4), cudaHostAllocMapped) !=
                 cudaSuccess ||
             cudaHostAlloc((void**)&h_def_patches_, patch_bytes, cudaHostAllocMapped) != cudaSuccess ||
-            cudaHostAlloc((void**)&h_def_counts_, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostAlloc((void**)const_cast<uint32_t**>(&h_def_counts_), 4 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
             cudaMalloc((void**)&d_def_jobs_, (size_t)def_job_cap_ * sizeof(uint4)) != cudaSuccess ||
             cudaMalloc((void**)&d_def_patches_, patch_bytes) != cudaSuccess ||
             cudaMalloc((void**)&d_def_counts_, 2 * sizeof(uint32_t)) != cudaSuccess)
             return VV_ERR_OOM;
-        h_def_counts_[0] = h_def_counts_[1] = 0;
+        h_def_counts_[0] = h_def_counts_[1] = h_def_counts_[2] = h_def_counts_[3] = 0;
         slot_job_.assign(total_slots_, -1);
     }
     deferred_ = true;
@@ -950,6 +951,7 @@ int GigaVoxelsRenderer::stage_uploads() {
     pending_slots_.clear();
     h_def_counts_[0] = nj;
     h_def_counts_[1] = np;
+    if (nj || np) h_def_counts_[2] = ++stage_gen_;  // applied once the enqueued work has run
     return VV_OK;
 }
 
@@ -960,7 +962,7 @@ int GigaVoxelsRenderer::enqueue_uploads() {
     uint32_t* counts = nullptr;
     if (cudaHostGetDevicePointer((void**)&jobs, h_def_jobs_, 0) != cudaSuccess ||
         cudaHostGetDevicePointer((void**)&patches, h_def_patches_, 0) != cudaSuccess ||
-        cudaHostGetDevicePointer((void**)&counts, h_def_counts_, 0) != cudaSuccess)
+        cudaHostGetDevicePointer((void**)&counts, (void*)h_def_counts_, 0) != cudaSuccess)
         return VV_ERR_CUDA;
     void* pool = nullptr;
     size_t pool_bytes = 0;
@@ -980,6 +982,8 @@ int GigaVoxelsRenderer::enqueue_uploads() {
     if (launch_node_patch_staged(d_def_patches_, d_def_counts_ + 1, def_patch_cap_, t.nodes, t.dim, ctx_->d_status,
                                  ctx_->stream) != cudaSuccess)
         return VV_ERR_CUDA;
+    // the staging's generation, recorded as applied after its patches
+    if (launch_read_word(counts + 2, counts + 3, ctx_->stream) != cudaSuccess) return VV_ERR_CUDA;
     return VV_OK;
 }
 

@@ -171,7 +171,10 @@ private:
     bool deferred_ = false;
     uint4* h_def_jobs_ = nullptr;
     vv_node_patch* h_def_patches_ = nullptr;
-    uint32_t* h_def_counts_ = nullptr;   // [0] jobs, [1] patches
+    // [0] jobs, [1] patches, [2] the staging's generation (host), [3] the
+    // generation the device last applied (written by the enqueued work)
+    volatile uint32_t* h_def_counts_ = nullptr;
+    uint32_t stage_gen_ = 0;
     // their device copies, pulled at the start of each enqueue
     uint4* d_def_jobs_ = nullptr;
     vv_node_patch* d_def_patches_ = nullptr;
