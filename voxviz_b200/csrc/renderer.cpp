@@ -706,7 +706,7 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
     if (dd_.unique_cap < ids) {
         if (dd_.unique) cudaFree(dd_.unique);
         dd_.unique = nullptr;
-        dd_.unique_cap = std::max(ids, 2 * dd_.unique_cap);
+        dd_.unique_cap = std::max(ids + ids / 4, 2 * dd_.unique_cap);  // headroom: counts vary a little
         if (cudaMalloc((void**)&dd_.unique, dd_.unique_cap * 4) != cudaSuccess) return VV_ERR_OOM;
     }
     const int* pd = tree_->pool_dim();
@@ -724,7 +724,7 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
         if (order_.cand_cap < ids) {
             if (order_.cand) cudaFree(order_.cand);
             order_.cand = nullptr;
-            order_.cand_cap = std::max(ids, 2 * order_.cand_cap);
+            order_.cand_cap = std::max(ids + ids / 4, 2 * order_.cand_cap);
             if (cudaMalloc((void**)&order_.cand, order_.cand_cap * 4) != cudaSuccess) {
                 order_.cand_cap = 0;
                 return VV_ERR_OOM;
@@ -759,7 +759,7 @@ int GigaVoxelsRenderer::update_device(uint32_t n, std::vector<uint32_t>& upload,
         if (h_cand_cap_ < ids) {
             if (h_cand_) cudaFreeHost(h_cand_);
             h_cand_ = nullptr;
-            h_cand_cap_ = std::max(ids, 2 * h_cand_cap_);
+            h_cand_cap_ = std::max(ids + ids / 4, 2 * h_cand_cap_);
             if (cudaHostAlloc((void**)&h_cand_, h_cand_cap_ * 4, cudaHostAllocMapped) != cudaSuccess) {
                 h_cand_cap_ = 0;
                 return VV_ERR_OOM;
