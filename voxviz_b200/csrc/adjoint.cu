@@ -268,11 +268,13 @@ __global__ void __launch_bounds__(128, 7) forward_ckpt_kernel(const __grid_const
     hdr[pix] = make_int2(vis.count, s.nsamples);
 }
 
-// 7 resident CTAs per SM (72 registers): the occupancy that measured
-// fastest for the walk.  F64: binary64 gradient rows; WSUM: the lanes of a
-// cell summed before the atomics (scatter_texels).
+// 6 resident CTAs per SM (80 registers, fewer spills): on the paged 1080p
+// frames 5.73-5.78 ms against 5.83-6.02 at 7 CTAs and 6.18-6.21 at 8 (the
+// atomics' contention, not the walk's latency, bounds it).  F64: binary64
+// gradient rows; WSUM: the lanes of a cell summed before the atomics
+// (scatter_texels).
 template <int FMT, bool F64, bool WSUM>
-__global__ void __launch_bounds__(128, 7) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
+__global__ void __launch_bounds__(128, 6) backward_kernel(const __grid_constant__ RaycastParams p, const int2* hdr,
                                                        const Ckpt* ckpt, int per_ray, const float4* dl_dcolor,
                                                        const GradTarget gt) {
     int px, py;
