@@ -429,6 +429,44 @@ def raycast_mode_ab(ctx, us, reps=2):
             "last_frame_bitexact": same}
 
 
+def compaction_ab(ctx, us, reps=2):
+    """The selection + histopyramid + compaction of the given frames (on the
+    current pools, after their ray cast) launched both ways - three launches
+    (compact.cu) and one launch per pyramid level - each timed with CUDA
+    events (vv_render's profiling events); both must give the same mask and
+    requests."""
+    import torch
+
+    import voxviz_b200 as vv
+
+    W, H = us[0].width, us[0].height
+    dev = torch.device("cuda", torch.cuda.current_device())
+    use = torch.empty((H, W, 12), dtype=torch.int32, device=dev)
+    out = {m: (torch.empty((H, W), dtype=torch.int32, device=dev), torch.empty((W * H, 4), dtype=torch.int32, device=dev),
+               torch.zeros(1, dtype=torch.int32, device=dev)) for m in ("three_launch", "per_level")}
+    ctx.set_profiling(True)
+    ms = {}
+    for name in ("three_launch", "per_level"):
+        ctx.set_compaction(per_level=name == "per_level")
+        mask, req, cnt = out[name]
+        t = []
+        for rep in range(reps + 1):
+            for u in us:
+                ctx.render(u, usage=use.data_ptr(), mask=mask.data_ptr(), requests=req.data_ptr(),
+                           request_count=cnt.data_ptr(), request_cap=W * H, passes=vv.VV_PASS_ALL)
+                _, b = ctx.last_times()
+                if rep:
+                    t.append(b)
+        ms[name] = float(np.mean(t))
+    ctx.set_compaction(per_level=False)
+    ctx.set_profiling(False)
+    a, b = out["three_launch"], out["per_level"]
+    n = int(a[2].item())
+    same = bool(torch.equal(a[0], b[0]) and n == int(b[2].item()) and torch.equal(a[1][:n], b[1][:n]))
+    return {"compact_ms_three_launch": round(ms["three_launch"], 4), "compact_ms_per_level": round(ms["per_level"], 4),
+            "frames": len(us), "reps": reps, "last_frame_equal": same}
+
+
 BATCH16_VIEWS, BATCH16_POOL_BYTES = 16, 8_324_000_000
 
 
@@ -614,6 +652,7 @@ def run_ours(args):
                                               roofline["issue"]["peak_ginst_s"], 4)
     fb = fwd_bwd_leg(ctx, timed_u[-16:], min(16, args.steps), peak)
     ab = raycast_mode_ab(ctx, timed_u)
+    cab = compaction_ab(ctx, timed_u)
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
@@ -639,6 +678,7 @@ def run_ours(args):
                    "resident": r.stats()["resident_bricks"], "pool_slots": r.stats()["pool_slots"]},
         "fwd_bwd": fb,
         "raycast_launch_ab": ab,
+        "compaction_ab": cab,
         "clocks": clk, "gpu_launches": None, "setup_s": round(setup_s, 1),
         "terrain_build": {"where": "gpu", "seconds": round(build_s, 2)},
     }

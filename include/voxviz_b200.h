@@ -279,6 +279,16 @@ int vv_ctx_set_profiling(vv_ctx* ctx, int32_t on);
 #define VV_RAYCAST_REFILL 1
 #define VV_RAYCAST_STAGED 2
 int vv_ctx_set_raycast_mode(vv_ctx* ctx, int32_t mode);
+/* How vv_render's selection + histopyramid + compaction are launched; the
+ * results are the same.  VV_COMPACT_FUSED (default): three launches (the
+ * selection and the pyramid's lowest five levels per 32x32-pixel node, the
+ * levels above in one CTA, then the offsets down and the compaction), for
+ * frames with at least 7 pyramid levels and at most 16384 level-5 nodes,
+ * else the per-level form.  VV_COMPACT_PER_LEVEL: one launch per pyramid
+ * level each way (GenerateHistoPyramid.frag's passes). */
+#define VV_COMPACT_FUSED 0
+#define VV_COMPACT_PER_LEVEL 1
+int vv_ctx_set_compaction(vv_ctx* ctx, int32_t mode);
 int vv_ctx_last_times(vv_ctx* ctx, float* raycast_ms, float* compact_ms);
 /* Footprint of one draw: the number of distinct node-pool entries and
  * brick-pool slots the ray cast of `u` reads (a counting variant of the same

@@ -51,3 +51,33 @@ def test_request_set_covers_all_kept_items(g):
     assert got_set <= kept
     # with 12 pushes an entry keeps the last 4 pushed items of its pixel (FIFO overwrite)
     assert got_set == kept
+
+
+@pytest.mark.parametrize("w,h,cap", [(64, 64, 0), (65, 65, 0), (127, 95, 0), (129, 1, 0), (2047, 3, 0), (97, 191, 0),
+                                     (640, 480, 0), (1920, 1080, 5000), (1023, 767, 0)])
+def test_three_launch_compaction_equals_per_level(g, w, h, cap):
+    """vv_ctx_set_compaction: the three-launch form (selection and the
+    pyramid's lowest five levels per level-5 node, the levels above in one
+    CTA, offsets down and compaction per node) gives the mask, count and
+    requests of the per-level passes, on sizes whose levels fold rows and
+    columns; the first sizes also against the oracle."""
+    sc, gs = g
+    u = sc.uniforms(sc.view(7, w, h))
+    kw = {"max_push": 8}
+    if cap:
+        kw["cap"] = cap
+    fused = gs.render(u, **kw)
+    gs.ctx.set_compaction(per_level=True)
+    try:
+        per_level = gs.render(u, **kw)
+    finally:
+        gs.ctx.set_compaction(per_level=False)
+    for k in ("mask", "requests"):
+        assert np.array_equal(fused[k], per_level[k]), k
+    assert fused["count"] == per_level["count"]
+    assert fused["status"] == per_level["status"] == 0
+    if w * h <= 128 * 128:
+        ref = helpers.oracle_frame(u, sc.oracle_scene(), **kw)
+        assert np.array_equal(fused["mask"], ref["mask"])
+        assert fused["count"] == ref["count"]
+        assert np.array_equal(fused["requests"], ref["requests"])

@@ -387,6 +387,13 @@ class Context:
             m = int(mode)
         self._ck(lib().vv_ctx_set_raycast_mode(self._h, m), "raycast mode")
 
+    def set_compaction(self, per_level: bool) -> None:
+        """vv_ctx_set_compaction: the selection + histopyramid + compaction in
+        three launches (default) or one launch per pyramid level (same
+        results)."""
+        self._ck(lib().vv_ctx_set_compaction(self._h, N.VV_COMPACT_PER_LEVEL if per_level else N.VV_COMPACT_FUSED),
+                 "compaction mode")
+
     def set_profiling(self, on: bool = True) -> None:
         self._ck(lib().vv_ctx_set_profiling(self._h, 1 if on else 0), "profiling")
 

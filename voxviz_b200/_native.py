@@ -244,6 +244,7 @@ class GradDesc(C.Structure):
 
 VV_GRAD_F64, VV_GRAD_WARP_SUM, VV_GRAD_SPREAD, VV_GRAD_SPREAD_KEEP = 1, 2, 4, 8
 VV_RAYCAST_TILES, VV_RAYCAST_REFILL, VV_RAYCAST_STAGED = 0, 1, 2
+VV_COMPACT_FUSED, VV_COMPACT_PER_LEVEL = 0, 1
 
 
 class BatchView(C.Structure):
@@ -296,6 +297,7 @@ SIGNATURES = {
     "vv_compact_requests_noalloc": (C.c_int, [P, P, C.c_int32, C.c_int32, P, P, C.c_int32, C.c_int32, P]),
     "vv_ctx_set_profiling": (C.c_int, [P, C.c_int32]),
     "vv_ctx_set_raycast_mode": (C.c_int, [P, C.c_int32]),
+    "vv_ctx_set_compaction": (C.c_int, [P, C.c_int32]),
     "vv_ckpt_bytes": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "vv_render_forward_ckpt": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32]),
     "vv_backward": (C.c_int, [P, C.c_int32, C.POINTER(Uniforms), P, P, C.c_int32, P]),

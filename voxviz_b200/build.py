@@ -25,9 +25,10 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 HOST_CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
 
-CU_SOURCES = ["kernels.cu", "ctx.cu", "noalloc.cu", "production.cu", "adjoint.cu", "batch.cu", "builder.cu"]
+CU_SOURCES = ["kernels.cu", "ctx.cu", "noalloc.cu", "production.cu", "adjoint.cu", "batch.cu", "builder.cu",
+              "compact.cu"]
 CPP_SOURCES = ["terrain.cpp", "octree.cpp", "gradients.cpp", "gvfile.cpp", "renderer.cpp", "scene.cpp", "capi.cpp"]
-HEADERS = ["kernels.cuh", "cellmask.cuh", "ctx.h", "terrain.h", "octree.h", "gvfile.h", "scene.h", "handles.h", "renderer.h", "production.h", "raycast_common.cuh",
+HEADERS = ["kernels.cuh", "cellmask.cuh", "select.cuh", "compact.h", "dxt.h", "ctx.h", "terrain.h", "octree.h", "gvfile.h", "scene.h", "handles.h", "renderer.h", "production.h", "raycast_common.cuh",
            "lod_bound.h", "gradients.h", "fixed_div.h"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,298 @@
+// compact.cu - the page-request compaction in three launches.
+//
+// GenerateSelectionMask.frag, GenerateHistoPyramid.frag and
+// CompressNodeUsageList.frag (GigaVoxelsRenderer.cpp:1937-2135) as the
+// per-level kernels of kernels.cu run them: a histopyramid whose levels halve
+// the frame (a level of odd size folds its last row / column into the last
+// parent), counts summed upwards, exclusive offsets handed downwards in each
+// parent's child order, and every selected pixel's entries written at its
+// offset.  Here the pyramid is cut at level 5:
+//   tile_up_kernel   one CTA per level-5 node: the selection of the pixels
+//                    under it (written to the mask) and the counts of its
+//                    subtree up to the node, in shared memory;
+//   top_kernel       one CTA: the pyramid above level 5, counts up and
+//                    offsets down, and the request count;
+//   tile_down_kernel one CTA per level-5 node: its subtree's counts again
+//                    (from the mask), the offsets down from the node's, and
+//                    the compaction of its pixels.
+// The pixels under a level-k node form a rectangle: a node range [a, b) at
+// level k+1 covers [2a, 2b) at level k, extended to the level's width when
+// b is the level-(k+1) width (the fold).  Same parents, same child order,
+// same sums: the offsets, and so the request order, equal the per-level
+// kernels' (integer arithmetic).
+#include <algorithm>
+
+#include "compact.h"
+#include "select.cuh"
+
+namespace vv {
+namespace {
+
+constexpr int kCut = 5;              // the level whose nodes the tile kernels own
+constexpr int kFoot = 2 << kCut;     // at most 2^(kCut+1) - 1 cells per axis under one node, at level 0
+constexpr int kTileThreads = 256;
+constexpr int kTopThreads = 1024;
+constexpr int kTopMaxCells = 16384;  // level-5 nodes one top CTA takes (with the levels above)
+
+struct Levels {
+    int n;                 // levels in the pyramid
+    int w[24], h[24];
+};
+
+// Children of parent (X, Y) at the finer level (w, h), in the order the
+// compaction walks them: the 2x2 block, then for an odd last row (x, y+2),
+// (x+1, y+2) and for an odd last column the (x+2, *) cells.
+__device__ __forceinline__ int children(int X, int Y, int w, int h, int* cx, int* cy) {
+    const int x = 2 * X, y = 2 * Y;
+    int n = 0;
+    cx[n] = x; cy[n++] = y;
+    cx[n] = x + 1; cy[n++] = y;
+    cx[n] = x; cy[n++] = y + 1;
+    cx[n] = x + 1; cy[n++] = y + 1;
+    if (y + 2 == h - 1) {
+        cx[n] = x; cy[n++] = y + 2;
+        cx[n] = x + 1; cy[n++] = y + 2;
+        if (x + 2 == w - 1) {
+            cx[n] = x + 2; cy[n++] = y + 2;
+            cx[n] = x + 2; cy[n++] = y + 1;
+            cx[n] = x + 2; cy[n++] = y;
+        }
+    } else if (x + 2 == w - 1) {
+        cx[n] = x + 2; cy[n++] = y + 1;
+        cx[n] = x + 2; cy[n++] = y;
+    }
+    return n;
+}
+
+// The subtree of level-kCut node (X, Y): its node rectangle at every level
+// k <= kCut, [x0[k], x1[k]) x [y0[k], y1[k]), and where level k's cells sit
+// in the shared arrays (base[k], row pitch x1[k] - x0[k]).
+struct Subtree {
+    int x0[kCut + 1], x1[kCut + 1], y0[kCut + 1], y1[kCut + 1];
+    int base[kCut + 2];
+};
+
+__device__ __forceinline__ void subtree(const Levels& L, int X, int Y, Subtree& t) {
+    t.x0[kCut] = X;
+    t.x1[kCut] = X + 1;
+    t.y0[kCut] = Y;
+    t.y1[kCut] = Y + 1;
+    for (int k = kCut - 1; k >= 0; --k) {
+        t.x0[k] = 2 * t.x0[k + 1];
+        t.x1[k] = t.x1[k + 1] == L.w[k + 1] ? L.w[k] : 2 * t.x1[k + 1];
+        t.y0[k] = 2 * t.y0[k + 1];
+        t.y1[k] = t.y1[k + 1] == L.h[k + 1] ? L.h[k] : 2 * t.y1[k + 1];
+    }
+    t.base[0] = 0;
+    for (int k = 0; k <= kCut; ++k) t.base[k + 1] = t.base[k] + (t.x1[k] - t.x0[k]) * (t.y1[k] - t.y0[k]);
+}
+
+// cells of a subtree at levels 0..kCut: at most the sum of kFoot^2 / 4^k
+constexpr int kSubtreeCells = kFoot * kFoot + (kFoot / 2) * (kFoot / 2) + (kFoot / 4) * (kFoot / 4) +
+                              (kFoot / 8) * (kFoot / 8) + (kFoot / 16) * (kFoot / 16) + 4 + 1;
+
+__device__ __forceinline__ uint32_t sub_cell(const uint32_t* a, const Subtree& t, int k, int x, int y) {
+    if (x < t.x0[k] || x >= t.x1[k] || y < t.y0[k] || y >= t.y1[k]) return 0u;  // outside the level
+    return a[t.base[k] + (y - t.y0[k]) * (t.x1[k] - t.x0[k]) + (x - t.x0[k])];
+}
+
+// counts of levels 1..kCut of the subtree from level 0's (in cnt)
+__device__ __forceinline__ void sweep_up(const Levels& L, const Subtree& t, uint32_t* cnt) {
+    for (int k = 0; k < kCut; ++k) {
+        const int w = t.x1[k + 1] - t.x0[k + 1], n = w * (t.y1[k + 1] - t.y0[k + 1]);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int X = t.x0[k + 1] + i % w, Y = t.y0[k + 1] + i / w;
+            int cx[9], cy[9];
+            const int m = children(X, Y, L.w[k], L.h[k], cx, cy);
+            uint32_t sum = 0u;
+            for (int j = 0; j < m; ++j) sum += sub_cell(cnt, t, k, cx[j], cy[j]);
+            cnt[t.base[k + 1] + i] = sum;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kTileThreads) tile_up_kernel(const __grid_constant__ Levels L,
+                                                                const uint4* __restrict__ usage,
+                                                                uint32_t* __restrict__ mask,
+                                                                uint32_t* __restrict__ cut_counts) {
+    __shared__ uint32_t cnt[kSubtreeCells];
+    __shared__ Subtree t;
+    const int X = blockIdx.x, Y = blockIdx.y;
+    if (threadIdx.x == 0) subtree(L, X, Y, t);
+    __syncthreads();
+    const int W = L.w[0], H = L.h[0];
+    const int w0 = t.x1[0] - t.x0[0], n0 = w0 * (t.y1[0] - t.y0[0]);
+    for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+        const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
+        const uint32_t bits = select_bits(usage, x, y, W, H);
+        mask[(size_t)y * W + x] = bits;
+        cnt[i] = bits != 0u ? 1u : 0u;
+    }
+    __syncthreads();
+    sweep_up(L, t, cnt);
+    if (threadIdx.x == 0) cut_counts[(size_t)Y * L.w[kCut] + X] = cnt[t.base[kCut]];
+}
+
+// The pyramid from level kCut up: counts, then offsets down to level kCut.
+// Shared arrays: counts and offsets of levels kCut..n-1, one after another.
+__global__ void __launch_bounds__(kTopThreads) top_kernel(const __grid_constant__ Levels L,
+                                                           const uint32_t* __restrict__ cut_counts,
+                                                           uint32_t* __restrict__ cut_offsets,
+                                                           uint32_t* __restrict__ request_count) {
+    extern __shared__ uint32_t sm[];
+    int base[25];
+    base[kCut] = 0;
+    for (int k = kCut; k < L.n; ++k) base[k + 1] = base[k] + L.w[k] * L.h[k];
+    uint32_t* cnt = sm;
+    uint32_t* off = sm + base[L.n];
+    const int n_cut = L.w[kCut] * L.h[kCut];
+    for (int i = threadIdx.x; i < n_cut; i += blockDim.x) cnt[i] = cut_counts[i];
+    __syncthreads();
+    for (int k = kCut; k + 1 < L.n; ++k) {
+        const int cw = L.w[k + 1], n = cw * L.h[k + 1];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            int cx[9], cy[9];
+            const int m = children(i % cw, i / cw, L.w[k], L.h[k], cx, cy);
+            uint32_t sum = 0u;
+            for (int j = 0; j < m; ++j)
+                if (cx[j] < L.w[k] && cy[j] < L.h[k]) sum += cnt[base[k] + cy[j] * L.w[k] + cx[j]];
+            cnt[base[k + 1] + i] = sum;
+        }
+        __syncthreads();
+    }
+    const int top = L.n - 1;
+    if (threadIdx.x == 0) {
+        off[base[top]] = 0u;
+        if (request_count) *request_count = cnt[base[top]];
+    }
+    __syncthreads();
+    for (int k = top - 1; k >= kCut; --k) {
+        const int w = L.w[k], n = w * L.h[k], cw = L.w[k + 1], ch = L.h[k + 1];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int x = i % w, y = i / w;
+            const int X = min(x >> 1, cw - 1), Y = min(y >> 1, ch - 1);
+            int cx[9], cy[9];
+            const int m = children(X, Y, w, L.h[k], cx, cy);
+            uint32_t o = off[base[k + 1] + Y * cw + X];
+            for (int j = 0; j < m; ++j) {
+                if (cx[j] == x && cy[j] == y) break;
+                if (cx[j] < w && cy[j] < L.h[k]) o += cnt[base[k] + cy[j] * w + cx[j]];
+            }
+            off[base[k] + i] = o;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n_cut; i += blockDim.x) cut_offsets[i] = off[i];
+}
+
+struct TileDown {
+    Levels L;
+    const uint4* usage;
+    const uint32_t* mask;
+    const uint32_t* cut_offsets;
+    uint32_t* requests;
+    int cap;
+    int max_push;
+};
+
+__global__ void __launch_bounds__(kTileThreads) tile_down_kernel(const __grid_constant__ TileDown p) {
+    __shared__ uint32_t cnt[kSubtreeCells];
+    __shared__ uint32_t off[kSubtreeCells];
+    __shared__ Subtree t;
+    const Levels& L = p.L;
+    const int X = blockIdx.x, Y = blockIdx.y;
+    if (threadIdx.x == 0) subtree(L, X, Y, t);
+    __syncthreads();
+    const int W = L.w[0];
+    const int w0 = t.x1[0] - t.x0[0], n0 = w0 * (t.y1[0] - t.y0[0]);
+    for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+        const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
+        cnt[i] = p.mask[(size_t)y * W + x] != 0u ? 1u : 0u;
+    }
+    __syncthreads();
+    sweep_up(L, t, cnt);
+    if (threadIdx.x == 0) off[t.base[kCut]] = p.cut_offsets[(size_t)Y * L.w[kCut] + X];
+    __syncthreads();
+    for (int k = kCut - 1; k >= 0; --k) {
+        const int w = t.x1[k] - t.x0[k], n = w * (t.y1[k] - t.y0[k]);
+        const int cw = L.w[k + 1], ch = L.h[k + 1];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int x = t.x0[k] + i % w, y = t.y0[k] + i / w;
+            const int PX = min(x >> 1, cw - 1), PY = min(y >> 1, ch - 1);
+            int cx[9], cy[9];
+            const int m = children(PX, PY, L.w[k], L.h[k], cx, cy);
+            uint32_t o = off[t.base[k + 1] + (PY - t.y0[k + 1]) * (t.x1[k + 1] - t.x0[k + 1]) + (PX - t.x0[k + 1])];
+            for (int j = 0; j < m; ++j) {
+                if (cx[j] == x && cy[j] == y) break;
+                o += sub_cell(cnt, t, k, cx[j], cy[j]);
+            }
+            off[t.base[k] + i] = o;
+        }
+        __syncthreads();
+    }
+    // CompressNodeUsageList.frag (:107-149): the kept entries of each
+    // selected pixel, at most max_push, at the pixel's offset
+    if (!p.requests || p.cap <= 0) return;
+    for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+        const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
+        const size_t pix = (size_t)y * W + x;
+        uint32_t bits = p.mask[pix];
+        if (bits == 0u) continue;
+        const uint32_t rank = off[i];
+        if (rank >= (uint32_t)p.cap) continue;
+        const uint4* o = p.usage + pix * 3;
+        const uint4 a = o[0], b = o[1], c = o[2];
+        const uint32_t list[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+        uint32_t out[4] = {0u, 0u, 0u, 0u};
+        int pushed = 0;
+        for (int item = 0; item < 12 && bits != 0u && pushed < p.max_push; ++item, bits >>= 1) {
+            if (bits & 1u) {
+                out[pushed & 3] = list[item];
+                ++pushed;
+            }
+        }
+        reinterpret_cast<uint4*>(p.requests)[rank] = make_uint4(out[0], out[1], out[2], out[3]);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_compact_fused(const CompactParams& p, uint32_t* mask, cudaStream_t s) {
+    if (p.levels <= kCut + 1 || p.levels > 24 || !mask) return cudaErrorNotSupported;
+    Levels L;
+    L.n = p.levels;
+    for (int k = 0; k < p.levels; ++k) {
+        L.w[k] = p.level_w[k];
+        L.h[k] = p.level_h[k];
+    }
+    const int n_cut = L.w[kCut] * L.h[kCut];
+    if (n_cut > kTopMaxCells) return cudaErrorNotSupported;
+    long long top_cells = 0;
+    for (int k = kCut; k < L.n; ++k) top_cells += (long long)L.w[k] * L.h[k];
+    const size_t top_bytes = (size_t)top_cells * 2 * sizeof(uint32_t);
+    if (top_bytes > 200 * 1024) return cudaErrorNotSupported;
+    if (top_bytes > 48 * 1024) {  // (on the current device; only frames above ~2.5 K x 2 K need it)
+        const cudaError_t e = cudaFuncSetAttribute(top_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)top_bytes);
+        if (e != cudaSuccess) return e;
+    }
+    // the per-level scratch of CompactParams: level-5 counts and offsets
+    uint32_t* cut_counts = p.counts;
+    uint32_t* cut_offsets = p.offsets;
+    const dim3 grid((unsigned)L.w[kCut], (unsigned)L.h[kCut]);
+    tile_up_kernel<<<grid, kTileThreads, 0, s>>>(L, p.usage, mask, cut_counts);
+    top_kernel<<<1, kTopThreads, top_bytes, s>>>(L, cut_counts, cut_offsets, p.request_count);
+    TileDown d;
+    d.L = L;
+    d.usage = p.usage;
+    d.mask = mask;
+    d.cut_offsets = cut_offsets;
+    d.requests = p.requests;
+    d.cap = p.cap;
+    d.max_push = p.max_push;
+    tile_down_kernel<<<grid, kTileThreads, 0, s>>>(d);
+    return cudaGetLastError();
+}
+
+}  // namespace vv

@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "compact.h"
 #include "ctx.h"
 #include "dxt.h"
 #include "cellmask.cuh"
@@ -702,8 +703,8 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
         if (rc) return rc;
         mask = c->d_mask;
     }
-    VV_CUDA(c, launch_select(usage, mask, c->d_counts, W, H, c->stream));
     if (!(passes & VV_PASS_COMPACT)) {
+        VV_CUDA(c, launch_select(usage, mask, c->d_counts, W, H, c->stream));
         if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
         return VV_OK;
     }
@@ -715,8 +716,22 @@ int vv_render(vv_ctx* c, int32_t tree, const vv_uniforms* u, const vv_frame_out*
     cp.request_count = out->request_count;
     cp.cap = out->requests ? out->request_cap : 0;
     cp.max_push = out->compress_max_push > 0 ? out->compress_max_push : 4;
-    VV_CUDA(c, launch_compact(cp, c->stream));
+    // three launches where the frame allows (compact.cu), else one per level
+    const cudaError_t fe = c->per_level_compaction ? cudaErrorNotSupported : launch_compact_fused(cp, mask, c->stream);
+    if (fe == cudaErrorNotSupported) {
+        VV_CUDA(c, launch_select(usage, mask, c->d_counts, W, H, c->stream));
+        VV_CUDA(c, launch_compact(cp, c->stream));
+    } else {
+        VV_CUDA(c, fe);
+    }
     if (c->profiling) VV_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
+    return VV_OK;
+}
+
+int vv_ctx_set_compaction(vv_ctx* c, int32_t mode) {
+    if (!c || (mode != VV_COMPACT_FUSED && mode != VV_COMPACT_PER_LEVEL))
+        return fail(c, VV_ERR_ARG, "unknown compaction mode");
+    c->per_level_compaction = mode == VV_COMPACT_PER_LEVEL;
     return VV_OK;
 }
 

@@ -87,6 +87,8 @@ struct vv_ctx {
     float4* d_spread = nullptr;
     size_t spread_elems = 0;
     long long spread_rows_kept = 0;  // rows per copy of sums kept by VV_GRAD_SPREAD_KEEP, else 0
+    // compaction in one launch per pyramid level instead of compact.cu's three
+    bool per_level_compaction = false;
     // ray-cast form (VV_RAYCAST_TILES / VV_RAYCAST_REFILL) and the refill
     // form's tile counter
     int raycast_mode = 0;
