@@ -41,28 +41,33 @@ struct Levels {
 
 // Children of parent (X, Y) at the finer level (w, h), in the order the
 // compaction walks them: the 2x2 block, then for an odd last row (x, y+2),
-// (x+1, y+2) and for an odd last column the (x+2, *) cells.
-__device__ __forceinline__ int children(int X, int Y, int w, int h, int* cx, int* cy) {
-    const int x = 2 * X, y = 2 * Y;
-    int n = 0;
-    cx[n] = x; cy[n++] = y;
-    cx[n] = x + 1; cy[n++] = y;
-    cx[n] = x; cy[n++] = y + 1;
-    cx[n] = x + 1; cy[n++] = y + 1;
-    if (y + 2 == h - 1) {
-        cx[n] = x; cy[n++] = y + 2;
-        cx[n] = x + 1; cy[n++] = y + 2;
-        if (x + 2 == w - 1) {
-            cx[n] = x + 2; cy[n++] = y + 2;
-            cx[n] = x + 2; cy[n++] = y + 1;
-            cx[n] = x + 2; cy[n++] = y;
-        }
-    } else if (x + 2 == w - 1) {
-        cx[n] = x + 2; cy[n++] = y + 1;
-        cx[n] = x + 2; cy[n++] = y;
+// (x+1, y+2) and for an odd last column the (x+2, *) cells.  Child j is
+// computed from j (no arrays: registers only).
+struct Kids {
+    int x, y, n;
+    bool row, col;  // the parent takes the odd last row / column
+    __device__ __forceinline__ Kids(int X, int Y, int w, int h) {
+        x = 2 * X;
+        y = 2 * Y;
+        row = y + 2 == h - 1;
+        col = x + 2 == w - 1;
+        n = 4 + (row ? 2 : 0) + (col ? (row ? 3 : 2) : 0);
     }
-    return n;
-}
+    __device__ __forceinline__ void at(int j, int& cx, int& cy) const {
+        if (j < 4) {
+            cx = x + (j & 1);
+            cy = y + (j >> 1);
+        } else if (row && j < 6) {
+            cx = x + (j - 4);
+            cy = y + 2;
+        } else {
+            // the column cells, bottom up: (x+2, y+2) after a folded row, then (x+2, y+1), (x+2, y)
+            const int r = j - (row ? 6 : 4);
+            cx = x + 2;
+            cy = y + (row ? 2 : 1) - r;
+        }
+    }
+};
 
 // The subtree of level-kCut node (X, Y): its node rectangle at every level
 // k <= kCut, [x0[k], x1[k]) x [y0[k], y1[k]), and where level k's cells sit
@@ -96,19 +101,45 @@ __device__ __forceinline__ uint32_t sub_cell(const uint32_t* a, const Subtree& t
     return a[t.base[k] + (y - t.y0[k]) * (t.x1[k] - t.x0[k]) + (x - t.x0[k])];
 }
 
-// counts of levels 1..kCut of the subtree from level 0's (in cnt)
-__device__ __forceinline__ void sweep_up(const Levels& L, const Subtree& t, uint32_t* cnt) {
-    for (int k = 0; k < kCut; ++k) {
-        const int w = t.x1[k + 1] - t.x0[k + 1], n = w * (t.y1[k + 1] - t.y0[k + 1]);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int X = t.x0[k + 1] + i % w, Y = t.y0[k + 1] + i / w;
-            int cx[9], cy[9];
-            const int m = children(X, Y, L.w[k], L.h[k], cx, cy);
-            uint32_t sum = 0u;
-            for (int j = 0; j < m; ++j) sum += sub_cell(cnt, t, k, cx[j], cy[j]);
-            cnt[t.base[k + 1] + i] = sum;
+__device__ __forceinline__ int level_cells(const Subtree& t, int k) {
+    return (t.x1[k] - t.x0[k]) * (t.y1[k] - t.y0[k]);
+}
+
+// The upper levels of a subtree hold few cells: from the first level (going
+// up) with at most kWarpCells cells one warp does the rest, with warp
+// barriers only.
+constexpr int kWarpCells = 64;
+
+// Level k+1 of the subtree's counts from level k's (cells i = first, first
+// + step, ...).
+__device__ __forceinline__ void up_level(const Levels& L, const Subtree& t, uint32_t* cnt, int k, int first,
+                                         int step) {
+    const int w = t.x1[k + 1] - t.x0[k + 1], n = level_cells(t, k + 1);
+    for (int i = first; i < n; i += step) {
+        const Kids kids(t.x0[k + 1] + i % w, t.y0[k + 1] + i / w, L.w[k], L.h[k]);
+        uint32_t sum = 0u;
+        for (int j = 0; j < kids.n; ++j) {
+            int cx, cy;
+            kids.at(j, cx, cy);
+            sum += sub_cell(cnt, t, k, cx, cy);
         }
+        cnt[t.base[k + 1] + i] = sum;
+    }
+}
+
+// counts of levels 1..kCut of the subtree from level 0's (in cnt); on
+// return warp 0 has every level, the other warps the block-swept ones
+__device__ __forceinline__ void sweep_up(const Levels& L, const Subtree& t, uint32_t* cnt) {
+    int k = 0;
+    for (; k < kCut && level_cells(t, k + 1) > kWarpCells; ++k) {
+        up_level(L, t, cnt, k, threadIdx.x, blockDim.x);
         __syncthreads();
+    }
+    if (threadIdx.x < 32) {
+        for (; k < kCut; ++k) {
+            up_level(L, t, cnt, k, threadIdx.x, 32);
+            __syncwarp();
+        }
     }
 }
 
@@ -152,11 +183,13 @@ __global__ void __launch_bounds__(kTopThreads) top_kernel(const __grid_constant_
     for (int k = kCut; k + 1 < L.n; ++k) {
         const int cw = L.w[k + 1], n = cw * L.h[k + 1];
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            int cx[9], cy[9];
-            const int m = children(i % cw, i / cw, L.w[k], L.h[k], cx, cy);
+            const Kids kids(i % cw, i / cw, L.w[k], L.h[k]);
             uint32_t sum = 0u;
-            for (int j = 0; j < m; ++j)
-                if (cx[j] < L.w[k] && cy[j] < L.h[k]) sum += cnt[base[k] + cy[j] * L.w[k] + cx[j]];
+            for (int j = 0; j < kids.n; ++j) {
+                int cx, cy;
+                kids.at(j, cx, cy);
+                if (cx < L.w[k] && cy < L.h[k]) sum += cnt[base[k] + cy * L.w[k] + cx];
+            }
             cnt[base[k + 1] + i] = sum;
         }
         __syncthreads();
@@ -167,23 +200,46 @@ __global__ void __launch_bounds__(kTopThreads) top_kernel(const __grid_constant_
         if (request_count) *request_count = cnt[base[top]];
     }
     __syncthreads();
+    // offsets down, per parent: each child gets the parent's offset plus the
+    // counts of the children before it
     for (int k = top - 1; k >= kCut; --k) {
-        const int w = L.w[k], n = w * L.h[k], cw = L.w[k + 1], ch = L.h[k + 1];
+        const int w = L.w[k], cw = L.w[k + 1], n = cw * L.h[k + 1];
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int x = i % w, y = i / w;
-            const int X = min(x >> 1, cw - 1), Y = min(y >> 1, ch - 1);
-            int cx[9], cy[9];
-            const int m = children(X, Y, w, L.h[k], cx, cy);
-            uint32_t o = off[base[k + 1] + Y * cw + X];
-            for (int j = 0; j < m; ++j) {
-                if (cx[j] == x && cy[j] == y) break;
-                if (cx[j] < w && cy[j] < L.h[k]) o += cnt[base[k] + cy[j] * w + cx[j]];
+            const Kids kids(i % cw, i / cw, w, L.h[k]);
+            uint32_t o = off[base[k + 1] + i];
+            for (int j = 0; j < kids.n; ++j) {
+                int cx, cy;
+                kids.at(j, cx, cy);
+                if (cx >= w || cy >= L.h[k]) continue;
+                const int c = base[k] + cy * w + cx;
+                off[c] = o;
+                o += cnt[c];
             }
-            off[base[k] + i] = o;
         }
         __syncthreads();
     }
     for (int i = threadIdx.x; i < n_cut; i += blockDim.x) cut_offsets[i] = off[i];
+}
+
+// Level k of the subtree's offsets from level k+1's: each parent (i = first,
+// first + step, ...) hands its offset plus the counts of the children before
+// each child down.
+__device__ __forceinline__ void down_level(const Levels& L, const Subtree& t, const uint32_t* cnt, uint32_t* off,
+                                           int k, int first, int step) {
+    const int pw = t.x1[k + 1] - t.x0[k + 1], n = level_cells(t, k + 1);
+    const int w = t.x1[k] - t.x0[k];
+    for (int i = first; i < n; i += step) {
+        const Kids kids(t.x0[k + 1] + i % pw, t.y0[k + 1] + i / pw, L.w[k], L.h[k]);
+        uint32_t o = off[t.base[k + 1] + i];
+        for (int j = 0; j < kids.n; ++j) {
+            int cx, cy;
+            kids.at(j, cx, cy);
+            if (cx >= L.w[k] || cy >= L.h[k]) continue;
+            const int c = t.base[k] + (cy - t.y0[k]) * w + (cx - t.x0[k]);
+            off[c] = o;
+            o += cnt[c];
+        }
+    }
 }
 
 struct TileDown {
@@ -214,21 +270,21 @@ __global__ void __launch_bounds__(kTileThreads) tile_down_kernel(const __grid_co
     sweep_up(L, t, cnt);
     if (threadIdx.x == 0) off[t.base[kCut]] = p.cut_offsets[(size_t)Y * L.w[kCut] + X];
     __syncthreads();
-    for (int k = kCut - 1; k >= 0; --k) {
-        const int w = t.x1[k] - t.x0[k], n = w * (t.y1[k] - t.y0[k]);
-        const int cw = L.w[k + 1], ch = L.h[k + 1];
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int x = t.x0[k] + i % w, y = t.y0[k] + i / w;
-            const int PX = min(x >> 1, cw - 1), PY = min(y >> 1, ch - 1);
-            int cx[9], cy[9];
-            const int m = children(PX, PY, L.w[k], L.h[k], cx, cy);
-            uint32_t o = off[t.base[k + 1] + (PY - t.y0[k + 1]) * (t.x1[k + 1] - t.x0[k + 1]) + (PX - t.x0[k + 1])];
-            for (int j = 0; j < m; ++j) {
-                if (cx[j] == x && cy[j] == y) break;
-                o += sub_cell(cnt, t, k, cx[j], cy[j]);
-            }
-            off[t.base[k] + i] = o;
+    // offsets down, per parent (the children of a node of the subtree are
+    // in the subtree, or outside the level): the small upper levels by warp
+    // 0, which holds their counts, then the rest by the block
+    int k = kCut - 1;
+    if (threadIdx.x < 32) {
+        for (; k >= 0 && level_cells(t, k + 1) <= kWarpCells; --k) {
+            down_level(L, t, cnt, off, k, threadIdx.x, 32);
+            __syncwarp();
         }
+    }
+    __syncthreads();
+    k = kCut - 1;
+    while (k >= 0 && level_cells(t, k + 1) <= kWarpCells) --k;
+    for (; k >= 0; --k) {
+        down_level(L, t, cnt, off, k, threadIdx.x, blockDim.x);
         __syncthreads();
     }
     // CompressNodeUsageList.frag (:107-149): the kept entries of each
@@ -237,22 +293,30 @@ __global__ void __launch_bounds__(kTileThreads) tile_down_kernel(const __grid_co
     for (int i = threadIdx.x; i < n0; i += blockDim.x) {
         const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
         const size_t pix = (size_t)y * W + x;
-        uint32_t bits = p.mask[pix];
+        const uint32_t bits = p.mask[pix];
         if (bits == 0u) continue;
         const uint32_t rank = off[i];
         if (rank >= (uint32_t)p.cap) continue;
         const uint4* o = p.usage + pix * 3;
         const uint4 a = o[0], b = o[1], c = o[2];
         const uint32_t list[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
-        uint32_t out[4] = {0u, 0u, 0u, 0u};
+        // the kept entries in order, at most max_push, each into entry
+        // (pushed mod 4): the last four pushed stay (registers throughout)
+        uint32_t o0 = 0u, o1 = 0u, o2 = 0u, o3 = 0u;
         int pushed = 0;
-        for (int item = 0; item < 12 && bits != 0u && pushed < p.max_push; ++item, bits >>= 1) {
-            if (bits & 1u) {
-                out[pushed & 3] = list[item];
+#pragma unroll
+        for (int item = 0; item < 12; ++item) {
+            if (((bits >> item) & 1u) && pushed < p.max_push) {
+                const uint32_t v = list[item];
+                const int s = pushed & 3;
+                o0 = s == 0 ? v : o0;
+                o1 = s == 1 ? v : o1;
+                o2 = s == 2 ? v : o2;
+                o3 = s == 3 ? v : o3;
                 ++pushed;
             }
         }
-        reinterpret_cast<uint4*>(p.requests)[rank] = make_uint4(out[0], out[1], out[2], out[3]);
+        reinterpret_cast<uint4*>(p.requests)[rank] = make_uint4(o0, o1, o2, o3);
     }
 }
 
