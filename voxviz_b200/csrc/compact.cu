@@ -31,6 +31,7 @@ namespace {
 constexpr int kCut = 5;              // the level whose nodes the tile kernels own
 constexpr int kFoot = 2 << kCut;     // at most 2^(kCut+1) - 1 cells per axis under one node, at level 0
 constexpr int kTileThreads = 256;
+constexpr int kTile = 1 << kCut;     // pixels per axis under a level-kCut node without folds
 constexpr int kTopThreads = 1024;
 constexpr int kTopMaxCells = 16384;  // level-5 nodes one top CTA takes (with the levels above)
 
@@ -149,11 +150,31 @@ __global__ void __launch_bounds__(kTileThreads) tile_up_kernel(const __grid_cons
                                                                 uint32_t* __restrict__ cut_counts) {
     __shared__ uint32_t cnt[kSubtreeCells];
     __shared__ Subtree t;
+    __shared__ uint32_t wsum[kTileThreads / 32];
     const int X = blockIdx.x, Y = blockIdx.y;
     if (threadIdx.x == 0) subtree(L, X, Y, t);
     __syncthreads();
     const int W = L.w[0], H = L.h[0];
     const int w0 = t.x1[0] - t.x0[0], n0 = w0 * (t.y1[0] - t.y0[0]);
+    if (w0 == kTile && n0 == kTile * kTile) {
+        // no fold under this node: its count is a plain sum
+        uint32_t c = 0u;
+        for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+            const int x = t.x0[0] + (i & (kTile - 1)), y = t.y0[0] + i / kTile;
+            const uint32_t bits = select_bits(usage, x, y, W, H);
+            mask[(size_t)y * W + x] = bits;
+            c += bits != 0u ? 1u : 0u;
+        }
+        c = __reduce_add_sync(0xFFFFFFFFu, c);
+        if ((threadIdx.x & 31u) == 0u) wsum[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t s = 0u;
+            for (int w = 0; w < kTileThreads / 32; ++w) s += wsum[w];
+            cut_counts[(size_t)Y * L.w[kCut] + X] = s;
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < n0; i += blockDim.x) {
         const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
         const uint32_t bits = select_bits(usage, x, y, W, H);
@@ -242,6 +263,16 @@ __device__ __forceinline__ void down_level(const Levels& L, const Subtree& t, co
     }
 }
 
+// The position of x in a Morton index (the even bits).
+__device__ __forceinline__ int even_bits(uint32_t m) {
+    m &= 0x55555555u;
+    m = (m | (m >> 1)) & 0x33333333u;
+    m = (m | (m >> 2)) & 0x0F0F0F0Fu;
+    m = (m | (m >> 4)) & 0x00FF00FFu;
+    m = (m | (m >> 8)) & 0x0000FFFFu;
+    return (int)m;
+}
+
 struct TileDown {
     Levels L;
     const uint4* usage;
@@ -252,16 +283,80 @@ struct TileDown {
     int max_push;
 };
 
+// CompressNodeUsageList.frag (:107-149): the kept entries of a selected
+// pixel in order, at most max_push, each into entry (pushed mod 4) - the
+// last four pushed stay (registers throughout) - at the pixel's offset.
+__device__ __forceinline__ void write_request(const TileDown& p, size_t pix, uint32_t bits, uint32_t rank) {
+    if (rank >= (uint32_t)p.cap) return;
+    const uint4* o = p.usage + pix * 3;
+    const uint4 a = o[0], b = o[1], c = o[2];
+    const uint32_t list[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+    uint32_t o0 = 0u, o1 = 0u, o2 = 0u, o3 = 0u;
+    int pushed = 0;
+#pragma unroll
+    for (int item = 0; item < 12; ++item) {
+        if (((bits >> item) & 1u) && pushed < p.max_push) {
+            const uint32_t v = list[item];
+            const int s = pushed & 3;
+            o0 = s == 0 ? v : o0;
+            o1 = s == 1 ? v : o1;
+            o2 = s == 2 ? v : o2;
+            o3 = s == 3 ? v : o3;
+            ++pushed;
+        }
+    }
+    reinterpret_cast<uint4*>(p.requests)[rank] = make_uint4(o0, o1, o2, o3);
+}
+
 __global__ void __launch_bounds__(kTileThreads) tile_down_kernel(const __grid_constant__ TileDown p) {
     __shared__ uint32_t cnt[kSubtreeCells];
     __shared__ uint32_t off[kSubtreeCells];
     __shared__ Subtree t;
+    __shared__ uint32_t wtot[kTileThreads / 32];
     const Levels& L = p.L;
     const int X = blockIdx.x, Y = blockIdx.y;
     if (threadIdx.x == 0) subtree(L, X, Y, t);
     __syncthreads();
     const int W = L.w[0];
     const int w0 = t.x1[0] - t.x0[0], n0 = w0 * (t.y1[0] - t.y0[0]);
+    if (w0 == kTile && n0 == kTile * kTile) {
+        // no fold under this node: the order under it is the Morton order
+        // of its 32x32 pixels (children (x,y), (x+1,y), (x,y+1), (x+1,y+1)
+        // at every level), so a pixel's offset is the node's plus the
+        // selected pixels before it in that order - one block-wide scan.
+        // Thread i takes Morton indices 4i..4i+3.
+        constexpr int kPer = kTile * kTile / kTileThreads;
+        uint32_t bits[kPer];
+        size_t pix[kPer];
+        uint32_t c = 0u;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const uint32_t m = (uint32_t)(threadIdx.x * kPer + j);
+            pix[j] = (size_t)(t.y0[0] + even_bits(m >> 1)) * W + (size_t)(t.x0[0] + even_bits(m));
+            bits[j] = p.mask[pix[j]];
+            c += bits[j] != 0u ? 1u : 0u;
+        }
+        const unsigned lane = threadIdx.x & 31u;
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= (unsigned)d) incl += v;
+        }
+        if (lane == 31u) wtot[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        uint32_t r = p.cut_offsets[(size_t)Y * L.w[kCut] + X] + incl - c;
+        for (int w = 0; w < (int)(threadIdx.x >> 5); ++w) r += wtot[w];
+        if (!p.requests || p.cap <= 0) return;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            if (bits[j] != 0u) {
+                write_request(p, pix[j], bits[j], r);
+                ++r;
+            }
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < n0; i += blockDim.x) {
         const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
         cnt[i] = p.mask[(size_t)y * W + x] != 0u ? 1u : 0u;
@@ -287,36 +382,12 @@ __global__ void __launch_bounds__(kTileThreads) tile_down_kernel(const __grid_co
         down_level(L, t, cnt, off, k, threadIdx.x, blockDim.x);
         __syncthreads();
     }
-    // CompressNodeUsageList.frag (:107-149): the kept entries of each
-    // selected pixel, at most max_push, at the pixel's offset
     if (!p.requests || p.cap <= 0) return;
     for (int i = threadIdx.x; i < n0; i += blockDim.x) {
         const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
         const size_t pix = (size_t)y * W + x;
         const uint32_t bits = p.mask[pix];
-        if (bits == 0u) continue;
-        const uint32_t rank = off[i];
-        if (rank >= (uint32_t)p.cap) continue;
-        const uint4* o = p.usage + pix * 3;
-        const uint4 a = o[0], b = o[1], c = o[2];
-        const uint32_t list[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
-        // the kept entries in order, at most max_push, each into entry
-        // (pushed mod 4): the last four pushed stay (registers throughout)
-        uint32_t o0 = 0u, o1 = 0u, o2 = 0u, o3 = 0u;
-        int pushed = 0;
-#pragma unroll
-        for (int item = 0; item < 12; ++item) {
-            if (((bits >> item) & 1u) && pushed < p.max_push) {
-                const uint32_t v = list[item];
-                const int s = pushed & 3;
-                o0 = s == 0 ? v : o0;
-                o1 = s == 1 ? v : o1;
-                o2 = s == 2 ? v : o2;
-                o3 = s == 3 ? v : o3;
-                ++pushed;
-            }
-        }
-        reinterpret_cast<uint4*>(p.requests)[rank] = make_uint4(o0, o1, o2, o3);
+        if (bits != 0u) write_request(p, pix, bits, off[i]);
     }
 }
 
