@@ -104,6 +104,16 @@ public:
     }
     uint32_t word0(uint32_t n) const { return word0_[n]; }
     uint32_t word1(uint32_t n) const { return word1_[n]; }
+    // Start loading node n's records into the cache (the page-request
+    // service walks nodes in request order, far apart in these arrays).
+    void prefetch(uint32_t n) const {
+        __builtin_prefetch(&parent_[n]);
+        __builtin_prefetch(&word0_[n]);
+        __builtin_prefetch(&level_[n]);
+        __builtin_prefetch(&ci_[n]);
+        __builtin_prefetch(&cj_[n]);
+        __builtin_prefetch(&ck_[n]);
+    }
     size_t nonconst_count() const { return nonconst_; }
 
     // Words in reference texture order (2 per grid cell), no brick resident.

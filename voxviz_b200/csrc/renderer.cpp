@@ -626,11 +626,19 @@ int GigaVoxelsRenderer::flush_device() {
         }
         if (cudaHostGetDevicePointer((void**)&dh_fpatch_, h_fpatch_, 0) != cudaSuccess) return VV_ERR_CUDA;
     }
+    constexpr size_t kAhead = 16;  // records prefetched ahead (far apart in the arrays)
     for (size_t k = 0; k < n; ++k) {
+        if (k + kAhead < n) tree_->prefetch(pending_nodes_[keep_[k + kAhead]]);
         const uint32_t i = keep_[k];
         h_fjobs_[k] = production_job(pending_slots_[i], pending_nodes_[i]);
     }
     for (size_t k = 0; k < np; ++k) {
+        if (k + kAhead < np) {
+            const uint32_t f = touched_[k + kAhead];
+            __builtin_prefetch(&w0_[f]);
+            __builtin_prefetch(&w1_[f]);
+            __builtin_prefetch(&touched_mark_[f]);
+        }
         const uint32_t t = touched_[k];
         vv_node_patch& q = h_fpatch_[k];
         tree_->grid_of(t, q.x, q.y, q.z);
@@ -847,8 +855,27 @@ int GigaVoxelsRenderer::apply_policy(std::vector<uint32_t>& upload) {
     root_on_device_ = false;
     evict_hint_ = 2 * (uint32_t)upload.size() + 1;
     // BrickPool::update (GigaVoxelsBrickPool.cpp:561-682), including the
-    // upload of a non-resident non-constant parent (:629-673).
-    for (uint32_t nidx : upload) {
+    // upload of a non-resident non-constant parent (:629-673).  The records
+    // of the node kAhead uploads on, and of the parent of the one half as
+    // far, are prefetched: the nodes are far apart in the host arrays.
+    constexpr size_t kAhead = 16;
+    for (size_t i = 0; i < upload.size(); ++i) {
+        if (i + kAhead < upload.size()) {
+            const uint32_t f = upload[i + kAhead];
+            __builtin_prefetch(&node_slot_[f]);
+            __builtin_prefetch(&w0_[f]);
+            __builtin_prefetch(&w1_[f]);
+            __builtin_prefetch(&touched_mark_[f]);
+            tree_->prefetch(f);
+        }
+        if (i + kAhead / 2 < upload.size()) {
+            const uint32_t par = tree_->parent(upload[i + kAhead / 2]);
+            if (par != kNoParent) {
+                __builtin_prefetch(&node_slot_[par]);
+                tree_->prefetch(par);
+            }
+        }
+        const uint32_t nidx = upload[i];
         if (node_slot_[nidx] >= 0) continue;
         int rc = upload_nodes(nidx);
         if (rc) return rc;
