@@ -478,7 +478,7 @@ struct PathSlots {
 // Each warp owns one 10^3-texel RGBA8 slot copy in shared memory.  When the
 // lanes that reach a brick segment together share a slot (__match_any_sync),
 // the largest such group copies that slot's 4000 bytes with one
-// cp.async.bulk (global -> this CTA's shared memory, no multicast) and
+// cp.async.bulk (global -> this CTA's own shared memory) and
 // samples it from shared memory; other lanes read the pool as usual.
 //   state = tag << 32 | mask: tag = the slot the buffer holds (kNoSlot while
 //   a copy is in flight), mask = the lanes reading it.  A group joins a
