@@ -682,13 +682,14 @@ def run_ours(args):
         "clocks": clk, "gpu_launches": None, "setup_s": round(setup_s, 1),
         "terrain_build": {"where": "gpu", "seconds": round(build_s, 2)},
     }
-    # our kernels per step. draw: raycast + select + (levels-1) pyramid up +
-    # (levels-1) down + total + compact; page-request service: de-duplication
-    # (first, count, scan, scatter) + classification (count, scan, scatter) +
-    # LRU order partition (count, scan, scatter) + brick production + node patch
-    levels = 11
-    draw_launches = 1 + 1 + 2 * (levels - 1) + 1 + 1
-    service_launches = 4 + 3 + 3 + 1 + 1
+    # our kernels per step (as the launch list of profiles/paged_1080p_launch_list.md
+    # counts them). draw: raycast + the three-launch selection / histopyramid /
+    # compaction; page-request service: request-count read-out, de-duplication
+    # (count, first, two scans, scatter), classification (count, scan,
+    # scatter), LRU order partition (count, scatter), the candidates'
+    # read-out, the pull of jobs and patches, brick production, node patch
+    draw_launches = 1 + 3
+    service_launches = 1 + 5 + 3 + 2 + 1 + 1 + 1 + 1
     out["gpu_launches"] = args.steps * (draw_launches + service_launches)
     if world == 1:
         out["batched_fp16"] = batched_fp16_leg(vv, octree, cams, local_rank, peak)
