@@ -54,7 +54,7 @@ def test_request_set_covers_all_kept_items(g):
 
 
 @pytest.mark.parametrize("w,h,cap", [(64, 64, 0), (65, 65, 0), (127, 95, 0), (129, 1, 0), (2047, 3, 0), (97, 191, 0),
-                                     (640, 480, 0), (1920, 1080, 5000), (1023, 767, 0)])
+                                     (640, 480, 0), (1920, 1080, 5000), (1023, 767, 0), (4096, 2160, 0)])
 def test_three_launch_compaction_equals_per_level(g, w, h, cap):
     """vv_ctx_set_compaction: the three-launch form (selection and the
     pyramid's lowest five levels per level-5 node, the levels above in one
