@@ -97,7 +97,7 @@ __device__ __forceinline__ void subtree(const Levels& L, int X, int Y, Subtree& 
 constexpr int kSubtreeCells = kFoot * kFoot + (kFoot / 2) * (kFoot / 2) + (kFoot / 4) * (kFoot / 4) +
                               (kFoot / 8) * (kFoot / 8) + (kFoot / 16) * (kFoot / 16) + 4 + 1;
 
-__device__ __forceinline__ uint32_t sub_cell(const uint32_t* a, const Subtree& t, int k, int x, int y) {
+__device__ __forceinline__ uint32_t sub_cell(const uint16_t* a, const Subtree& t, int k, int x, int y) {
     if (x < t.x0[k] || x >= t.x1[k] || y < t.y0[k] || y >= t.y1[k]) return 0u;  // outside the level
     return a[t.base[k] + (y - t.y0[k]) * (t.x1[k] - t.x0[k]) + (x - t.x0[k])];
 }
@@ -113,7 +113,7 @@ constexpr int kWarpCells = 64;
 
 // Level k+1 of the subtree's counts from level k's (cells i = first, first
 // + step, ...).
-__device__ __forceinline__ void up_level(const Levels& L, const Subtree& t, uint32_t* cnt, int k, int first,
+__device__ __forceinline__ void up_level(const Levels& L, const Subtree& t, uint16_t* cnt, int k, int first,
                                          int step) {
     const int w = t.x1[k + 1] - t.x0[k + 1], n = level_cells(t, k + 1);
     for (int i = first; i < n; i += step) {
@@ -124,13 +124,13 @@ __device__ __forceinline__ void up_level(const Levels& L, const Subtree& t, uint
             kids.at(j, cx, cy);
             sum += sub_cell(cnt, t, k, cx, cy);
         }
-        cnt[t.base[k + 1] + i] = sum;
+        cnt[t.base[k + 1] + i] = (uint16_t)sum;
     }
 }
 
 // counts of levels 1..kCut of the subtree from level 0's (in cnt); on
 // return warp 0 has every level, the other warps the block-swept ones
-__device__ __forceinline__ void sweep_up(const Levels& L, const Subtree& t, uint32_t* cnt) {
+__device__ __forceinline__ void sweep_up(const Levels& L, const Subtree& t, uint16_t* cnt) {
     int k = 0;
     for (; k < kCut && level_cells(t, k + 1) > kWarpCells; ++k) {
         up_level(L, t, cnt, k, threadIdx.x, blockDim.x);
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_up_kernel(const __grid_cons
                                                                 const uint4* __restrict__ usage,
                                                                 uint32_t* __restrict__ mask,
                                                                 uint32_t* __restrict__ cut_counts) {
-    __shared__ uint32_t cnt[kSubtreeCells];
+    __shared__ uint16_t cnt[kSubtreeCells];  // counts of at most 63 x 63 pixels fit in 16 bits
     __shared__ Subtree t;
     __shared__ uint32_t wsum[kTileThreads / 32];
     const int X = blockIdx.x, Y = blockIdx.y;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_up_kernel(const __grid_cons
         const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
         const uint32_t bits = select_bits(usage, x, y, W, H);
         mask[(size_t)y * W + x] = bits;
-        cnt[i] = bits != 0u ? 1u : 0u;
+        cnt[i] = bits != 0u ? 1 : 0;
     }
     __syncthreads();
     sweep_up(L, t, cnt);
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kTopThreads) top_kernel(const __grid_constant_
 // Level k of the subtree's offsets from level k+1's: each parent (i = first,
 // first + step, ...) hands its offset plus the counts of the children before
 // each child down.
-__device__ __forceinline__ void down_level(const Levels& L, const Subtree& t, const uint32_t* cnt, uint32_t* off,
+__device__ __forceinline__ void down_level(const Levels& L, const Subtree& t, const uint16_t* cnt, uint32_t* off,
                                            int k, int first, int step) {
     const int pw = t.x1[k + 1] - t.x0[k + 1], n = level_cells(t, k + 1);
     const int w = t.x1[k] - t.x0[k];
@@ -309,7 +309,7 @@ __device__ __forceinline__ void write_request(const TileDown& p, size_t pix, uin
 }
 
 __global__ void __launch_bounds__(kTileThreads) tile_down_kernel(const __grid_constant__ TileDown p) {
-    __shared__ uint32_t cnt[kSubtreeCells];
+    __shared__ uint16_t cnt[kSubtreeCells];  // counts of at most 63 x 63 pixels fit in 16 bits
     __shared__ uint32_t off[kSubtreeCells];
     __shared__ Subtree t;
     __shared__ uint32_t wtot[kTileThreads / 32];
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_down_kernel(const __grid_co
     }
     for (int i = threadIdx.x; i < n0; i += blockDim.x) {
         const int x = t.x0[0] + i % w0, y = t.y0[0] + i / w0;
-        cnt[i] = p.mask[(size_t)y * W + x] != 0u ? 1u : 0u;
+        cnt[i] = p.mask[(size_t)y * W + x] != 0u ? 1 : 0;
     }
     __syncthreads();
     sweep_up(L, t, cnt);
