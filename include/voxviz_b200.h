@@ -336,8 +336,10 @@ int vv_backward(vv_ctx* ctx, int32_t tree, const vv_uniforms* u, const float* dl
  * per texel and cell group. */
 #define VV_GRAD_WARP_SUM 2
 /* Spread the atomics of a binary32 gradient (not with VV_GRAD_F64, else
- * VV_ERR_ARG) over VV_GRAD_SPREAD_COPIES copies of the rows: the warps of a
- * CTA add to different copies (fewer concurrent atomics on one address).
+ * VV_ERR_ARG) over VV_GRAD_SPREAD_COPIES copies of the rows: the four warps
+ * of a CTA add to different copies (fewer concurrent atomics on one
+ * address; eight copies would also separate neighbouring CTAs, for 1-3 %
+ * on the paged frames at twice the memory).
  * The extra copies live in context memory ((copies - 1) * rows * 16000
  * bytes, rows = rows_cap with a slot map, else the pool's slots; kept
  * between calls) and are added into `grad` on the stream after the adjoint

@@ -126,7 +126,8 @@ __device__ __forceinline__ void texel_atomic(const GradTarget& gt, size_t i, flo
         atomicAdd(g + 3, (double)v.w);
     } else {
         float4* g = (float4*)gt.grad + i;
-        const unsigned c = (threadIdx.x >> 5) & (unsigned)(gt.copies - 1);
+        // the warp's copy: its index in the CTA, then the CTA's column parity
+        const unsigned c = ((threadIdx.x >> 5) | ((blockIdx.x & 1u) << 2)) & (unsigned)(gt.copies - 1);
         if (c) g = gt.spread + (size_t)(c - 1u) * (size_t)gt.spread_rows * 1000u + i;
         asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(g), "f"(v.x), "f"(v.y), "f"(v.z),
                      "f"(v.w)
@@ -366,6 +367,8 @@ cudaError_t launch_spread_reduce(const GradTarget& grad, cudaStream_t s) {
         case 2: spread_reduce_kernel<1><<<blocks, threads, 0, s>>>((float4*)grad.grad, grad.spread, grad.rows_used,
                                                                    grad.spread_rows); break;
         case 4: spread_reduce_kernel<3><<<blocks, threads, 0, s>>>((float4*)grad.grad, grad.spread, grad.rows_used,
+                                                                   grad.spread_rows); break;
+        case 8: spread_reduce_kernel<7><<<blocks, threads, 0, s>>>((float4*)grad.grad, grad.spread, grad.rows_used,
                                                                    grad.spread_rows); break;
         default: return cudaErrorInvalidValue;
     }

@@ -69,10 +69,11 @@ cudaError_t launch_forward_ckpt(int fmt, const RaycastParams& p, void* ckpt, int
 // 4 doubles) per texel, 1000 texels per row; row = brick-pool slot (dense,
 // slot_map NULL) or the row the slot map assigns (claimed on first touch
 // from rows_used, at most rows_cap rows).  With copies > 1 (binary32 rows)
-// warp w of a CTA adds to copy w % copies: copy 0 is `grad`, copy k > 0
-// starts at spread + (k - 1) * spread_rows * 1000 (spread_rows = rows_cap,
-// or the pool's slots for dense rows; all zero before the first launch;
-// launch_spread_reduce adds the rows in use into `grad` and zeroes them).
+// warp w of CTA b adds to copy (w + 4 (b.x mod 2)) mod copies: copy 0 is
+// `grad`, copy k > 0 starts at spread + (k - 1) * spread_rows * 1000
+// (spread_rows = rows_cap, or the pool's slots for dense rows; all zero
+// before the first launch; launch_spread_reduce adds the rows in use into
+// `grad` and zeroes them).
 struct GradTarget {
     void* grad;
     int f64;
@@ -80,7 +81,7 @@ struct GradTarget {
     int* slot_map;
     int* rows_used;
     int rows_cap;
-    int copies;       // 1, 2 or 4
+    int copies;       // 1, 2, 4 or 8
     float4* spread;   // copies 1..copies-1
     int spread_rows;  // rows per copy
 };
